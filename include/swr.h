@@ -1,0 +1,197 @@
+/* swr.h - C ABI of the B200 path tracer (drop-in for vikkre/master_thesis's SoftwareRenderer
+ * PathTracer path).
+ *
+ * Conventions
+ *  - Every call returns an int status: SWR_OK (0) or one of the SWR_ERR_* codes. No C++ exception
+ *    crosses this boundary. swr_last_error() returns a thread-local "system: message" string for
+ *    the last failure on the calling thread, in the spirit of the reference's InitException
+ *    (software_renderer/init_exception.h:9-19).
+ *  - Pointers are plain C pointers. Arguments documented "device or host" may point to either;
+ *    the library inspects the pointer and stages host memory through the device itself.
+ *  - Device work is queued on the given CUDA stream (a cudaStream_t passed as void*, NULL = the
+ *    legacy default stream) and is asynchronous unless stated; swr_sync waits for it. A scene
+ *    handle must not be used by two host threads at the same time; different handles on different
+ *    streams may run concurrently.
+ */
+#ifndef SWR_H
+#define SWR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWR_ABI_VERSION 1
+
+enum {
+  SWR_OK = 0,
+  SWR_ERR_IO = 1,          /* file missing / unreadable (InitException from the loaders) */
+  SWR_ERR_PARSE = 2,       /* malformed scene / camera / renderer / mesh file */
+  SWR_ERR_ALLOC = 3,       /* device or host allocation failed */
+  SWR_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+  SWR_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  SWR_ERR_INVALID = 6,     /* bad argument */
+  SWR_ERR_UNSUPPORTED = 7  /* valid request this build does not handle */
+};
+
+/* Render semantics.
+ * SWR_MODE_REFERENCE: exactly the reference's PathTracer::traceSinglePath (path_tracer.cpp:42-97):
+ *   pixel-centre camera rays, the first back-face hits skipped (using up a depth slot), a path
+ *   contributes its throughput product only when it hits a light source from the front, no
+ *   Russian roulette, image = sum * 2*pi/spp (lightStrength is not used, as in the reference).
+ * SWR_MODE_PHYSICAL: the same scenes and random numbers with emission L_e = color * lightStrength
+ *   collected at emitters hit from the front (emitters absorb), two-sided Lambertian BRDF with
+ *   per-triangle albedo, uniform-hemisphere sampling weight 2*albedo*cos, optional Russian
+ *   roulette with a constant survival probability, image = sum / spp. */
+enum { SWR_MODE_REFERENCE = 0, SWR_MODE_PHYSICAL = 1 };
+
+typedef struct swr_material {
+  float color[3];          /* GraphicsObject::color */
+  float diffuse_t;         /* cumulative event thresholds, graphics_object.cpp:48-51 */
+  float reflect_t;
+  float transparent_t;
+  float refraction_index;
+  uint32_t light_source;   /* nonzero for lightSource(...) objects */
+  float light_strength;
+} swr_material;
+
+/* World-space scene. Triangles are numbered in object-major order (the global triangle id of
+ * the hit results); objects in scene-file order. */
+typedef struct swr_scene_desc {
+  uint32_t num_objects;
+  uint32_t num_vertices;
+  uint32_t num_triangles;
+  uint32_t reserved;
+  const float* vertex_pos;             /* [num_vertices*3] world positions */
+  const float* vertex_normal;          /* [num_vertices*3] world normals as the reference keeps
+                                          them (transformed, not renormalised) */
+  const uint32_t* tri_vertices;        /* [num_triangles*3] global vertex indices v0 v1 v2 */
+  const uint32_t* tri_object;          /* [num_triangles] owning object, non-decreasing */
+  const uint32_t* tri_rank;            /* [num_triangles] position in the reference's visit order
+                                          (closest-hit ties go to the lower rank); NULL = id order */
+  const uint32_t* object_first_vertex; /* [num_objects+1] vertex range of each object; its box is
+                                          built over that range in order, first point padded */
+  const swr_material* materials;       /* [num_objects] */
+  const float* tri_albedo;             /* [num_triangles*3] or NULL (physical mode albedo) */
+} swr_scene_desc;
+
+typedef struct swr_build_opts {
+  uint32_t sah_bins;       /* 0 = 32 */
+  uint32_t max_leaf;       /* triangles per leaf, 1..3; 0 = 3 */
+  uint32_t threads;        /* host build threads, 0 = all */
+  uint32_t reserved;
+} swr_build_opts;
+
+/* Camera as GraphicsEngine::render derives it (graphics_engine.cpp:42-46): inverse view and
+ * projection matrices (row-major m[row][col], row-vector convention) and the eye position. */
+typedef struct swr_camera {
+  float view_inv[16];
+  float proj_inv[16];
+  float origin[3];
+  float reserved;
+} swr_camera;
+
+typedef struct swr_render_opts {
+  uint32_t width, height;  /* image size (argv[3], argv[4] of the reference CLI) */
+  uint32_t spp;            /* raysPerPixel */
+  uint32_t max_depth;      /* visionJumpCount, 1..31 */
+  uint64_t seed;           /* key of the counter-based RNG */
+  uint32_t mode;           /* SWR_MODE_* */
+  uint32_t rr_depth;       /* physical mode: Russian roulette at path vertices >= rr_depth (0=off) */
+  float rr_survive;        /* physical mode: survival probability, (0, 1] */
+  uint32_t wave_size;      /* paths in flight, 0 = automatic */
+  uint32_t block_size;     /* threads per block of the shading kernel, 0 = automatic */
+  uint32_t flags;          /* SWR_RENDER_* */
+} swr_render_opts;
+
+#define SWR_RENDER_SAMPLES_OUT 1u   /* write per-sample radiance to the samples buffer */
+
+typedef struct swr_hit {
+  uint32_t tri;            /* global triangle id, 0xFFFFFFFF on a miss */
+  uint32_t obj;            /* object index, 0xFFFFFFFF on a miss */
+  float dist2;             /* squared distance origin -> hit point, the reference's comparison key */
+  float t;                 /* ray parameter of the hit */
+} swr_hit;
+
+typedef struct swr_scene swr_scene;
+typedef struct swr_host_scene swr_host_scene;
+
+/* ---------------------------------------------------------------------------------------------
+ * Library */
+const char* swr_last_error(void);
+int swr_abi_version(void);
+/* Waits for all work queued on stream. */
+int swr_sync(void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Host-side file surface (software_renderer/mesh_manager.cpp:30-60 createObjectsFromFile,
+ * obj_loader.cpp, stl_loader.cpp, input_parser.cpp, graphic/graphics_object.cpp:12-52 init).
+ * OBJ meshes are read from basepath + "../res/obj/", STL meshes from "../res/stl/" relative to
+ * the working directory, exactly like the reference. */
+int swr_host_scene_load(const char* scene_path, const char* basepath, swr_host_scene** out);
+/* Fills a descriptor whose arrays point into the host scene (valid until it is freed). */
+int swr_host_scene_desc(const swr_host_scene* hs, swr_scene_desc* out);
+/* 1 when every tie rank comes from the reference's exact BVH order, 0 when some mesh was too
+ * large for it (then ties inside that mesh go to the lower triangle index). */
+int swr_host_scene_ranks_exact(const swr_host_scene* hs);
+void swr_host_scene_free(swr_host_scene* hs);
+
+/* Camera file -> per-image matrices (camera.cpp:19-51, graphics_engine.cpp:42-46). With
+ * use_fov_key nonzero an optional fov(degrees) key is honoured; otherwise the field of view is the
+ * reference's fixed pi/4. */
+int swr_camera_load(const char* camera_path, uint32_t width, uint32_t height, uint32_t use_fov_key,
+                    swr_camera* out);
+/* Renderer file (main.cpp:62-66, path_tracer.cpp:13-16): accepts PathTracer; returns its
+ * visionJumpCount and raysPerPixel. */
+int swr_renderer_load(const char* renderer_path, uint32_t* max_depth, uint32_t* spp);
+
+/* Derived per-triangle data exactly as the reference's Triangle / GraphicsObject compute them
+ * (triangle.cpp:4-17, graphics_object.cpp:25): edges e0 = v1-v0, e1 = v2-v0 [3*ntri each],
+ * den = d00 d01 d11 denom [4*ntri], triangle boxes lo.xyz hi.xyz [6*ntri], object boxes
+ * [6*nobj]. Any output may be NULL. Host memory. */
+int swr_scene_derive(const swr_scene_desc* desc, float* tri_e0, float* tri_e1, float* tri_den,
+                     float* tri_box, float* obj_box);
+
+/* ---------------------------------------------------------------------------------------------
+ * Device scene (replaces MeshManager + GraphicsEngine::init + Scene::init, scene.cpp:13-20). The
+ * library copies what it needs; the caller keeps ownership of the descriptor's arrays. */
+int swr_scene_create(const swr_scene_desc* desc, const swr_build_opts* opts, swr_scene** out);
+void swr_scene_destroy(swr_scene* scene);
+/* Wide-BVH statistics: nodes, depth, bytes of nodes and triangle records. */
+int swr_scene_stats(const swr_scene* scene, uint64_t out[8]);
+
+/* Closest hit per ray (replaces Scene::traceRay, scene.cpp:22-56, with its exact semantics:
+ * same triangle, same squared distance, ties to the reference's visit order).
+ * ray_o, ray_d: [n*4] floats (x y z unused), device or host. out: [n] swr_hit, device or host. */
+int swr_trace_closest(swr_scene* scene, const float* ray_o, const float* ray_d, uint64_t n,
+                      swr_hit* out, void* stream);
+
+/* As swr_trace_closest, also writing per ray the number of wide-BVH nodes visited and triangles
+ * tested (counts: [2*n] uint32, device or host). Instrumentation for the traffic model. */
+int swr_trace_closest_stats(swr_scene* scene, const float* ray_o, const float* ray_d, uint64_t n,
+                            swr_hit* out, uint32_t* counts, void* stream);
+
+/* Full image (replaces GraphicsEngine::render + PathTracer::renderPixel,
+ * graphics_engine.cpp:42-97, path_tracer.cpp:18-40). rgb_out: [height*width*3] floats, row-major
+ * (x + y*width)*3 as the reference's image buffer, unclamped radiance, device or host.
+ * samples_out (optional, only with SWR_RENDER_SAMPLES_OUT): [height*width*spp*4] floats, per
+ * sample r g b and a flag (1 = the path reached a light), device or host. */
+int swr_render(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts, float* rgb_out,
+               float* samples_out, void* stream);
+
+/* As swr_render, also returning the number of rays traced (camera prefix + all bounces). */
+int swr_render_stats(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
+                     float* rgb_out, float* samples_out, void* stream, uint64_t* rays_traced);
+
+/* Reference-style 8-bit quantisation (graphics_engine.cpp:90-95: clamp to [0,1], *255, truncate)
+ * and P6 PPM writer (graphics_engine.cpp:32-40). Host memory. */
+int swr_quantize_rgb8(const float* rgb, uint32_t width, uint32_t height, uint8_t* out);
+int swr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWR_H */

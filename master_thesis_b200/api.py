@@ -1,0 +1,200 @@
+"""Python tooling over the C ABI: world-space scene data, the device scene handle, closest-hit
+queries and renders. Device buffers are torch tensors; host buffers are numpy arrays (the
+library stages host memory itself, which is the end-to-end path the reference's callers see).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _native as N
+from ._native import check, ptr
+
+MAT_DTYPE = np.dtype([("color", "<f4", (3,)), ("diffuse_t", "<f4"), ("reflect_t", "<f4"),
+                      ("transparent_t", "<f4"), ("refraction_index", "<f4"),
+                      ("light_source", "<u4"), ("light_strength", "<f4")])
+assert MAT_DTYPE.itemsize == ctypes.sizeof(N.Material)
+
+
+class SceneData:
+    """World-space scene in the layout of swr_scene_desc (numpy, host memory)."""
+
+    def __init__(self, vpos, vnrm, tri, tri_obj, obj_first_vertex, materials, tri_rank=None,
+                 tri_albedo=None, ranks_exact=True):
+        self.vpos = np.ascontiguousarray(vpos, dtype=np.float32).reshape(-1, 3)
+        self.vnrm = np.ascontiguousarray(vnrm, dtype=np.float32).reshape(-1, 3)
+        self.tri = np.ascontiguousarray(tri, dtype=np.uint32).reshape(-1, 3)
+        self.tri_obj = np.ascontiguousarray(tri_obj, dtype=np.uint32).reshape(-1)
+        self.obj_first_vertex = np.ascontiguousarray(obj_first_vertex, dtype=np.uint32).reshape(-1)
+        self.materials = np.ascontiguousarray(materials, dtype=MAT_DTYPE).reshape(-1)
+        self.tri_rank = None if tri_rank is None else np.ascontiguousarray(tri_rank, dtype=np.uint32).reshape(-1)
+        self.tri_albedo = None if tri_albedo is None else np.ascontiguousarray(tri_albedo, dtype=np.float32).reshape(-1, 3)
+        self.ranks_exact = ranks_exact
+
+    @property
+    def num_triangles(self):
+        return self.tri.shape[0]
+
+    @property
+    def num_objects(self):
+        return self.materials.shape[0]
+
+    def desc(self):
+        d = N.SceneDesc()
+        d.num_objects = self.num_objects
+        d.num_vertices = self.vpos.shape[0]
+        d.num_triangles = self.num_triangles
+        d.vertex_pos = ptr(self.vpos)
+        d.vertex_normal = ptr(self.vnrm)
+        d.tri_vertices = ptr(self.tri)
+        d.tri_object = ptr(self.tri_obj)
+        d.tri_rank = ptr(self.tri_rank)
+        d.object_first_vertex = ptr(self.obj_first_vertex)
+        d.materials = ptr(self.materials)
+        d.tri_albedo = ptr(self.tri_albedo)
+        return d
+
+    def derive(self):
+        """Edges, dot products, triangle and object boxes as the reference computes them."""
+        nt, no = self.num_triangles, self.num_objects
+        out = dict(e0=np.empty((nt, 3), np.float32), e1=np.empty((nt, 3), np.float32),
+                   den=np.empty((nt, 4), np.float32), tri_box=np.empty((nt, 6), np.float32),
+                   obj_box=np.empty((no, 6), np.float32))
+        d = self.desc()
+        check(N.lib.swr_scene_derive(ctypes.byref(d), ptr(out["e0"]), ptr(out["e1"]),
+                                     ptr(out["den"]), ptr(out["tri_box"]), ptr(out["obj_box"])))
+        return out
+
+
+def load_scene(scene_path, basepath):
+    """Scene file -> SceneData through the library's MeshManager-equivalent loader."""
+    h = ctypes.c_void_p()
+    check(N.lib.swr_host_scene_load(os.fsencode(scene_path), os.fsencode(basepath), ctypes.byref(h)))
+    try:
+        d = N.SceneDesc()
+        check(N.lib.swr_host_scene_desc(h, ctypes.byref(d)))
+        nv, nt, no = d.num_vertices, d.num_triangles, d.num_objects
+
+        def arr(p, n, dt):
+            return np.ctypeslib.as_array((dt * n).from_address(p)).copy()
+
+        vpos = arr(d.vertex_pos, nv * 3, ctypes.c_float)
+        vnrm = arr(d.vertex_normal, nv * 3, ctypes.c_float)
+        tri = arr(d.tri_vertices, nt * 3, ctypes.c_uint32)
+        tobj = arr(d.tri_object, nt, ctypes.c_uint32)
+        rank = arr(d.tri_rank, nt, ctypes.c_uint32)
+        ofv = arr(d.object_first_vertex, no + 1, ctypes.c_uint32)
+        mats = np.frombuffer(ctypes.string_at(d.materials, no * MAT_DTYPE.itemsize), dtype=MAT_DTYPE).copy()
+        exact = bool(N.lib.swr_host_scene_ranks_exact(h))
+    finally:
+        N.lib.swr_host_scene_free(h)
+    return SceneData(vpos, vnrm, tri, tobj, ofv, mats, tri_rank=rank, ranks_exact=exact)
+
+
+def load_camera(camera_path, width, height, use_fov_key=False):
+    c = N.Camera()
+    check(N.lib.swr_camera_load(os.fsencode(camera_path), width, height, 1 if use_fov_key else 0,
+                                ctypes.byref(c)))
+    return c
+
+
+def camera_arrays(cam):
+    return (np.array(cam.view_inv, np.float32).reshape(4, 4),
+            np.array(cam.proj_inv, np.float32).reshape(4, 4),
+            np.array(cam.origin, np.float32))
+
+
+def load_renderer(renderer_path):
+    depth, spp = ctypes.c_uint32(), ctypes.c_uint32()
+    check(N.lib.swr_renderer_load(os.fsencode(renderer_path), ctypes.byref(depth), ctypes.byref(spp)))
+    return depth.value, spp.value
+
+
+def _stream_handle(stream):
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except ImportError:
+            pass
+        return None
+    return getattr(stream, "cuda_stream", stream)
+
+
+class Scene:
+    """Device scene (wide BVH + triangle records) built from SceneData."""
+
+    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0):
+        self.data = data
+        d = data.desc()
+        o = N.BuildOpts(sah_bins, max_leaf, threads, 0)
+        self._h = ctypes.c_void_p()
+        check(N.lib.swr_scene_create(ctypes.byref(d), ctypes.byref(o), ctypes.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib.swr_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stats(self):
+        out = (ctypes.c_uint64 * 8)()
+        check(N.lib.swr_scene_stats(self._h, out))
+        keys = ["nodes", "depth", "node_bytes", "tri_bytes", "triangles", "objects", "node_size", "tri_size"]
+        return dict(zip(keys, list(out)))
+
+    def trace(self, ray_o, ray_d, out=None, counts=None, stream=None):
+        """Closest hit per ray. ray_o/ray_d: (n,4) float32 (numpy = host, torch cuda = device).
+        Returns (n,4) uint32-viewed hits (tri, obj, dist2 bits, t bits) of the same kind."""
+        n = ray_o.shape[0]
+        if out is None:
+            if isinstance(ray_o, np.ndarray):
+                out = np.empty((n, 4), np.uint32)
+            else:
+                import torch
+                out = torch.empty((n, 4), dtype=torch.int32, device=ray_o.device)
+        s = _stream_handle(stream)
+        if counts is not None:
+            check(N.lib.swr_trace_closest_stats(self._h, ptr(ray_o), ptr(ray_d), n, ptr(out), ptr(counts), s))
+        else:
+            check(N.lib.swr_trace_closest(self._h, ptr(ray_o), ptr(ray_d), n, ptr(out), s))
+        return out
+
+    def render(self, cam, width, height, spp, depth, seed=0, mode=N.MODE_REFERENCE, rr_depth=0,
+               rr_survive=1.0, wave_size=0, block_size=0, out=None, samples=None, stream=None,
+               return_rays=False):
+        """Renders an image (height, width, 3) float32 into `out` (torch cuda tensor or numpy)."""
+        o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size,
+                         block_size, N.RENDER_SAMPLES_OUT if samples is not None else 0)
+        if out is None:
+            import torch
+            out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+        s = _stream_handle(stream)
+        rays = ctypes.c_uint64(0)
+        check(N.lib.swr_render_stats(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(out), ptr(samples),
+                                     s, ctypes.byref(rays)))
+        return (out, rays.value) if return_rays else out
+
+
+def quantize_rgb8(img):
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    h, w = img.shape[:2]
+    out = np.empty((h, w, 3), np.uint8)
+    check(N.lib.swr_quantize_rgb8(ptr(img), w, h, ptr(out)))
+    return out
+
+
+def write_ppm(path, rgb8):
+    rgb8 = np.ascontiguousarray(rgb8, dtype=np.uint8)
+    h, w = rgb8.shape[:2]
+    check(N.lib.swr_write_ppm(os.fsencode(path), ptr(rgb8), w, h))

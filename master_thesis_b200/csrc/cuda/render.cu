@@ -1,0 +1,450 @@
+// Wavefront path tracer (C ABI: swr_render).
+//
+// Work decomposition: a global sample index g = pixel * spp + sample over the image (processed
+// in pixel chunks). Per chunk:
+//   k_camera   one thread per pixel: primary ray through the pixel centre and the reference's
+//              back-face skipping prefix (path_tracer.cpp:50-57). This prefix uses no random
+//              numbers, so it is the same for every sample of the pixel and is traced once per
+//              pixel; its first scattering hit is stored in a per-pixel record.
+//   loop until no path is live and every sample has been injected:
+//     k_shade  shades the traced queue and injects new samples (taking their first hit from the
+//              pixel record) up to the queue capacity; continuing paths are appended to the other
+//              queue with one atomic per warp (ballot + popc compaction); finished samples write
+//              their radiance to a per-sample slot.
+//     k_trace  persistent closest-hit traversal over the new queue.
+//   k_resolve  sums each pixel's sample slots in sample order and scales, as renderPixel does.
+// Queue counters and the injection window live in a small device control block that the
+// kernels advance themselves, so the host only launches kernels and polls completion.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "shading.cuh"
+#include "swr_internal.cuh"
+
+namespace swr {
+namespace {
+
+using swrx::f3;
+using swrx::mk;
+
+constexpr uint32_t kDeadSlot = 0xFFFFFFFFu;
+constexpr int kTraceBlock = 128;
+constexpr uint64_t kChunkSamples = 1ull << 27;
+
+struct Ctrl {
+  unsigned int count[2];
+  unsigned int cursor[2];
+  unsigned int inj_n[2];
+  unsigned int pad0[2];
+  unsigned long long inj_base[2];
+  unsigned long long injected;
+  unsigned long long total;
+  unsigned long long rays;
+  unsigned long long pad1;
+};
+
+struct Queue {
+  float4* o;  // o.xyz | pixel (chunk-local)
+  float4* d;  // d.xyz | sample
+  float4* c;  // throughput | (i << 8) | v
+  float4* l;  // physical: gathered radiance
+  uint2* hit;  // slot | t
+};
+
+struct Frame {
+  float vi[16], pi[16];
+  float org[3];
+  uint32_t W, H, spp, depth, mode, rr_depth;
+  float rr_q;
+  uint64_t seed;
+  uint32_t pixel0;   // first pixel of the chunk
+  uint32_t npix;     // pixels in the chunk
+  uint32_t capacity;
+  float4* cam;       // [npix*2] per-pixel first hit: (o, t) (d, slot | i << 27)
+  float4* contrib;   // [npix*spp] per-sample radiance + flag
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__global__ void __launch_bounds__(kTraceBlock) k_camera(DevScene sc, Frame F, Ctrl* __restrict__ ctrl) {
+  __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned traced = 0;
+  if (k < F.npix) {
+  const uint32_t pix = F.pixel0 + k;
+  const uint32_t px = pix % F.W, py = pix / F.W;
+  f3 o = mk(F.org[0], F.org[1], F.org[2]);
+  const f3 d = swrx::primary_dir(F.vi, F.pi, px, py, F.W, F.H);
+  float4 rec0 = make_float4(0, 0, 0, 0), rec1 = make_float4(0, 0, 0, __uint_as_float(kDeadSlot));
+  for (uint32_t i = 0; i < F.depth; ++i) {
+    swrx::Hit h;
+    ++traced;
+    if (!swrx::trace_closest<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, o, d,
+                                    stack + threadIdx.x, kTraceBlock, h, nullptr))
+      break;
+    const f3 p = swrx::hit_point(o, d, h.t);
+    const f3 n = swrx::shading_normal(sc.tris, sc.shade, h.slot, p);
+    if (swrx::vdot(n, d) > 0.0f) {
+      o = swrx::vadd(p, swrx::vscale(0.01f, d));
+      continue;
+    }
+    rec0 = make_float4(o.x, o.y, o.z, h.t);
+    rec1 = make_float4(d.x, d.y, d.z, __uint_as_float(h.slot | (i << 27)));
+    break;
+  }
+  F.cam[2 * (size_t)k] = rec0;
+  F.cam[2 * (size_t)k + 1] = rec1;
+  }
+  // count the traced camera-prefix rays: warp sum, one atomic per warp
+  for (int off = 16; off > 0; off >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, off);
+  if (lane_id() == 0 && traced) atomicAdd(&ctrl->rays, (unsigned long long)traced);
+}
+
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock)
+    k_shade(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, Queue in, Queue out, int parity) {
+  const uint32_t n_in = ctrl->count[parity];
+  const uint32_t n_inj = ctrl->inj_n[parity];
+  const unsigned long long inj_base = ctrl->inj_base[parity];
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (blockIdx.x * kBlock >= n_in + n_inj) return;
+
+  bool live = false;
+  swrx::PathState st;
+  uint32_t pixel = 0, sample = 0, slot = kDeadSlot;
+  float t = 0.0f;
+  bool have = false;
+  if (i < n_in) {
+    const float4 qo = in.o[i], qd = in.d[i], qc = in.c[i];
+    const uint2 h = in.hit[i];
+    pixel = __float_as_uint(qo.w);
+    sample = __float_as_uint(qd.w);
+    const uint32_t meta = __float_as_uint(qc.w);
+    st.o = mk(qo.x, qo.y, qo.z);
+    st.d = mk(qd.x, qd.y, qd.z);
+    st.c = mk(qc.x, qc.y, qc.z);
+    st.i = (meta >> 8) & 0xFFu;
+    st.v = meta & 0xFFu;
+    if (F.mode == 1) {
+      const float4 ql = in.l[i];
+      st.L = mk(ql.x, ql.y, ql.z);
+    } else {
+      st.L = mk(0, 0, 0);
+    }
+    slot = h.x;
+    t = __uint_as_float(h.y);
+    have = true;
+  } else if (i < n_in + n_inj) {
+    const unsigned long long g = inj_base + (i - n_in);
+    pixel = (uint32_t)(g / F.spp);
+    sample = (uint32_t)(g % F.spp);
+    const float4 r0 = F.cam[2 * (size_t)pixel], r1 = F.cam[2 * (size_t)pixel + 1];
+    const uint32_t bits = __float_as_uint(r1.w);
+    st.c = mk(1.0f, 1.0f, 1.0f);
+    st.L = mk(0.0f, 0.0f, 0.0f);
+    st.v = 0;
+    if (bits != kDeadSlot) {
+      st.o = mk(r0.x, r0.y, r0.z);
+      st.d = mk(r1.x, r1.y, r1.z);
+      st.i = bits >> 27;
+      slot = bits & 0x07FFFFFFu;
+      t = r0.w;
+    }
+    have = true;
+  }
+  if (have) {
+    uint32_t outcome = swrx::kEndDark;
+    if (slot != kDeadSlot) {
+      swrx::ShadeParams P;
+      P.seed = F.seed;
+      P.pixel = F.pixel0 + pixel;
+      P.sample = sample;
+      P.depth = F.depth;
+      P.mode = F.mode;
+      P.rr_depth = F.rr_depth;
+      P.rr_q = F.rr_q;
+      outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
+    }
+    if (outcome == swrx::kContinue) {
+      live = true;
+    } else {
+      float4 r;
+      if (F.mode == 0)
+        r = (outcome == swrx::kEndLight) ? make_float4(st.c.x, st.c.y, st.c.z, 1.0f)
+                                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      else
+        r = make_float4(st.L.x, st.L.y, st.L.z, 1.0f);
+      F.contrib[(size_t)pixel * F.spp + sample] = r;
+    }
+  }
+  // warp-aggregated append of the live paths
+  const unsigned mask = __ballot_sync(0xffffffffu, live);
+  if (mask == 0u) return;
+  unsigned base = 0;
+  const unsigned leader = __ffs(mask) - 1;
+  if (lane_id() == leader) base = atomicAdd(&ctrl->count[parity ^ 1], (unsigned)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (live) {
+    const unsigned j = base + __popc(mask & ((1u << lane_id()) - 1u));
+    out.o[j] = make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel));
+    out.d[j] = make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample));
+    out.c[j] = make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((st.i << 8) | st.v));
+    if (F.mode == 1) out.l[j] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+  }
+}
+
+__global__ void __launch_bounds__(kTraceBlock)
+    k_trace(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, Queue q, int parity) {
+  __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
+  // parity p: trace queue p^1, prepare the injection window of the next shade (parity p^1)
+  const int qp = parity ^ 1;
+  const unsigned n = ctrl->count[qp];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long rem = ctrl->total - ctrl->injected;
+    const unsigned long long room = (unsigned long long)F.capacity - n;
+    const unsigned long long m = rem < room ? rem : room;
+    ctrl->inj_base[qp] = ctrl->injected;
+    ctrl->inj_n[qp] = (unsigned)m;
+    ctrl->injected += m;
+    ctrl->count[parity] = 0u;
+    ctrl->rays += n;
+  }
+  for (;;) {
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(&ctrl->cursor[qp], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const unsigned i = base + lane_id();
+    if (i < n) {
+      const float4 o = q.o[i], d = q.d[i];
+      swrx::Hit h;
+      swrx::trace_closest<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, mk(o.x, o.y, o.z),
+                                 mk(d.x, d.y, d.z), stack + threadIdx.x, kTraceBlock, h, nullptr);
+      q.hit[i] = make_uint2(h.slot, __float_as_uint(h.t));
+    }
+  }
+}
+
+__global__ void k_resolve(Frame F, float* __restrict__ img) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= F.npix) return;
+  float r = 0.0f, g = 0.0f, b = 0.0f;
+  const float4* c = F.contrib + (size_t)k * F.spp;
+  for (uint32_t s = 0; s < F.spp; ++s) {
+    const float4 v = c[s];
+    if (v.w != 0.0f) {
+      r = __fadd_rn(r, v.x);
+      g = __fadd_rn(g, v.y);
+      b = __fadd_rn(b, v.z);
+    }
+  }
+  // reference: finalColor *= 2.0f * M_PI * (1.0f / float(spp)), scalar and products in double
+  const float inv = __fdiv_rn(1.0f, (float)F.spp);
+  const double s = (F.mode == 0) ? __dmul_rn(6.283185307179586, (double)inv) : (double)inv;
+  float* o = img + (size_t)(F.pixel0 + k) * 3;
+  o[0] = __double2float_rn(__dmul_rn((double)r, s));
+  o[1] = __double2float_rn(__dmul_rn((double)g, s));
+  o[2] = __double2float_rn(__dmul_rn((double)b, s));
+}
+
+struct Workspace {
+  size_t qbytes = 0, cam_px = 0, contrib_n = 0;
+  void* qbuf = nullptr;
+  void* cam = nullptr;
+  void* contrib = nullptr;
+  Ctrl* ctrl = nullptr;
+  Ctrl* host_ctrl = nullptr;
+};
+
+int ensure(void** p, size_t& have, size_t want, size_t elem) {
+  if (have >= want && *p) return SWR_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  have = 0;
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(want * elem, 256));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(SWR_ERR_ALLOC, std::string("CUDA: workspace allocation of ") +
+                                        std::to_string(want * elem) + " bytes failed");
+  }
+  have = want;
+  return SWR_OK;
+}
+
+}  // namespace
+
+// Per-scene workspace storage (kept behind an opaque pointer in the scene).
+struct RenderWorkspace : Workspace {};
+
+static RenderWorkspace* workspace_of(swr_scene* s);
+
+int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
+                float* samples_out, void* stream_, uint64_t* rays_out) {
+  if (!s || !cam || !o || !rgb_out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (o->width == 0 || o->height == 0 || o->spp == 0)
+    return set_error(SWR_ERR_INVALID, "swr: zero image size or samples");
+  if (o->max_depth == 0 || o->max_depth > 31)
+    return set_error(SWR_ERR_INVALID, "swr: max_depth must be 1..31");
+  if (o->mode > 1) return set_error(SWR_ERR_INVALID, "swr: unknown mode");
+  if (o->mode == 1 && o->rr_depth != 0 && !(o->rr_survive > 0.0f && o->rr_survive <= 1.0f))
+    return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+  if ((uint64_t)o->width * o->height >= (1ull << 32))
+    return set_error(SWR_ERR_INVALID, "swr: image too large");
+  if ((o->flags & SWR_RENDER_SAMPLES_OUT) && !samples_out)
+    return set_error(SWR_ERR_INVALID, "swr: SWR_RENDER_SAMPLES_OUT without a samples buffer");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  RenderWorkspace* ws = workspace_of(s);
+  if (!ws) return set_error(SWR_ERR_ALLOC, "swr: workspace");
+
+  const uint64_t npix_total = (uint64_t)o->width * o->height;
+  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
+  uint32_t cap = o->wave_size ? o->wave_size : (1u << 21);
+  cap = (uint32_t)std::min<uint64_t>(cap, px_per_chunk * o->spp);
+  cap = std::max<uint32_t>(32, (cap + 255u) & ~255u);
+  int rc;
+  const size_t qbytes = (size_t)cap * (4 * sizeof(float4) + sizeof(uint2)) * 2;
+  if ((rc = ensure(&ws->qbuf, ws->qbytes, qbytes, 1))) return rc;
+  if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
+  if ((rc = ensure(&ws->contrib, ws->contrib_n, px_per_chunk * o->spp, sizeof(float4)))) return rc;
+  if (!ws->ctrl) {
+    SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
+  }
+
+  Queue Q[2];
+  {
+    char* b = (char*)ws->qbuf;
+    for (int p = 0; p < 2; ++p) {
+      Q[p].o = (float4*)b; b += (size_t)cap * sizeof(float4);
+      Q[p].d = (float4*)b; b += (size_t)cap * sizeof(float4);
+      Q[p].c = (float4*)b; b += (size_t)cap * sizeof(float4);
+      Q[p].l = (float4*)b; b += (size_t)cap * sizeof(float4);
+      Q[p].hit = (uint2*)b; b += (size_t)cap * sizeof(uint2);
+    }
+  }
+
+  // output staging for host pointers
+  float* img = rgb_out;
+  float* img_dev = nullptr;
+  const bool host_img = is_host_pointer(rgb_out);
+  if (host_img) {
+    SWR_CUDA(cudaMallocAsync((void**)&img_dev, npix_total * 3 * sizeof(float), stream));
+    img = img_dev;
+  }
+  const bool want_samples = (o->flags & SWR_RENDER_SAMPLES_OUT) != 0;
+  const bool host_samples = want_samples && is_host_pointer(samples_out);
+
+  Frame F;
+  std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
+  std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
+  std::memcpy(F.org, cam->origin, sizeof(F.org));
+  F.W = o->width;
+  F.H = o->height;
+  F.spp = o->spp;
+  F.depth = o->max_depth;
+  F.mode = o->mode;
+  F.rr_depth = (o->mode == 1) ? o->rr_depth : 0;
+  F.rr_q = (o->mode == 1 && o->rr_depth) ? o->rr_survive : 1.0f;
+  F.seed = o->seed;
+  F.capacity = cap;
+  F.cam = (float4*)ws->cam;
+  F.contrib = (float4*)ws->contrib;
+
+  int block = o->block_size ? (int)o->block_size : 256;
+  if (block != 128 && block != 256 && block != 512) return set_error(SWR_ERR_INVALID, "swr: block_size must be 128, 256 or 512");
+  int trace_per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace, kTraceBlock, 0));
+  const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
+  const unsigned shade_grid = (cap + block - 1) / block;
+  uint64_t rays = 0;
+
+  for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
+    const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
+    F.pixel0 = (uint32_t)p0;
+    F.npix = np;
+    const uint64_t total = (uint64_t)np * o->spp;
+    Ctrl init;
+    std::memset(&init, 0, sizeof(init));
+    init.total = total;
+    init.inj_base[0] = 0;
+    init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, total);
+    init.injected = init.inj_n[0];
+    SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
+    *ws->host_ctrl = init;
+    SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    SWR_CUDA(cudaGetLastError());
+    uint64_t k = 0;
+    for (;;) {
+      const int kChunk = 8;
+      for (int c = 0; c < kChunk; ++c, ++k) {
+        const int p = (int)(k & 1);
+        switch (block) {
+          case 128: k_shade<128><<<shade_grid, 128, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+          case 512: k_shade<512><<<shade_grid, 512, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+          default: k_shade<256><<<shade_grid, 256, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+        }
+        k_trace<<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
+      }
+      SWR_CUDA(cudaGetLastError());
+      SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl, ws->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+      SWR_CUDA(cudaStreamSynchronize(stream));
+      const Ctrl& h = *ws->host_ctrl;
+      const int np_ = (int)(k & 1);
+      if (h.count[np_] == 0 && h.inj_n[np_] == 0 && h.injected == h.total) {
+        rays += h.rays;
+        break;
+      }
+    }
+    k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
+    SWR_CUDA(cudaGetLastError());
+    if (want_samples) {
+      const size_t bytes = (size_t)np * o->spp * sizeof(float4);
+      SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)p0 * o->spp * 4, F.contrib, bytes,
+                               host_samples ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream));
+    }
+  }
+  if (host_img) {
+    SWR_CUDA(cudaMemcpyAsync(rgb_out, img_dev, npix_total * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    SWR_CUDA(cudaFreeAsync(img_dev, stream));
+  }
+  if (host_img || host_samples) SWR_CUDA(cudaStreamSynchronize(stream));
+  if (rays_out) *rays_out = rays;
+  return SWR_OK;
+}
+
+static RenderWorkspace* workspace_of(swr_scene* s) {
+  if (!s->workspace) s->workspace = new RenderWorkspace();
+  return (RenderWorkspace*)s->workspace;
+}
+
+void free_workspace(swr_scene* s) {
+  RenderWorkspace* ws = (RenderWorkspace*)s->workspace;
+  if (!ws) return;
+  if (ws->qbuf) cudaFree(ws->qbuf);
+  if (ws->cam) cudaFree(ws->cam);
+  if (ws->contrib) cudaFree(ws->contrib);
+  if (ws->ctrl) cudaFree(ws->ctrl);
+  if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
+  delete ws;
+  s->workspace = nullptr;
+}
+
+}  // namespace swr
+
+extern "C" {
+
+int swr_render(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
+               float* samples_out, void* stream) {
+  return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, nullptr);
+}
+
+int swr_render_stats(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
+                     float* samples_out, void* stream, uint64_t* rays_traced) {
+  return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, rays_traced);
+}
+
+}  // extern "C"

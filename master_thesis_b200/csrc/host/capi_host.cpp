@@ -1,0 +1,173 @@
+// Host-side half of the C ABI: error reporting, the file surface, derived triangle data and
+// image output. No CUDA here.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+
+#include "../../../include/swr.h"
+#include "capi_common.h"
+#include "surface.h"
+
+namespace swr {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+}  // namespace swr
+
+using swr::set_error;
+
+struct swr_host_scene {
+  swr::HostScene s;
+  std::vector<swr_material> mats;
+  std::vector<uint32_t> obj_first_vertex;
+};
+
+extern "C" {
+
+const char* swr_last_error(void) { return swr::g_last_error.c_str(); }
+
+int swr_abi_version(void) { return SWR_ABI_VERSION; }
+
+int swr_host_scene_load(const char* scene_path, const char* basepath, swr_host_scene** out) {
+  if (!scene_path || !basepath || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  try {
+    std::unique_ptr<swr_host_scene> hs(new swr_host_scene());
+    hs->s = swr::load_scene_file(scene_path, basepath);
+    for (const auto& o : hs->s.objects) {
+      swr_material m;
+      for (int k = 0; k < 3; ++k) m.color[k] = o.mat.color[k];
+      m.diffuse_t = o.mat.diffuse_t;
+      m.reflect_t = o.mat.reflect_t;
+      m.transparent_t = o.mat.transparent_t;
+      m.refraction_index = o.mat.refraction_index;
+      m.light_source = o.mat.light ? 1u : 0u;
+      m.light_strength = o.mat.light_strength;
+      hs->mats.push_back(m);
+      hs->obj_first_vertex.push_back(o.first_vertex);
+    }
+    hs->obj_first_vertex.push_back((uint32_t)hs->s.vpos.size());
+    *out = hs.release();
+    return SWR_OK;
+  } catch (const swr::SurfaceError& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SWR_ERR_PARSE, std::string("swr: ") + e.what());
+  }
+}
+
+int swr_host_scene_desc(const swr_host_scene* hs, swr_scene_desc* d) {
+  if (!hs || !d) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  std::memset(d, 0, sizeof(*d));
+  d->num_objects = (uint32_t)hs->s.objects.size();
+  d->num_vertices = (uint32_t)hs->s.vpos.size();
+  d->num_triangles = (uint32_t)hs->s.num_tris();
+  d->vertex_pos = hs->s.vpos.empty() ? nullptr : hs->s.vpos[0].v;
+  d->vertex_normal = hs->s.vnrm.empty() ? nullptr : hs->s.vnrm[0].v;
+  d->tri_vertices = hs->s.tri.data();
+  d->tri_object = hs->s.tri_obj.data();
+  d->tri_rank = hs->s.tri_rank.data();
+  d->object_first_vertex = hs->obj_first_vertex.data();
+  d->materials = hs->mats.data();
+  d->tri_albedo = nullptr;
+  return SWR_OK;
+}
+
+int swr_host_scene_ranks_exact(const swr_host_scene* hs) { return hs && hs->s.ranks_exact ? 1 : 0; }
+
+void swr_host_scene_free(swr_host_scene* hs) { delete hs; }
+
+int swr_camera_load(const char* camera_path, uint32_t width, uint32_t height, uint32_t use_fov_key,
+                    swr_camera* out) {
+  if (!camera_path || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (width == 0 || height == 0) return set_error(SWR_ERR_INVALID, "swr: zero image size");
+  try {
+    swr::CameraParams c = swr::load_camera_file(camera_path);
+    swr::CameraFrame f = swr::camera_frame(c, width, height, use_fov_key != 0);
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) {
+        out->view_inv[i * 4 + j] = f.view_inv.m[i][j];
+        out->proj_inv[i * 4 + j] = f.proj_inv.m[i][j];
+      }
+    for (int k = 0; k < 3; ++k) out->origin[k] = f.origin[k];
+    out->reserved = 0.0f;
+    return SWR_OK;
+  } catch (const swr::SurfaceError& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SWR_ERR_PARSE, std::string("swr: ") + e.what());
+  }
+}
+
+int swr_renderer_load(const char* renderer_path, uint32_t* max_depth, uint32_t* spp) {
+  if (!renderer_path) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  try {
+    swr::RendererParams r = swr::load_renderer_file(renderer_path);
+    if (r.name != "PathTracer")
+      return set_error(SWR_ERR_UNSUPPORTED, "swr: renderer \"" + r.name + "\" is not provided");
+    if (max_depth) *max_depth = r.vision_jump_count;
+    if (spp) *spp = r.rays_per_pixel;
+    return SWR_OK;
+  } catch (const swr::SurfaceError& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SWR_ERR_PARSE, std::string("swr: ") + e.what());
+  }
+}
+
+int swr_scene_derive(const swr_scene_desc* d, float* tri_e0, float* tri_e1, float* tri_den,
+                     float* tri_box, float* obj_box) {
+  int rc = swr::validate_desc(d);
+  if (rc) return rc;
+  swr::Derived dv;
+  swr::derive(*d, dv);
+  const size_t nt = d->num_triangles, no = d->num_objects;
+  for (size_t t = 0; t < nt; ++t) {
+    for (int k = 0; k < 3; ++k) {
+      if (tri_e0) tri_e0[3 * t + k] = dv.e0[t][k];
+      if (tri_e1) tri_e1[3 * t + k] = dv.e1[t][k];
+      if (tri_box) {
+        tri_box[6 * t + k] = dv.tri_box[t].lo[k];
+        tri_box[6 * t + 3 + k] = dv.tri_box[t].hi[k];
+      }
+    }
+    if (tri_den)
+      for (int k = 0; k < 4; ++k) tri_den[4 * t + k] = dv.den[t][k];
+  }
+  if (obj_box)
+    for (size_t o = 0; o < no; ++o)
+      for (int k = 0; k < 3; ++k) {
+        obj_box[6 * o + k] = dv.obj_box[o].lo[k];
+        obj_box[6 * o + 3 + k] = dv.obj_box[o].hi[k];
+      }
+  return SWR_OK;
+}
+
+int swr_quantize_rgb8(const float* rgb, uint32_t width, uint32_t height, uint8_t* out) {
+  if (!rgb || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  const size_t n = (size_t)width * height * 3;
+  for (size_t i = 0; i < n; ++i) {
+    // std::clamp(c, 0, 1) then truncation of c * 255.0f to a byte (graphics_engine.cpp:90-95)
+    float c = rgb[i];
+    c = (c < 0.0f) ? 0.0f : ((1.0f < c) ? 1.0f : c);
+    out[i] = (uint8_t)(int)(c * 255.0f);
+  }
+  return SWR_OK;
+}
+
+int swr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height) {
+  if (!path || !rgb8) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  std::ofstream f(path, std::ios::out | std::ios::binary);
+  if (!f) return set_error(SWR_ERR_IO, std::string("swr: cannot write \"") + path + "\"");
+  f << "P6\n" << width << "\n" << height << "\n" << 255u << "\n";
+  f.write((const char*)rgb8, (std::streamsize)width * height * 3);
+  return f ? SWR_OK : set_error(SWR_ERR_IO, std::string("swr: write failed \"") + path + "\"");
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+// Exact reproduction of the reference's BVH topology, used only to know the order in which the
+// reference visits leaves (its closest-hit ties go to the first leaf in left-first DFS order).
+//
+// The reference (software_renderer/math/bounding_volume_hierachy.cpp:9-75) builds the tree by
+// repeatedly merging the pair of live nodes whose box centres are closest (squared float
+// distance, strict <, first pair in list-scan order on ties) and appending the parent at the end
+// of the list. That is O(n^2) per merge. This implementation makes the same choices in about
+// O(n^2) total by keeping, for every live node, its best later partner; it is checked against the
+// reference's own builder tree by tree in the tests.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "rmath.h"
+
+namespace swr {
+
+struct RefTree {
+  // node i < n is leaf i (element i); node n+k is the k-th merge. left/right are -1 for leaves.
+  std::vector<int32_t> left, right;
+  int32_t root = -1;
+};
+
+// Builds the tree over the given leaf boxes (in input order) and returns the element indices in
+// left-first DFS order. If tree is non-null the full topology is returned too.
+std::vector<uint32_t> ref_bvh_leaf_order(const std::vector<Box>& boxes, RefTree* tree = nullptr);
+
+}  // namespace swr

@@ -1,0 +1,33 @@
+// Host construction of the traversal BVH: binned-SAH binary tree, collapsed into the compressed
+// 8-wide node format of swr_bvh.cuh. This is an acceleration structure of this library only;
+// the reference's own (agglomerative) tree matters solely for tie order, see ref_bvh.h.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace swr {
+
+struct PrimBox {
+  float lo[3], hi[3];
+};
+
+struct WideBvhOptions {
+  uint32_t sah_bins = 32;
+  uint32_t max_leaf = 3;       // triangles per leaf child (1..3)
+  uint32_t threads = 0;        // 0 = hardware concurrency
+};
+
+struct WideBvh {
+  std::vector<uint32_t> words;     // 20 32-bit words per node (five float4)
+  std::vector<uint32_t> prim_order;  // triangle record slot -> primitive index
+  uint32_t num_nodes = 0;
+  uint32_t depth = 0;              // deepest node level (root = 1)
+  uint32_t binary_nodes = 0;
+  double sah_cost = 0.0;           // SAH cost of the binary tree (traversal 1, intersection 1)
+};
+
+// Boxes must already include whatever safety margin the traversal needs.
+WideBvh build_wide_bvh(const std::vector<PrimBox>& prims, const WideBvhOptions& opt);
+
+}  // namespace swr

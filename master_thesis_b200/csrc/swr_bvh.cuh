@@ -1,0 +1,202 @@
+// Compressed 8-wide BVH and the closest-hit traversal with the reference's hit semantics.
+//
+// Node record: 80 bytes = five float4, 16-byte aligned (every node touches exactly three 32-byte
+// sectors). Child boxes are quantised to 8 bits per plane on a per-node power-of-two grid
+// (after Ylitie, Karras, Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed
+// Wide BVHs", HPG 2017); the encoding details below are this project's own.
+//
+//   f4[0] = p.x p.y p.z | ex | ey<<8 | ez<<16 | imask<<24     grid origin, exponents, inner mask
+//   f4[1] = child_base | tri_base | meta[0..3] | meta[4..7]    meta = (count<<5)|offset for leaf
+//                                                               slots, 0 for inner/empty slots
+//   f4[2] = qlo_x[0..7] | qlo_y[0..7]
+//   f4[3] = qlo_z[0..7] | qhi_x[0..7]
+//   f4[4] = qhi_y[0..7] | qhi_z[0..7]
+//
+// Inner children of a node are stored contiguously from child_base in increasing slot order;
+// triangles of its leaf children contiguously from tri_base (at most 24 per node, at most 3 per
+// leaf). The builder places children so that slot s holds the child lying towards octant corner s;
+// a ray whose direction has sign bits `oct` visits slots in increasing (s ^ oct), near to far.
+//
+// Triangle record: 48 bytes = three float4:
+//   v0.x v0.y v0.z e0.x | e0.y e0.z e1.x e1.y | e1.z id rank obj
+// where e0 = v1 - v0, e1 = v2 - v0 exactly as the reference's Triangle computes them, id is the
+// global triangle id, rank its position in the reference's visit order (ties), obj its object.
+//
+// Hit rule (what makes the result bit-identical to Scene::traceRay, scene.cpp:22-56): the
+// reference tests every triangle whose own box and whose object's box pass its slab test, with
+// its Moller-Trumbore arithmetic, and keeps the smallest squared distance, the first in its
+// visit order on ties. Here candidates come from the wide BVH (boxes conservatively enlarged,
+// nodes farther than the current best times (1 + 2^-10) pruned); a candidate that would beat
+// the current best by (distance^2, rank) is accepted only if both reference slab tests pass.
+#pragma once
+
+#include "swr_exact.cuh"
+
+namespace swrx {
+
+constexpr int kNodeF4 = 5;
+constexpr int kTriF4 = 3;
+constexpr int kStackShared = 8;   // entries per thread kept in shared memory
+constexpr int kStackTotal = 64;   // maximum traversal stack depth (checked at build time)
+constexpr float kPruneSlack = 1.0f + 1.0f / 1024.0f;
+
+struct Hit {
+  uint32_t slot;   // index into the triangle records, 0xFFFFFFFF on a miss
+  uint32_t id;     // global triangle id
+  uint32_t rank;
+  uint32_t obj;
+  float t;
+  float d2;
+};
+
+struct TraceStats {
+  uint32_t nodes;
+  uint32_t tris;
+};
+
+// Stack of node groups; the first kStackShared entries live in `shared` with the given stride
+// (entry-major, thread-minor layout), the rest in thread-local memory.
+struct GroupStack {
+  uint2* shared;
+  int stride;
+  int sp;
+  uint2 local[kStackTotal - kStackShared];
+  SWR_HD void push(uint2 v) {
+    if (sp < kStackShared) shared[sp * stride] = v;
+    else local[sp - kStackShared] = v;
+    ++sp;
+  }
+  SWR_HD uint2 pop() {
+    --sp;
+    return (sp < kStackShared) ? shared[sp * stride] : local[sp - kStackShared];
+  }
+};
+
+SWR_HD float4 ldg4(const float4* p) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+
+// Closest hit of ray (o, d). obj_boxes/tri_boxes hold the reference's own boxes (lo.xyz, hi.xyz)
+// per object and per triangle record. Returns false on a miss.
+template <bool kStats>
+SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                          const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
+                          f3 o, f3 d, uint2* stack_shared, int stack_stride, Hit& hit,
+                          TraceStats* stats) {
+  const f3 inv = vinv(d);  // exact reciprocal, used by the reference slab tests
+  // traversal reciprocal: zero components replaced by a tiny value of the same sign
+  const float tiny = 1e-20f;
+  const float dx = (fabsf(d.x) < tiny) ? copysignf(tiny, d.x) : d.x;
+  const float dy = (fabsf(d.y) < tiny) ? copysignf(tiny, d.y) : d.y;
+  const float dz = (fabsf(d.z) < tiny) ? copysignf(tiny, d.z) : d.z;
+  const float idx = 1.0f / dx, idy = 1.0f / dy, idz = 1.0f / dz;
+  const uint32_t oct = (idx < 0.0f ? 1u : 0u) | (idy < 0.0f ? 2u : 0u) | (idz < 0.0f ? 4u : 0u);
+
+  hit.slot = 0xFFFFFFFFu;
+  hit.id = 0xFFFFFFFFu;
+  hit.rank = 0xFFFFFFFFu;
+  hit.obj = 0xFFFFFFFFu;
+  hit.t = INFINITY;
+  hit.d2 = INFINITY;
+  float tprune = INFINITY;
+
+  GroupStack st;
+  st.shared = stack_shared;
+  st.stride = stack_stride;
+  st.sp = 0;
+
+  // node group: x = child_base, y = hits (bits 24..31, in visit order) | imask (bits 0..7)
+  uint2 ng = make_uint2(0u, (1u << (24 + oct)) | 1u);  // the root, as inner slot 0
+  uint2 tg = make_uint2(0u, 0u);                        // triangle group: base, hit bits 0..23
+  for (;;) {
+    if (ng.y & 0xFF000000u) {
+      const uint32_t k = (uint32_t)ffs(ng.y >> 24) - 1u;
+      ng.y &= ~(1u << (24 + k));
+      const uint32_t slot = k ^ oct;
+      const uint32_t child = ng.x + (uint32_t)popc(ng.y & ((1u << slot) - 1u) & 0xFFu);
+      if (ng.y & 0xFF000000u) st.push(ng);
+      if (kStats) stats->nodes++;
+
+      const float4* np = nodes + (size_t)child * kNodeF4;
+      const float4 n0 = ldg4(np + 0), n1 = ldg4(np + 1), n2 = ldg4(np + 2);
+      const float4 n3 = ldg4(np + 3), n4 = ldg4(np + 4);
+      const uint32_t hdr = f2bits(n0.w);
+      const float ex = bits2f((hdr & 0xFFu) << 23);
+      const float ey = bits2f(((hdr >> 8) & 0xFFu) << 23);
+      const float ez = bits2f(((hdr >> 16) & 0xFFu) << 23);
+      const uint32_t imask = hdr >> 24;
+      const float ax = ex * idx, ay = ey * idy, az = ez * idz;
+      const float bx = (n0.x - o.x) * idx, by = (n0.y - o.y) * idy, bz = (n0.z - o.z) * idz;
+      // near/far plane bytes by direction sign
+      const uint32_t lox0 = f2bits(n2.x), lox1 = f2bits(n2.y), loy0 = f2bits(n2.z), loy1 = f2bits(n2.w);
+      const uint32_t loz0 = f2bits(n3.x), loz1 = f2bits(n3.y), hix0 = f2bits(n3.z), hix1 = f2bits(n3.w);
+      const uint32_t hiy0 = f2bits(n4.x), hiy1 = f2bits(n4.y), hiz0 = f2bits(n4.z), hiz1 = f2bits(n4.w);
+      const uint32_t nx0 = (oct & 1u) ? hix0 : lox0, nx1 = (oct & 1u) ? hix1 : lox1;
+      const uint32_t fx0 = (oct & 1u) ? lox0 : hix0, fx1 = (oct & 1u) ? lox1 : hix1;
+      const uint32_t ny0 = (oct & 2u) ? hiy0 : loy0, ny1 = (oct & 2u) ? hiy1 : loy1;
+      const uint32_t fy0 = (oct & 2u) ? loy0 : hiy0, fy1 = (oct & 2u) ? loy1 : hiy1;
+      const uint32_t nz0 = (oct & 4u) ? hiz0 : loz0, nz1 = (oct & 4u) ? hiz1 : loz1;
+      const uint32_t fz0 = (oct & 4u) ? loz0 : hiz0, fz1 = (oct & 4u) ? loz1 : hiz1;
+      const uint32_t meta0 = f2bits(n1.z), meta1 = f2bits(n1.w);
+      uint32_t inner = 0, trih = 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int sh = (i & 3) * 8;
+        const uint32_t m = ((i < 4 ? meta0 : meta1) >> sh) & 0xFFu;
+        const float qnx = (float)(((i < 4 ? nx0 : nx1) >> sh) & 0xFFu);
+        const float qny = (float)(((i < 4 ? ny0 : ny1) >> sh) & 0xFFu);
+        const float qnz = (float)(((i < 4 ? nz0 : nz1) >> sh) & 0xFFu);
+        const float qfx = (float)(((i < 4 ? fx0 : fx1) >> sh) & 0xFFu);
+        const float qfy = (float)(((i < 4 ? fy0 : fy1) >> sh) & 0xFFu);
+        const float qfz = (float)(((i < 4 ? fz0 : fz1) >> sh) & 0xFFu);
+        const float tnx = fmaf(qnx, ax, bx), tny = fmaf(qny, ay, by), tnz = fmaf(qnz, az, bz);
+        const float tfx = fmaf(qfx, ax, bx), tfy = fmaf(qfy, ay, by), tfz = fmaf(qfz, az, bz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tprune));
+        const bool is_inner = (imask >> i) & 1u;
+        if (tn <= tf && (is_inner || m != 0u)) {
+          if (is_inner) inner |= 1u << (i ^ (int)oct);
+          else trih |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+        }
+      }
+      ng = make_uint2(f2bits(n1.x), (inner << 24) | imask);
+      tg = make_uint2(f2bits(n1.y), trih);
+    }
+
+    while (tg.y) {
+      const uint32_t j = (uint32_t)ffs(tg.y) - 1u;
+      tg.y &= tg.y - 1u;
+      const uint32_t s = tg.x + j;
+      if (kStats) stats->tris++;
+      const float4* tp = tris + (size_t)s * kTriF4;
+      const float4 a = ldg4(tp + 0), b = ldg4(tp + 1), c = ldg4(tp + 2);
+      float t, d2;
+      if (!ref_intersect(o, d, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y), mk(b.z, b.w, c.x), t, d2))
+        continue;
+      const uint32_t rank = f2bits(c.z);
+      if (!(d2 < hit.d2 || (d2 == hit.d2 && rank < hit.rank))) continue;
+      const uint32_t obj = f2bits(c.w);
+      if (!ref_slab(tri_boxes + (size_t)s * 6, tri_boxes + (size_t)s * 6 + 3, o, inv)) continue;
+      if (!ref_slab(obj_boxes + (size_t)obj * 6, obj_boxes + (size_t)obj * 6 + 3, o, inv)) continue;
+      hit.slot = s;
+      hit.id = f2bits(c.y);
+      hit.rank = rank;
+      hit.obj = obj;
+      hit.t = t;
+      hit.d2 = d2;
+      tprune = t * kPruneSlack;
+    }
+
+    if (!(ng.y & 0xFF000000u)) {
+      if (st.sp == 0) break;
+      ng = st.pop();
+    }
+  }
+  return hit.slot != 0xFFFFFFFFu;
+}
+
+}  // namespace swrx
