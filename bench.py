@@ -1,0 +1,333 @@
+"""Benchmark of the path tracer on the terrain workload (the plain method at scale):
+1024x1024-cell heightfield terrain (2,097,152 triangles, seeded 6-octave fBm heights in [0, 0.2])
+in 64x64 OBJ tiles, 64 icospheres of subdivision 4 (radii log-uniform 0.01-0.1), 4 emissive quads;
+1920x1080 pixels, 64 samples per pixel, depth 8, reference semantics (so the reference's CPU path
+renders the identical files with the identical estimator).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+
+One step = one full image (all pixels x spp samples). `value` is Msamples/s with the scene
+resident in device memory; `e2e` renders through the C ABI into a pinned host buffer (the
+library's device->host copy of the image inside the timed region). With N>1 every rank renders
+its own image of the same scene with its own seed (independent units, weak scaling); no
+collective is on the data path. The reference arm (--impl reference) times the reference's own
+CPU implementation (oracle/_ref/ref_bench: the unmodified SoftwareRenderer sources) on this
+machine's cores for a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: scene parameters, image, spp, depth
+    "c2": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=64,
+               depth=8, seed=2024),
+    "c1": dict(kind="cornell", W=256, H=256, spp=16, depth=5, seed=1),
+}
+METRIC = "Msamples/s (camera paths per second)"
+
+
+def make_scene(cfg, root):
+    from master_thesis_b200 import scenes
+    if cfg["kind"] == "terrain":
+        return scenes.terrain(cfg["seed"], root, cells=cfg["cells"], tile=cfg["tile"], spheres=cfg["spheres"],
+                              sphere_subdiv=cfg["subdiv"], lights=cfg["lights"])
+    return scenes.cornell(cfg["seed"], root)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        loaded = [x for x in sm if x > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """ncu DRAM bytes per launch of the bounce traversal kernel and the algorithmic bytes of the same
+    launch, from the committed summary of one capture (profiles/k_trace_terrain.json)."""
+    p = os.path.join(ROOT, "profiles", "k_trace_terrain.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+def cpu_reference(cfg, files, threads, budget_s, impl_bin):
+    """Times the reference's own PathTracer (unmodified sources) on a bounded pixel sample."""
+    W, H, spp, depth = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
+    fast = ["fast"] if cfg["kind"] == "terrain" else []
+
+    def run(pixels):
+        out = subprocess.run([impl_bin, files["basepath"], files["scene"], files["camera"], str(W), str(H), str(spp),
+                              str(depth), str(threads), str(pixels)] + fast, capture_output=True, text=True,
+                             timeout=1800)
+        if out.returncode != 0:
+            raise RuntimeError("ref_bench failed: " + out.stderr[-2000:])
+        return json.loads(out.stdout.strip().splitlines()[-1])
+
+    probe = run(max(threads, 8))
+    rate = probe["samples"] / max(probe["render_s"], 1e-6)
+    pixels = int(max(threads * 2, min(W * H, budget_s * rate / spp)))
+    res = run(pixels)
+    res["load_s_probe"] = probe["load_s"]
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scene-dir", default=None)
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    W, H, spp, depth = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
+    workload = ("terrain %dx%d cells (%d tiles) + %d icospheres (subdiv %d) + %d emissive quads, %dx%d, %d spp, "
+                "depth %d, reference semantics" % (cfg["cells"], cfg["cells"], (cfg["cells"] // cfg["tile"]) ** 2,
+                                                  cfg["spheres"], cfg["subdiv"], cfg["lights"], W, H, spp, depth)
+                if cfg["kind"] == "terrain" else
+                "cornell 36 tris, %dx%d, %d spp, depth %d, reference semantics" % (W, H, spp, depth))
+    tmp = args.scene_dir or tempfile.mkdtemp(prefix="swr_bench_")
+    files_path = os.path.join(tmp, "files.json")
+    if os.path.exists(files_path):
+        files = json.load(open(files_path))
+    else:
+        files = make_scene(cfg, tmp)
+        json.dump(files, open(files_path, "w"))
+    nproc = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import refdump
+        if not os.path.exists(refdump.REF_BENCH):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench was not built"}))
+            return
+        res = cpu_reference(cfg, files, nproc, args.cpu_budget * max(1, args.steps // 5), refdump.REF_BENCH)
+        v = res["msamples_per_s"]
+        sample = "%d of %d pixels (every k-th), %d spp, depth %d, %d threads" % (res["pixels"], W * H, spp, depth, nproc)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": W * H * spp / (v * 1e6) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene files)", "config": {"workload": workload},
+            "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": nproc, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_load_s": res["load_s"]}))
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        import datetime
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import master_thesis_b200 as swr
+
+    t0 = time.time()
+    sd = swr.load_scene(files["scene"], files["basepath"])
+    t1 = time.time()
+    scene = swr.Scene(sd)
+    torch.cuda.synchronize()
+    t2 = time.time()
+    stats = scene.stats()
+    cam = swr.load_camera(files["camera"], W, H)
+    seed = 1000 + rank
+    out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def render(o, **kw):
+        return scene.render(cam, W, H, spp, depth, seed=seed, out=o, stream=stream, return_profile=True, **kw)
+
+    for _ in range(max(args.warmup, 3)):
+        render(out)
+    torch.cuda.synchronize()
+    # traffic model: node visits and triangle tests of the bounce traversal (separate, untimed run)
+    _, cprof = render(out, count=True)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    barrier()
+    step_ms, profs = [], []
+    for _ in range(args.steps):
+        flush.fill_(1.0)  # evict L2 between steps (256 MB > 126 MB L2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, pr = render(out, profile=True)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        profs.append(pr)
+    barrier()
+    # end to end: the same call with a pinned host output buffer
+    host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
+    e2e_ms, e2e_prof = [], []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, pr = render(host)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+        e2e_prof.append(pr)
+    barrier()
+    clk = clocks.stop()
+
+    tot = torch.tensor([sum(step_ms), sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_ms, total_e2e_ms = float(tot[0]), float(tot[1])
+    samples = W * H * spp * world * args.steps
+    value = samples / (total_ms / 1e3) / 1e6
+    e2e_value = samples / (total_e2e_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel (bounce traversal): algorithmic bytes per launch =
+    # rays * (32 B ray in + 8 B hit out) + node visits * 80 B + triangle tests * 48 B
+    launches = sum(p["trace_launches"] for p in profs)
+    trace_ms = sum(p["trace_ms"] for p in profs)
+    rays_per_step = profs[-1]["bounce_rays"]
+    bytes_per_step = rays_per_step * 40 + cprof["node_visits"] * 80 + cprof["tri_tests"] * 48
+    per_launch_bytes = bytes_per_step * args.steps / max(launches, 1)
+    per_launch_s = trace_ms / 1e3 / max(launches, 1)
+    achieved = per_launch_bytes / per_launch_s / 1e9
+    peak, peak_kind = measured_peaks()
+    tp = profile_traffic()
+    traffic = None
+    if tp and tp.get("workload") == args.config:
+        # DRAM bytes per algorithmic byte of the captured launch, applied to this launch's bytes
+        traffic = per_launch_bytes * tp["dram_bytes"] / tp["algorithmic_bytes"]
+    mrays = sum(p["rays"] for p in profs) / (sum(step_ms) / 1e3) / 1e6
+    launches_total = sum(p["launches"] for p in profs)
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import refdump
+            if os.path.exists(refdump.REF_BENCH):
+                try:
+                    r = cpu_reference(cfg, files, nproc, args.cpu_budget, refdump.REF_BENCH)
+                    cpu = {"value": r["msamples_per_s"], "unit": "Msamples/s", "cores": nproc, "kind": "reference",
+                           "sample": "%d of %d pixels (every k-th), %d spp, depth %d; reference load+build %.1f s"
+                                     % (r["pixels"], W * H, spp, depth, r["load_s"])}
+                except Exception as ex:  # the baseline is reported, never required
+                    cpu = {"value": None, "unit": "Msamples/s", "cores": nproc, "kind": "reference",
+                           "sample": "failed: %s" % str(ex)[:200]}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
+            "config": {"workload": workload, "triangles": int(sd.num_triangles), "objects": int(sd.num_objects),
+                       "pixels": W * H, "spp": spp, "depth": depth, "l2": "flushed between steps (256 MB write)",
+                       "parallelism": "independent images per GPU" if world > 1 else "single GPU",
+                       "bvh_nodes": stats["nodes"], "bvh_depth": stats["depth"]},
+            "e2e": {"value": e2e_value, "unit": "Msamples/s",
+                    "h2d_bytes_per_step": int(e2e_prof[-1]["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(e2e_prof[-1]["d2h_bytes"])},
+            "mrays_per_s": mrays,
+            "rays_per_sample": profs[-1]["rays"] / (W * H * spp),
+            "roofline": {"bound": "hbm", "kernel": "k_trace (bounce traversal)", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": per_launch_bytes,
+                         "node_visits_per_ray": cprof["node_visits"] / max(cprof["bounce_rays"], 1),
+                         "tri_tests_per_ray": cprof["tri_tests"] / max(cprof["bounce_rays"], 1)},
+            "kernel_ms_per_step": {k: sum(p[k] for p in profs) / args.steps for k in
+                                   ("trace_ms", "shade_ms", "camera_ms", "resolve_ms")},
+            "gpu_launches": int(launches_total),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "setup_s": {"load": t1 - t0, "build_upload": t2 - t1},
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -181,9 +181,27 @@ int swr_trace_closest_stats(swr_scene* scene, const float* ray_o, const float* r
 int swr_render(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts, float* rgb_out,
                float* samples_out, void* stream);
 
-/* As swr_render, also returning the number of rays traced (camera prefix + all bounces). */
-int swr_render_stats(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
-                     float* rgb_out, float* samples_out, void* stream, uint64_t* rays_traced);
+#define SWR_RENDER_PROFILE 2u       /* time each kernel kind with CUDA events (see swr_render_profile) */
+#define SWR_RENDER_COUNT 4u         /* count wide-BVH node visits and triangle tests of the bounce
+                                       traversal kernel (slower; for the traffic model only) */
+
+/* Per-call instrumentation of swr_render_profiled. Times are device milliseconds summed over the
+ * launches of each kernel kind (with SWR_RENDER_PROFILE). */
+typedef struct swr_render_profile {
+  uint64_t rays;            /* rays traced: camera prefix + all bounces */
+  uint64_t bounce_rays;     /* rays traced by the bounce traversal kernel */
+  uint64_t node_visits;     /* with SWR_RENDER_COUNT: nodes fetched by the bounce traversal */
+  uint64_t tri_tests;       /* with SWR_RENDER_COUNT: triangle records tested by it */
+  uint64_t iterations;      /* shade/trace rounds */
+  uint64_t launches;        /* kernels launched by the call */
+  uint64_t trace_launches;  /* launches of the bounce traversal kernel */
+  uint64_t h2d_bytes, d2h_bytes;  /* explicit host<->device copies made by the call */
+  double trace_ms, shade_ms, camera_ms, resolve_ms;
+} swr_render_profile;
+
+/* As swr_render, filling *prof (which may be NULL). */
+int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
+                        float* rgb_out, float* samples_out, void* stream, swr_render_profile* prof);
 
 /* Reference-style 8-bit quantisation (graphics_engine.cpp:90-95: clamp to [0,1], *255, truncate)
  * and P6 PPM writer (graphics_engine.cpp:32-40). Host memory. */

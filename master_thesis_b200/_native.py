@@ -23,6 +23,8 @@ SWR_ERR_UNSUPPORTED = 7
 MODE_REFERENCE = 0
 MODE_PHYSICAL = 1
 RENDER_SAMPLES_OUT = 1
+RENDER_PROFILE = 2
+RENDER_COUNT = 4
 
 
 class SwrError(RuntimeError):
@@ -66,6 +68,15 @@ class RenderOpts(ctypes.Structure):
                 ("flags", ctypes.c_uint32)]
 
 
+class RenderProfile(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ["rays", "bounce_rays", "node_visits", "tri_tests", "iterations",
+                                               "launches", "trace_launches", "h2d_bytes", "d2h_bytes"]] + \
+               [(n, ctypes.c_double) for n in ["trace_ms", "shade_ms", "camera_ms", "resolve_ms"]]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 P = ctypes.c_void_p
 U32 = ctypes.c_uint32
 U64 = ctypes.c_uint64
@@ -89,8 +100,8 @@ SIGNATURES = {
     "swr_trace_closest": (I, [P, P, P, U64, P, P]),
     "swr_trace_closest_stats": (I, [P, P, P, U64, P, P, P]),
     "swr_render": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P]),
-    "swr_render_stats": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P,
-                             ctypes.POINTER(U64)]),
+    "swr_render_profiled": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P,
+                                ctypes.POINTER(RenderProfile)]),
     "swr_quantize_rgb8": (I, [P, U32, U32, P]),
     "swr_write_ppm": (I, [ctypes.c_char_p, P, U32, U32]),
 }

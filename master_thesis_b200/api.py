@@ -172,18 +172,20 @@ class Scene:
 
     def render(self, cam, width, height, spp, depth, seed=0, mode=N.MODE_REFERENCE, rr_depth=0,
                rr_survive=1.0, wave_size=0, block_size=0, out=None, samples=None, stream=None,
-               return_rays=False):
-        """Renders an image (height, width, 3) float32 into `out` (torch cuda tensor or numpy)."""
-        o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size,
-                         block_size, N.RENDER_SAMPLES_OUT if samples is not None else 0)
+               profile=False, count=False, return_profile=False):
+        """Renders an image (height, width, 3) float32 into `out` (torch cuda tensor or numpy array;
+        a numpy array makes the library stage the result through the device)."""
+        flags = (N.RENDER_SAMPLES_OUT if samples is not None else 0) | (N.RENDER_PROFILE if profile else 0) | \
+            (N.RENDER_COUNT if count else 0)
+        o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size, block_size, flags)
         if out is None:
             import torch
             out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
         s = _stream_handle(stream)
-        rays = ctypes.c_uint64(0)
-        check(N.lib.swr_render_stats(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(out), ptr(samples),
-                                     s, ctypes.byref(rays)))
-        return (out, rays.value) if return_rays else out
+        prof = N.RenderProfile()
+        check(N.lib.swr_render_profiled(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(out), ptr(samples),
+                                        s, ctypes.byref(prof)))
+        return (out, prof.as_dict()) if return_profile else out
 
 
 def quantize_rgb8(img):

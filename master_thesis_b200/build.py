@@ -19,12 +19,13 @@ LIB = os.path.join(HERE, "lib")
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
+HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function",
+              "-I/usr/local/cuda/include"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
                      "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 HOST_SRC = ["host/surface.cpp", "host/ref_bvh.cpp", "host/wide_bvh.cpp", "host/derive.cpp",
-            "host/capi_host.cpp"]
+            "host/capi_host.cpp", "host/scene_pack.cpp"]
 CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu"]
 CLI_SRC = "cli/swr_main.cpp"
 

@@ -41,7 +41,9 @@ struct Ctrl {
   unsigned long long injected;
   unsigned long long total;
   unsigned long long rays;
-  unsigned long long pad1;
+  unsigned long long bounce_rays;
+  unsigned long long nodes;
+  unsigned long long tris;
 };
 
 struct Queue {
@@ -195,6 +197,7 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+template <bool kStats>
 __global__ void __launch_bounds__(kTraceBlock)
     k_trace(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, Queue q, int parity) {
   __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
@@ -210,7 +213,9 @@ __global__ void __launch_bounds__(kTraceBlock)
     ctrl->injected += m;
     ctrl->count[parity] = 0u;
     ctrl->rays += n;
+    ctrl->bounce_rays += n;
   }
+  swrx::TraceStats st{0, 0};
   for (;;) {
     unsigned base = 0;
     if (lane_id() == 0) base = atomicAdd(&ctrl->cursor[qp], 32u);
@@ -220,9 +225,20 @@ __global__ void __launch_bounds__(kTraceBlock)
     if (i < n) {
       const float4 o = q.o[i], d = q.d[i];
       swrx::Hit h;
-      swrx::trace_closest<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, mk(o.x, o.y, o.z),
-                                 mk(d.x, d.y, d.z), stack + threadIdx.x, kTraceBlock, h, nullptr);
+      swrx::trace_closest<kStats>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, mk(o.x, o.y, o.z),
+                                  mk(d.x, d.y, d.z), stack + threadIdx.x, kTraceBlock, h, &st);
       q.hit[i] = make_uint2(h.slot, __float_as_uint(h.t));
+    }
+  }
+  if (kStats) {
+    unsigned long long nv = st.nodes, tv = st.tris;
+    for (int off = 16; off > 0; off >>= 1) {
+      nv += __shfl_down_sync(0xffffffffu, nv, off);
+      tv += __shfl_down_sync(0xffffffffu, tv, off);
+    }
+    if (lane_id() == 0) {
+      atomicAdd(&ctrl->nodes, nv);
+      atomicAdd(&ctrl->tris, tv);
     }
   }
 }
@@ -280,8 +296,57 @@ struct RenderWorkspace : Workspace {};
 
 static RenderWorkspace* workspace_of(swr_scene* s);
 
+namespace {
+
+// Records CUDA events around kernel launches of one kind and sums their durations.
+struct KernelTimer {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  size_t used = 0;
+  double ms[4] = {0, 0, 0, 0};
+  bool on = false;
+  cudaError_t begin(cudaStream_t st, int k) {
+    if (!on) return cudaSuccess;
+    if (used + 2 > ev.size()) {
+      for (int i = 0; i < 2; ++i) {
+        cudaEvent_t e;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        ev.push_back(e);
+      }
+      kind.push_back(0);
+    }
+    kind[used / 2] = k;
+    return cudaEventRecord(ev[used], st);
+  }
+  cudaError_t end(cudaStream_t st) {
+    if (!on) return cudaSuccess;
+    cudaError_t r = cudaEventRecord(ev[used + 1], st);
+    used += 2;
+    return r;
+  }
+  // call after a stream synchronize: folds the recorded pairs into the totals
+  cudaError_t collect() {
+    for (size_t i = 0; i < used; i += 2) {
+      float t = 0.0f;
+      cudaError_t r = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      if (r != cudaSuccess) return r;
+      ms[kind[i / 2]] += t;
+    }
+    used = 0;
+    return cudaSuccess;
+  }
+  ~KernelTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+enum { kTimeTrace = 0, kTimeShade = 1, kTimeCamera = 2, kTimeResolve = 3 };
+
+}  // namespace
+
 int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
-                float* samples_out, void* stream_, uint64_t* rays_out) {
+                float* samples_out, void* stream_, swr_render_profile* prof) {
   if (!s || !cam || !o || !rgb_out) return set_error(SWR_ERR_INVALID, "swr: null argument");
   if (o->width == 0 || o->height == 0 || o->spp == 0)
     return set_error(SWR_ERR_INVALID, "swr: zero image size or samples");
@@ -294,10 +359,18 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     return set_error(SWR_ERR_INVALID, "swr: image too large");
   if ((o->flags & SWR_RENDER_SAMPLES_OUT) && !samples_out)
     return set_error(SWR_ERR_INVALID, "swr: SWR_RENDER_SAMPLES_OUT without a samples buffer");
+  int block = o->block_size ? (int)o->block_size : 256;
+  if (block != 128 && block != 256 && block != 512)
+    return set_error(SWR_ERR_INVALID, "swr: block_size must be 128, 256 or 512");
   cudaStream_t stream = (cudaStream_t)stream_;
   SWR_CUDA(cudaSetDevice(s->device));
   RenderWorkspace* ws = workspace_of(s);
   if (!ws) return set_error(SWR_ERR_ALLOC, "swr: workspace");
+  swr_render_profile P;
+  std::memset(&P, 0, sizeof(P));
+  KernelTimer timer;
+  timer.on = (o->flags & SWR_RENDER_PROFILE) != 0;
+  const bool count = (o->flags & SWR_RENDER_COUNT) != 0;
 
   const uint64_t npix_total = (uint64_t)o->width * o->height;
   const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
@@ -353,13 +426,13 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   F.cam = (float4*)ws->cam;
   F.contrib = (float4*)ws->contrib;
 
-  int block = o->block_size ? (int)o->block_size : 256;
-  if (block != 128 && block != 256 && block != 512) return set_error(SWR_ERR_INVALID, "swr: block_size must be 128, 256 or 512");
   int trace_per_sm = 0;
-  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace, kTraceBlock, 0));
+  if (count)
+    SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace<true>, kTraceBlock, 0));
+  else
+    SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace<false>, kTraceBlock, 0));
   const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
   const unsigned shade_grid = (cap + block - 1) / block;
-  uint64_t rays = 0;
 
   for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
     const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
@@ -375,44 +448,77 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
     *ws->host_ctrl = init;
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+    P.h2d_bytes += sizeof(Ctrl);
+    SWR_CUDA(timer.begin(stream, kTimeCamera));
     k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    SWR_CUDA(timer.end(stream));
     SWR_CUDA(cudaGetLastError());
+    P.launches++;
     uint64_t k = 0;
+    // every path ends within max_depth rounds of its injection and each round injects up to the
+    // queue capacity, so this many rounds always suffice; more means a logic error
+    const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
     for (;;) {
+      if (k > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
       const int kChunk = 8;
       for (int c = 0; c < kChunk; ++c, ++k) {
         const int p = (int)(k & 1);
+        SWR_CUDA(timer.begin(stream, kTimeShade));
         switch (block) {
           case 128: k_shade<128><<<shade_grid, 128, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
           case 512: k_shade<512><<<shade_grid, 512, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
           default: k_shade<256><<<shade_grid, 256, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
         }
-        k_trace<<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
+        SWR_CUDA(timer.end(stream));
+        SWR_CUDA(timer.begin(stream, kTimeTrace));
+        if (count)
+          k_trace<true><<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
+        else
+          k_trace<false><<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
+        SWR_CUDA(timer.end(stream));
+        P.launches += 2;
+        P.trace_launches++;
       }
       SWR_CUDA(cudaGetLastError());
       SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl, ws->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+      P.d2h_bytes += sizeof(Ctrl);
       SWR_CUDA(cudaStreamSynchronize(stream));
+      SWR_CUDA(timer.collect());
       const Ctrl& h = *ws->host_ctrl;
       const int np_ = (int)(k & 1);
       if (h.count[np_] == 0 && h.inj_n[np_] == 0 && h.injected == h.total) {
-        rays += h.rays;
+        P.rays += h.rays;
+        P.bounce_rays += h.bounce_rays;
+        P.node_visits += h.nodes;
+        P.tri_tests += h.tris;
+        P.iterations += k;
         break;
       }
     }
+    SWR_CUDA(timer.begin(stream, kTimeResolve));
     k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
+    SWR_CUDA(timer.end(stream));
     SWR_CUDA(cudaGetLastError());
+    P.launches++;
     if (want_samples) {
       const size_t bytes = (size_t)np * o->spp * sizeof(float4);
       SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)p0 * o->spp * 4, F.contrib, bytes,
                                host_samples ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream));
+      if (host_samples) P.d2h_bytes += bytes;
     }
   }
   if (host_img) {
     SWR_CUDA(cudaMemcpyAsync(rgb_out, img_dev, npix_total * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream));
     SWR_CUDA(cudaFreeAsync(img_dev, stream));
+    P.d2h_bytes += npix_total * 3 * sizeof(float);
   }
-  if (host_img || host_samples) SWR_CUDA(cudaStreamSynchronize(stream));
-  if (rays_out) *rays_out = rays;
+  if (host_img || host_samples || timer.on) SWR_CUDA(cudaStreamSynchronize(stream));
+  if (timer.on) SWR_CUDA(timer.collect());
+  P.trace_ms = timer.ms[kTimeTrace];
+  P.shade_ms = timer.ms[kTimeShade];
+  P.camera_ms = timer.ms[kTimeCamera];
+  P.resolve_ms = timer.ms[kTimeResolve];
+  if (prof) *prof = P;
   return SWR_OK;
 }
 
@@ -442,9 +548,9 @@ int swr_render(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, fl
   return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, nullptr);
 }
 
-int swr_render_stats(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
-                     float* samples_out, void* stream, uint64_t* rays_traced) {
-  return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, rays_traced);
+int swr_render_profiled(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
+                        float* samples_out, void* stream, swr_render_profile* prof) {
+  return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, prof);
 }
 
 }  // extern "C"

@@ -6,7 +6,7 @@
 #include <memory>
 
 #include "../host/capi_common.h"
-#include "../host/wide_bvh.h"
+#include "../host/scene_pack.h"
 #include "swr_internal.cuh"
 
 namespace swr {
@@ -37,12 +37,6 @@ int upload(void** dst, const std::vector<T>& v) {
   }
   if (!v.empty()) SWR_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
   return SWR_OK;
-}
-
-inline float ubits(uint32_t u) {
-  float f;
-  std::memcpy(&f, &u, 4);
-  return f;
 }
 
 constexpr int kTraceBlock = 128;
@@ -150,86 +144,11 @@ int swr_sync(void* stream) {
 int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_scene** out) {
   if (!out) return set_error(SWR_ERR_INVALID, "swr: null output handle");
   *out = nullptr;
-  int rc = swr::validate_desc(d);
-  if (rc) return rc;
   try {
-    swr::Derived dv;
-    swr::derive(*d, dv);
-    const uint32_t nt = d->num_triangles, no = d->num_objects;
-    // traversal boxes: the reference boxes, enlarged by a margin tied to the scene's scale so
-    // that rounding in the quantised slab tests can never lose a box the reference's test hits
-    float slo[3] = {INFINITY, INFINITY, INFINITY}, shi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t t = 0; t < nt; ++t)
-      for (int k = 0; k < 3; ++k) {
-        slo[k] = std::min(slo[k], dv.tri_box[t].lo[k]);
-        shi[k] = std::max(shi[k], dv.tri_box[t].hi[k]);
-      }
-    float ext = 0.0f, mabs = 0.0f;
-    for (int k = 0; k < 3; ++k) {
-      ext = std::max(ext, shi[k] - slo[k]);
-      mabs = std::max(mabs, std::max(std::fabs(slo[k]), std::fabs(shi[k])));
-    }
-    if (!std::isfinite(ext) || !std::isfinite(mabs))
-      return set_error(SWR_ERR_INVALID, "swr: scene has non-finite vertex coordinates");
-    const float eps = ext * (1.0f / 65536.0f) + mabs * (1.0f / 1048576.0f) + 1e-30f;
-    std::vector<swr::PrimBox> prims(nt);
-    for (uint32_t t = 0; t < nt; ++t)
-      for (int k = 0; k < 3; ++k) {
-        prims[t].lo[k] = dv.tri_box[t].lo[k] - eps;
-        prims[t].hi[k] = dv.tri_box[t].hi[k] + eps;
-      }
-    swr::WideBvhOptions wo;
-    if (opts) {
-      if (opts->sah_bins) wo.sah_bins = opts->sah_bins;
-      if (opts->max_leaf) wo.max_leaf = opts->max_leaf;
-      wo.threads = opts->threads;
-    }
-    if (wo.max_leaf > 3) return set_error(SWR_ERR_INVALID, "swr: max_leaf must be 1..3");
-    swr::WideBvh bvh = swr::build_wide_bvh(prims, wo);
-    if (bvh.depth + 1 > (uint32_t)swrx::kStackTotal)
-      return set_error(SWR_ERR_UNSUPPORTED, "swr: BVH deeper than the traversal stack");
-
-    const uint32_t ns = (uint32_t)bvh.prim_order.size();
-    std::vector<float4> tris((size_t)ns * 3), shade((size_t)ns * 4);
-    std::vector<float> tboxes((size_t)ns * 6), albedo((size_t)ns * 3), oboxes((size_t)no * 6);
-    std::vector<uint32_t> slot_of(nt);
+    swr::PackedScene pk;
+    int rc = swr::pack_scene(d, opts, pk);
+    if (rc) return rc;
     std::unique_ptr<swr_scene> s(new swr_scene());
-    s->slot_to_id.resize(ns);
-    for (uint32_t sl = 0; sl < ns; ++sl) {
-      const uint32_t t = bvh.prim_order[sl];
-      slot_of[t] = sl;
-      s->slot_to_id[sl] = t;
-      const uint32_t obj = d->tri_object[t];
-      const uint32_t rank = d->tri_rank ? d->tri_rank[t] : t;
-      const swr::V3 &v0 = dv.v0[t], &e0 = dv.e0[t], &e1 = dv.e1[t];
-      tris[3 * (size_t)sl + 0] = make_float4(v0[0], v0[1], v0[2], e0[0]);
-      tris[3 * (size_t)sl + 1] = make_float4(e0[1], e0[2], e1[0], e1[1]);
-      tris[3 * (size_t)sl + 2] = make_float4(e1[2], swr::ubits(t), swr::ubits(rank), swr::ubits(obj));
-      shade[4 * (size_t)sl] = make_float4(dv.den[t][0], dv.den[t][1], dv.den[t][2], dv.den[t][3]);
-      for (int c = 0; c < 3; ++c) {
-        const uint32_t vi = d->tri_vertices[3 * (size_t)t + c];
-        const float* nv = d->vertex_normal + 3 * (size_t)vi;
-        shade[4 * (size_t)sl + 1 + c] = make_float4(nv[0], nv[1], nv[2], 0.0f);
-      }
-      for (int k = 0; k < 3; ++k) {
-        tboxes[6 * (size_t)sl + k] = dv.tri_box[t].lo[k];
-        tboxes[6 * (size_t)sl + 3 + k] = dv.tri_box[t].hi[k];
-        albedo[3 * (size_t)sl + k] = d->tri_albedo ? d->tri_albedo[3 * (size_t)t + k] : d->materials[obj].color[k];
-      }
-    }
-    std::vector<float4> mats((size_t)no * 3);
-    for (uint32_t o = 0; o < no; ++o) {
-      const swr_material& m = d->materials[o];
-      for (int k = 0; k < 3; ++k) {
-        oboxes[6 * (size_t)o + k] = dv.obj_box[o].lo[k];
-        oboxes[6 * (size_t)o + 3 + k] = dv.obj_box[o].hi[k];
-      }
-      mats[3 * (size_t)o + 0] = make_float4(m.color[0], m.color[1], m.color[2], m.diffuse_t);
-      mats[3 * (size_t)o + 1] = make_float4(m.reflect_t, m.transparent_t, m.refraction_index,
-                                            swr::ubits(m.light_source ? 1u : 0u));
-      mats[3 * (size_t)o + 2] = make_float4(m.color[0] * m.light_strength, m.color[1] * m.light_strength,
-                                            m.color[2] * m.light_strength, m.light_strength);
-    }
     SWR_CUDA(cudaGetDevice(&s->device));
     SWR_CUDA(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
     struct Guard {
@@ -238,14 +157,14 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
         if (p) swr_scene_destroy(p);
       }
     } guard{s.get()};
-    if ((rc = swr::upload(&s->d_nodes, bvh.words))) return rc;
-    if ((rc = swr::upload(&s->d_tris, tris))) return rc;
-    if ((rc = swr::upload(&s->d_shade, shade))) return rc;
-    if ((rc = swr::upload(&s->d_tri_boxes, tboxes))) return rc;
-    if ((rc = swr::upload(&s->d_obj_boxes, oboxes))) return rc;
-    if ((rc = swr::upload(&s->d_mats, mats))) return rc;
-    if ((rc = swr::upload(&s->d_albedo, albedo))) return rc;
-    if ((rc = swr::upload(&s->d_slot_of, slot_of))) return rc;
+    if ((rc = swr::upload(&s->d_nodes, pk.nodes))) return rc;
+    if ((rc = swr::upload(&s->d_tris, pk.tris))) return rc;
+    if ((rc = swr::upload(&s->d_shade, pk.shade))) return rc;
+    if ((rc = swr::upload(&s->d_tri_boxes, pk.tri_boxes))) return rc;
+    if ((rc = swr::upload(&s->d_obj_boxes, pk.obj_boxes))) return rc;
+    if ((rc = swr::upload(&s->d_mats, pk.mats))) return rc;
+    if ((rc = swr::upload(&s->d_albedo, pk.albedo))) return rc;
+    if ((rc = swr::upload(&s->d_slot_of, pk.slot_of))) return rc;
     s->scratch_bytes = 256;
     SWR_CUDA(cudaMalloc(&s->d_scratch, s->scratch_bytes));
     SWR_CUDA(cudaMemset(s->d_scratch, 0, s->scratch_bytes));
@@ -258,13 +177,14 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
     ds.mats = (const float4*)s->d_mats;
     ds.albedo = (const float*)s->d_albedo;
     ds.slot_of = (const uint32_t*)s->d_slot_of;
-    ds.num_nodes = bvh.num_nodes;
-    ds.num_slots = ns;
-    ds.num_objects = no;
-    ds.num_tris = nt;
-    s->depth = bvh.depth;
-    s->node_bytes = (uint64_t)bvh.num_nodes * 80;
-    s->tri_bytes = (uint64_t)ns * 48;
+    ds.num_nodes = pk.num_nodes;
+    ds.num_slots = (uint32_t)pk.slot_to_id.size();
+    ds.num_objects = d->num_objects;
+    ds.num_tris = d->num_triangles;
+    s->depth = pk.depth;
+    s->node_bytes = (uint64_t)pk.num_nodes * 80;
+    s->tri_bytes = (uint64_t)ds.num_slots * 48;
+    s->slot_to_id = std::move(pk.slot_to_id);
     guard.p = nullptr;
     *out = s.release();
     return SWR_OK;

@@ -1,0 +1,30 @@
+// Host assembly of the device scene records: the wide BVH over conservatively enlarged
+// reference boxes, triangle records in leaf order, shading records, boxes and materials.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../../include/swr.h"
+
+namespace swr {
+
+struct PackedScene {
+  std::vector<uint32_t> nodes;    // 20 words per wide node
+  std::vector<float4> tris;       // 3 per slot: v0|e0|e1|id rank obj
+  std::vector<float4> shade;      // 4 per slot: (d00 d01 d11 denom) (n0) (n1) (n2)
+  std::vector<float> tri_boxes;   // 6 per slot
+  std::vector<float> obj_boxes;   // 6 per object
+  std::vector<float4> mats;       // 3 per object
+  std::vector<float> albedo;      // 3 per slot
+  std::vector<uint32_t> slot_of;  // triangle id -> slot
+  std::vector<uint32_t> slot_to_id;
+  uint32_t num_nodes = 0, depth = 0;
+};
+
+// Validates and packs; returns SWR_OK or an error code (message in swr_last_error).
+int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene& out);
+
+}  // namespace swr

@@ -26,6 +26,11 @@
 #define M_PI 3.14159265358979323846 /* the same double as glibc's M_PI */
 #endif
 
+/* exported for known-answer tests of the generator */
+void swo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  swo_philox4x32_10(ctr, key, out);
+}
+
 typedef struct {
   float x, y, z;
 } v3f;

@@ -1,0 +1,89 @@
+"""CPU build of the kernels' traversal and shading code (tests/native/twin.cpp) against the oracle
+and the reference's golden outputs: checks the wide-BVH construction, the quantised traversal
+with its pruning, and the shading arithmetic without a GPU."""
+import numpy as np
+import pytest
+
+import master_thesis_b200 as swr
+from master_thesis_b200 import scenes
+from helpers import (GOLDEN_CASES, Twin, golden, golden_camera, golden_scene, ref_pixel_from_samples,
+                     rays_uniform)
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_twin_hits_match_reference_golden(name):
+    g = golden(name)
+    tw = Twin(golden_scene(g))
+    tri, d2, _ = tw.trace(g["ray_o"], g["ray_d"])
+    assert np.array_equal(tri, g["hit_id"])
+    assert np.array_equal(d2.view(np.uint32), g["hit_d2"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("max_leaf", [1, 3])
+def test_twin_hits_match_oracle_random_rays(name, max_leaf):
+    g = golden(name)
+    sd = golden_scene(g)
+    tw = Twin(sd, max_leaf=max_leaf)
+    osc = O.OracleScene.from_scene_data(sd)
+    ro, rd = rays_uniform(20000, sd.vpos.min(0) - 0.3, sd.vpos.max(0) + 0.3, seed=11)
+    tri, d2, t = tw.trace(ro, rd)
+    otri, od2, ot = osc.trace(ro, rd)
+    assert np.array_equal(tri, otri)
+    assert np.array_equal(d2.view(np.uint32), od2.view(np.uint32))
+    assert np.array_equal(t.view(np.uint32), ot.view(np.uint32))
+
+
+def test_twin_axis_aligned_and_degenerate_rays():
+    """Rays with zero direction components, rays starting on box faces and through shared edges
+    (exact ties between the two triangles of a quad)."""
+    g = golden("ref_cornell_box_with_blocks")
+    sd = golden_scene(g)
+    tw = Twin(sd)
+    osc = O.OracleScene.from_scene_data(sd)
+    rng = np.random.default_rng(3)
+    n = 6000
+    ro = np.zeros((n, 4), np.float32)
+    rd = np.zeros((n, 4), np.float32)
+    ro[:, :3] = rng.uniform(-1.1, 1.1, (n, 3)).astype(np.float32)
+    # snap some origins to the walls' planes and some coordinates to 0
+    ro[:1000, 0] = np.float32(1.0)
+    ro[1000:2000, 1] = np.float32(-1.0)
+    ro[2000:3000, 2] = 0.0
+    axes = rng.integers(0, 3, n)
+    rd[np.arange(n), axes] = rng.choice([-1.0, 1.0, -0.0], n)
+    # diagonal rays through the quads' shared edges
+    rd[3000:4000, :3] = np.float32([-1.0, 1.0, 1.0]) / np.float32(np.sqrt(3.0))
+    rd[4000:5000, :3] = np.float32([-1.0, -1.0, 0.0])
+    rd[5000:, :3] = rng.normal(size=(1000, 3)).astype(np.float32)
+    rd[:, :3] /= np.maximum(np.linalg.norm(rd[:, :3], axis=1, keepdims=True), 1e-30)
+    tri, d2, _ = tw.trace(ro, rd)
+    otri, od2, _ = osc.trace(ro, rd)
+    assert np.array_equal(tri, otri)
+    assert np.array_equal(d2.view(np.uint32), od2.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_twin_reference_radiance_matches_golden(name):
+    g = golden(name)
+    tw = Twin(golden_scene(g))
+    W, H, spp, depth, seed = [int(x) for x in g["params"]]
+    ps = tw.render(golden_camera(g), W, H, spp, depth, seed)
+    assert np.array_equal(ps.view(np.uint32), g["per_sample"].view(np.uint32))
+    assert np.array_equal(ref_pixel_from_samples(ps, spp).view(np.uint32), g["per_pixel"].view(np.uint32))
+
+
+def test_twin_physical_mode_matches_fp64_oracle(tmp_path):
+    s = scenes.cornell(3, str(tmp_path))
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    tw = Twin(sd)
+    osc = O.OracleScene.from_scene_data(sd)
+    W, H = 24, 18
+    cam = swr.load_camera(s["camera"], W, H, use_fov_key=True)
+    vi, pi, org = swr.camera_arrays(cam)
+    ps = tw.render(cam, W, H, 32, 5, 77, mode=1, rr_depth=3, rr_q=0.8)
+    pp64, _ = O.render_physical64(osc, O.camera(vi, pi, org), W, H, 32, 5, 77, rr_depth=3, rr_q=0.8)
+    m = ps[..., :3].astype(np.float64).mean(1)
+    # same paths, float vs double arithmetic: agreement to float rounding
+    assert np.max(np.abs(m - pp64) / (np.abs(pp64) + 1e-3)) < 1e-4
