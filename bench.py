@@ -35,6 +35,9 @@ CONFIGS = {
     "c2": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=64,
                depth=8, seed=2024),
     "c1": dict(kind="cornell", W=256, H=256, spp=16, depth=5, seed=1),
+    # the terrain scene at a reduced image size, for profiler captures of single kernel launches
+    "c2s": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=16,
+                depth=8, seed=2024),
 }
 METRIC = "Msamples/s (camera paths per second)"
 
