@@ -311,7 +311,8 @@ def main():
                        "bvh_nodes": stats["nodes"], "bvh_depth": stats["depth"]},
             "e2e": {"value": e2e_value, "unit": "Msamples/s",
                     "h2d_bytes_per_step": int(e2e_prof[-1]["h2d_bytes"]),
-                    "d2h_bytes_per_step": int(e2e_prof[-1]["d2h_bytes"])},
+                    "d2h_bytes_per_step": int(e2e_prof[-1]["d2h_bytes"]),
+                    "step_ms": {"min": min(e2e_ms), "median": statistics.median(e2e_ms), "max": max(e2e_ms)}},
             "mrays_per_s": mrays,
             "rays_per_sample": profs[-1]["rays"] / (W * H * spp),
             "roofline": {"bound": "hbm", "kernel": "k_trace (bounce traversal)", "achieved": achieved, "peak": peak,

@@ -81,7 +81,8 @@ typedef struct swr_build_opts {
   uint32_t sah_bins;       /* 0 = 32 */
   uint32_t max_leaf;       /* triangles per leaf, 1..3; 0 = 3 */
   uint32_t threads;        /* host build threads, 0 = all */
-  uint32_t reserved;
+  uint32_t leaf_cost_pct;  /* SAH cost of a triangle test relative to a wide-node visit, in
+                              percent (1..400); 0 = 30 */
 } swr_build_opts;
 
 /* Camera as GraphicsEngine::render derives it (graphics_engine.cpp:42-46): inverse view and
@@ -101,9 +102,13 @@ typedef struct swr_render_opts {
   uint32_t mode;           /* SWR_MODE_* */
   uint32_t rr_depth;       /* physical mode: Russian roulette at path vertices >= rr_depth (0=off) */
   float rr_survive;        /* physical mode: survival probability, (0, 1] */
-  uint32_t wave_size;      /* paths in flight, 0 = automatic */
+  uint32_t wave_size;      /* paths in flight, 0 = 2^23 (capped by the samples of a chunk) */
   uint32_t block_size;     /* threads per block of the shading kernel, 0 = automatic */
   uint32_t flags;          /* SWR_RENDER_* */
+  uint32_t refill;         /* bounce traversal: idle lanes (1..32) that trigger a refill, 0 = 8 */
+  uint32_t trace_blocks;   /* bounce traversal: resident blocks per SM targeted by the register
+                              budget, one of 0 (compiler's choice), 8, 10, 12 */
+  uint32_t reserved;
 } swr_render_opts;
 
 #define SWR_RENDER_SAMPLES_OUT 1u   /* write per-sample radiance to the samples buffer */
@@ -184,6 +189,10 @@ int swr_render(swr_scene* scene, const swr_camera* cam, const swr_render_opts* o
 #define SWR_RENDER_PROFILE 2u       /* time each kernel kind with CUDA events (see swr_render_profile) */
 #define SWR_RENDER_COUNT 4u         /* count wide-BVH node visits and triangle tests of the bounce
                                        traversal kernel (slower; for the traffic model only) */
+#define SWR_RENDER_STATIC_FETCH 8u  /* bounce traversal takes rays 32 at a time per warp and runs
+                                       them to completion, instead of refilling idle lanes */
+#define SWR_RENDER_POSTPONE 16u     /* bounce traversal postpones triangle tests while few lanes of
+                                       a warp have any (keeps warps in one phase) */
 
 /* Per-call instrumentation of swr_render_profiled. Times are device milliseconds summed over the
  * launches of each kernel kind (with SWR_RENDER_PROFILE). */

@@ -25,6 +25,8 @@ MODE_PHYSICAL = 1
 RENDER_SAMPLES_OUT = 1
 RENDER_PROFILE = 2
 RENDER_COUNT = 4
+RENDER_STATIC_FETCH = 8
+RENDER_POSTPONE = 16
 
 
 class SwrError(RuntimeError):
@@ -51,7 +53,7 @@ class SceneDesc(ctypes.Structure):
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("sah_bins", ctypes.c_uint32), ("max_leaf", ctypes.c_uint32),
-                ("threads", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("threads", ctypes.c_uint32), ("leaf_cost_pct", ctypes.c_uint32)]
 
 
 class Camera(ctypes.Structure):
@@ -65,7 +67,8 @@ class RenderOpts(ctypes.Structure):
                 ("seed", ctypes.c_uint64), ("mode", ctypes.c_uint32),
                 ("rr_depth", ctypes.c_uint32), ("rr_survive", ctypes.c_float),
                 ("wave_size", ctypes.c_uint32), ("block_size", ctypes.c_uint32),
-                ("flags", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("trace_blocks", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class RenderProfile(ctypes.Structure):

@@ -125,10 +125,10 @@ def _stream_handle(stream):
 class Scene:
     """Device scene (wide BVH + triangle records) built from SceneData."""
 
-    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0):
+    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0):
         self.data = data
         d = data.desc()
-        o = N.BuildOpts(sah_bins, max_leaf, threads, 0)
+        o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct)
         self._h = ctypes.c_void_p()
         check(N.lib.swr_scene_create(ctypes.byref(d), ctypes.byref(o), ctypes.byref(self._h)))
 
@@ -172,12 +172,14 @@ class Scene:
 
     def render(self, cam, width, height, spp, depth, seed=0, mode=N.MODE_REFERENCE, rr_depth=0,
                rr_survive=1.0, wave_size=0, block_size=0, out=None, samples=None, stream=None,
-               profile=False, count=False, return_profile=False):
+               profile=False, count=False, return_profile=False, static_fetch=False, refill=0,
+               trace_blocks=0):
         """Renders an image (height, width, 3) float32 into `out` (torch cuda tensor or numpy array;
         a numpy array makes the library stage the result through the device)."""
         flags = (N.RENDER_SAMPLES_OUT if samples is not None else 0) | (N.RENDER_PROFILE if profile else 0) | \
-            (N.RENDER_COUNT if count else 0)
-        o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size, block_size, flags)
+            (N.RENDER_COUNT if count else 0) | (N.RENDER_STATIC_FETCH if static_fetch else 0)
+        o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size, block_size, flags,
+                         refill, trace_blocks, 0)
         if out is None:
             import torch
             out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")

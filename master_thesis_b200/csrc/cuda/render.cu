@@ -63,6 +63,7 @@ struct Frame {
   uint32_t pixel0;   // first pixel of the chunk
   uint32_t npix;     // pixels in the chunk
   uint32_t capacity;
+  uint32_t refill;   // idle lanes that trigger a refill in the bounce traversal
   float4* cam;       // [npix*2] per-pixel first hit: (o, t) (d, slot | i << 27)
   float4* contrib;   // [npix*spp] per-sample radiance + flag
 };
@@ -243,6 +244,73 @@ __global__ void __launch_bounds__(kTraceBlock)
   }
 }
 
+// Persistent traversal with per-lane refill: each lane keeps its own ray's traversal state;
+// when at least F.refill lanes of the warp have finished, the warp takes that many new rays from
+// the queue with one atomic and the idle lanes start them. This keeps lanes busy while the
+// slowest ray of a batch is still walking the tree.
+// kMinBlocks > 0 caps the register budget so that many blocks fit on one SM.
+template <bool kStats, int kMinBlocks, bool kPostpone>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
+    k_trace_dyn(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, Queue q, int parity) {
+  __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
+  const int qp = parity ^ 1;
+  const unsigned n = ctrl->count[qp];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long rem = ctrl->total - ctrl->injected;
+    const unsigned long long room = (unsigned long long)F.capacity - n;
+    const unsigned long long m = rem < room ? rem : room;
+    ctrl->inj_base[qp] = ctrl->injected;
+    ctrl->inj_n[qp] = (unsigned)m;
+    ctrl->injected += m;
+    ctrl->count[parity] = 0u;
+    ctrl->rays += n;
+    ctrl->bounce_rays += n;
+  }
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  swrx::TraceStats st{0, 0};
+  swrx::Traversal tr;
+  bool active = false, exhausted = false;
+  unsigned ray = 0;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(&ctrl->cursor[qp], (unsigned)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) exhausted = true;
+      if (!active) {
+        const unsigned j = base + __popc(idle & lt);
+        if (j < n) {
+          const float4 o = q.o[j], d = q.d[j];
+          tr.init(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), stack + threadIdx.x, kTraceBlock);
+          ray = j;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active && tr.template step<kStats, kPostpone>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, &st)) {
+      q.hit[ray] = make_uint2(tr.hit.slot, __float_as_uint(tr.hit.t));
+      active = false;
+    }
+  }
+  if (kStats) {
+    unsigned long long nv = st.nodes, tv = st.tris;
+    for (int off = 16; off > 0; off >>= 1) {
+      nv += __shfl_down_sync(0xffffffffu, nv, off);
+      tv += __shfl_down_sync(0xffffffffu, tv, off);
+    }
+    if (lane == 0) {
+      atomicAdd(&ctrl->nodes, nv);
+      atomicAdd(&ctrl->tris, tv);
+    }
+  }
+}
+
 __global__ void k_resolve(Frame F, float* __restrict__ img) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= F.npix) return;
@@ -266,10 +334,11 @@ __global__ void k_resolve(Frame F, float* __restrict__ img) {
 }
 
 struct Workspace {
-  size_t qbytes = 0, cam_px = 0, contrib_n = 0;
+  size_t qbytes = 0, cam_px = 0, contrib_n = 0, stage_n = 0;
   void* qbuf = nullptr;
   void* cam = nullptr;
   void* contrib = nullptr;
+  void* stage = nullptr;  // device image for callers that pass a host output buffer
   Ctrl* ctrl = nullptr;
   Ctrl* host_ctrl = nullptr;
 };
@@ -374,7 +443,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
 
   const uint64_t npix_total = (uint64_t)o->width * o->height;
   const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
-  uint32_t cap = o->wave_size ? o->wave_size : (1u << 21);
+  uint32_t cap = o->wave_size ? o->wave_size : (1u << 23);
   cap = (uint32_t)std::min<uint64_t>(cap, px_per_chunk * o->spp);
   cap = std::max<uint32_t>(32, (cap + 255u) & ~255u);
   int rc;
@@ -404,7 +473,8 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   float* img_dev = nullptr;
   const bool host_img = is_host_pointer(rgb_out);
   if (host_img) {
-    SWR_CUDA(cudaMallocAsync((void**)&img_dev, npix_total * 3 * sizeof(float), stream));
+    if ((rc = ensure(&ws->stage, ws->stage_n, npix_total * 3, sizeof(float)))) return rc;
+    img_dev = (float*)ws->stage;
     img = img_dev;
   }
   const bool want_samples = (o->flags & SWR_RENDER_SAMPLES_OUT) != 0;
@@ -426,11 +496,26 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   F.cam = (float4*)ws->cam;
   F.contrib = (float4*)ws->contrib;
 
+  using TraceKernel = void (*)(DevScene, Frame, Ctrl*, Queue, int);
+  const bool static_fetch = (o->flags & SWR_RENDER_STATIC_FETCH) != 0;
+  TraceKernel trace_kernel;
+  const bool postpone = (o->flags & SWR_RENDER_POSTPONE) != 0;
+  switch (o->trace_blocks) {
+    case 0:
+      trace_kernel = postpone ? (count ? k_trace_dyn<true, 0, true> : k_trace_dyn<false, 0, true>)
+                              : (count ? k_trace_dyn<true, 0, false> : k_trace_dyn<false, 0, false>);
+      break;
+    case 10:
+      trace_kernel = postpone ? (count ? k_trace_dyn<true, 10, true> : k_trace_dyn<false, 10, true>)
+                              : (count ? k_trace_dyn<true, 10, false> : k_trace_dyn<false, 10, false>);
+      break;
+    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0 or 10");
+  }
+  if (static_fetch) trace_kernel = count ? k_trace<true> : k_trace<false>;
+  if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  F.refill = o->refill ? o->refill : 8;
   int trace_per_sm = 0;
-  if (count)
-    SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace<true>, kTraceBlock, 0));
-  else
-    SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace<false>, kTraceBlock, 0));
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, trace_kernel, kTraceBlock, 0));
   const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
   const unsigned shade_grid = (cap + block - 1) / block;
 
@@ -471,10 +556,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
         }
         SWR_CUDA(timer.end(stream));
         SWR_CUDA(timer.begin(stream, kTimeTrace));
-        if (count)
-          k_trace<true><<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
-        else
-          k_trace<false><<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
+        trace_kernel<<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
         SWR_CUDA(timer.end(stream));
         P.launches += 2;
         P.trace_launches++;
@@ -509,7 +591,6 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   }
   if (host_img) {
     SWR_CUDA(cudaMemcpyAsync(rgb_out, img_dev, npix_total * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream));
-    SWR_CUDA(cudaFreeAsync(img_dev, stream));
     P.d2h_bytes += npix_total * 3 * sizeof(float);
   }
   if (host_img || host_samples || timer.on) SWR_CUDA(cudaStreamSynchronize(stream));
@@ -533,6 +614,7 @@ void free_workspace(swr_scene* s) {
   if (ws->qbuf) cudaFree(ws->qbuf);
   if (ws->cam) cudaFree(ws->cam);
   if (ws->contrib) cudaFree(ws->contrib);
+  if (ws->stage) cudaFree(ws->stage);
   if (ws->ctrl) cudaFree(ws->ctrl);
   if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
   delete ws;

@@ -54,10 +54,14 @@ int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene&
     if (opts->sah_bins) wo.sah_bins = opts->sah_bins;
     if (opts->max_leaf) wo.max_leaf = opts->max_leaf;
     wo.threads = opts->threads;
+    if (opts->leaf_cost_pct > 400)
+      return set_error(SWR_ERR_INVALID, "swr: leaf_cost_pct must be 0..400");
+    if (opts->leaf_cost_pct) wo.prim_cost = opts->leaf_cost_pct / 100.0;
   }
   if (wo.max_leaf > 3) return set_error(SWR_ERR_INVALID, "swr: max_leaf must be 1..3");
   WideBvh bvh = build_wide_bvh(prims, wo);
-  if (bvh.depth + 1 > kMaxStack)
+  // a traversal keeps at most one node group and one postponed triangle group per level
+  if (2 * bvh.depth + 2 > kMaxStack)
     return set_error(SWR_ERR_UNSUPPORTED, "swr: BVH deeper than the traversal stack");
 
   const uint32_t ns = (uint32_t)bvh.prim_order.size();

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <functional>
+#include <limits>
 #include <stdexcept>
 #include <thread>
 
@@ -197,6 +199,60 @@ WideBvh build_wide_bvh(const std::vector<PrimBox>& prims, const WideBvhOptions& 
     out.sah_cost = c;
   }
 
+  // SAH-optimal collapse into 8-wide nodes (the dynamic program of Ylitie, Karras, Laine 2017,
+  // section 4.1). For every binary node n: cost[n][i] = cheapest way to represent n's subtree by
+  // at most i children of a wide node (i = 1..8); as one child it is either a leaf (at most
+  // max_leaf triangles, cost area * count * kPrim) or a wide node (area * kNode + the cheapest
+  // split of its subtree into at most 8 children). dist[n][j] = cheapest split of n's two binary
+  // children into j children in total.
+  const double kNode = 1.0, kPrim = opt.prim_cost;
+  const double INF = std::numeric_limits<double>::infinity();
+  std::vector<double> cost((size_t)nb * 9, INF), dist((size_t)nb * 9, INF);
+  std::vector<uint8_t> dist_k((size_t)nb * 9, 0), from_fewer((size_t)nb * 9, 0), as_leaf(nb, 0);
+  for (int64_t n = (int64_t)nb - 1; n >= 0; --n) {
+    const BNode& b = bn[n];
+    const double a = (double)area(b.lo, b.hi);
+    double* C = &cost[(size_t)n * 9];
+    double* D = &dist[(size_t)n * 9];
+    const double leaf = tri_count[n] <= opt.max_leaf ? a * (double)tri_count[n] * kPrim : INF;
+    double inner = INF;
+    if (!b.count) {
+      const double* CL = &cost[(size_t)b.left * 9];
+      const double* CR = &cost[(size_t)b.right * 9];
+      for (int j = 2; j <= 8; ++j)
+        for (int k = 1; k < j; ++k) {
+          const double v = CL[k] + CR[j - k];
+          if (v < D[j]) {
+            D[j] = v;
+            dist_k[(size_t)n * 9 + j] = (uint8_t)k;
+          }
+        }
+      inner = a * kNode + D[8];
+    }
+    as_leaf[n] = leaf <= inner ? 1 : 0;
+    C[1] = std::min(leaf, inner);
+    for (int i = 2; i <= 8; ++i) {
+      if (C[i - 1] <= D[i]) {
+        C[i] = C[i - 1];
+        from_fewer[(size_t)n * 9 + i] = 1;
+      } else {
+        C[i] = D[i];
+      }
+    }
+  }
+  // children of binary node n when it is spent on at most i wide-node slots
+  std::vector<uint32_t> ch;
+  std::function<void(uint32_t, int)> spread = [&](uint32_t n, int i) {
+    while (i > 1 && from_fewer[(size_t)n * 9 + i]) --i;
+    if (i == 1) {
+      ch.push_back(n);
+      return;
+    }
+    const int k = dist_k[(size_t)n * 9 + i];
+    spread(bn[n].left, k);
+    spread(bn[n].right, i - k);
+  };
+
   struct Task {
     uint32_t bnode, wide, depth;
   };
@@ -208,28 +264,13 @@ WideBvh build_wide_bvh(const std::vector<PrimBox>& prims, const WideBvhOptions& 
     Task tk = q.front();
     q.pop_front();
     out.depth = std::max(out.depth, tk.depth);
-    std::vector<uint32_t> ch;
-    if (bn[tk.bnode].count) ch.push_back(tk.bnode);
-    else {
-      ch.push_back(bn[tk.bnode].left);
-      ch.push_back(bn[tk.bnode].right);
-    }
-    while (ch.size() < 8) {
-      int pick = -1;
-      float best = -1.0f;
-      for (size_t i = 0; i < ch.size(); ++i) {
-        const BNode& c = bn[ch[i]];
-        if (c.count) continue;
-        const float a = area(c.lo, c.hi);
-        if (a > best) {
-          best = a;
-          pick = (int)i;
-        }
-      }
-      if (pick < 0) break;
-      const uint32_t e = ch[pick];
-      ch[pick] = bn[e].left;
-      ch.push_back(bn[e].right);
+    ch.clear();
+    if (bn[tk.bnode].count || as_leaf[tk.bnode]) {
+      ch.push_back(tk.bnode);  // a scene small enough to be one leaf: a root with one leaf child
+    } else {
+      const int k = dist_k[(size_t)tk.bnode * 9 + 8];
+      spread(bn[tk.bnode].left, k);
+      spread(bn[tk.bnode].right, 8 - k);
     }
     // slot assignment: child towards octant corner s goes to slot s
     float ulo[3] = {INFINITY, INFINITY, INFINITY}, uhi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -307,7 +348,7 @@ WideBvh build_wide_bvh(const std::vector<PrimBox>& prims, const WideBvhOptions& 
         qlo[k][s] = (uint8_t)std::max(0.0, std::min(255.0, lo));
         qhi[k][s] = (uint8_t)std::max(0.0, std::min(255.0, hi));
       }
-      if (tri_count[c] <= opt.max_leaf) {
+      if (as_leaf[c] || (c == tk.bnode)) {
         gather.clear();
         std::vector<uint32_t> st{c};
         while (!st.empty()) {

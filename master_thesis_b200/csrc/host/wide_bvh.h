@@ -16,6 +16,7 @@ struct WideBvhOptions {
   uint32_t sah_bins = 32;
   uint32_t max_leaf = 3;       // triangles per leaf child (1..3)
   uint32_t threads = 0;        // 0 = hardware concurrency
+  double prim_cost = 0.3;      // SAH cost of a triangle test relative to a wide-node visit
 };
 
 struct WideBvh {

@@ -54,8 +54,11 @@ struct TraceStats {
   uint32_t tris;
 };
 
-// Stack of node groups; the first kStackShared entries live in `shared` with the given stride
-// (entry-major, thread-minor layout), the rest in thread-local memory.
+// Stack of groups; the first kStackShared entries live in `shared` with the given stride
+// (entry-major, thread-minor layout), the rest in thread-local memory. Node groups and postponed
+// triangle groups share it; triangle groups carry kTriGroup in .x.
+constexpr uint32_t kTriGroup = 0x80000000u;
+
 struct GroupStack {
   uint2* shared;
   int stride;
@@ -80,40 +83,78 @@ SWR_HD float4 ldg4(const float4* p) {
 #endif
 }
 
-// Closest hit of ray (o, d). obj_boxes/tri_boxes hold the reference's own boxes (lo.xyz, hi.xyz)
-// per object and per triangle record. Returns false on a miss.
-template <bool kStats>
-SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __restrict__ tris,
-                          const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
-                          f3 o, f3 d, uint2* stack_shared, int stack_stride, Hit& hit,
-                          TraceStats* stats) {
-  const f3 inv = vinv(d);  // exact reciprocal, used by the reference slab tests
-  // traversal reciprocal: zero components replaced by a tiny value of the same sign
-  const float tiny = 1e-20f;
-  const float dx = (fabsf(d.x) < tiny) ? copysignf(tiny, d.x) : d.x;
-  const float dy = (fabsf(d.y) < tiny) ? copysignf(tiny, d.y) : d.y;
-  const float dz = (fabsf(d.z) < tiny) ? copysignf(tiny, d.z) : d.z;
-  const float idx = 1.0f / dx, idy = 1.0f / dy, idz = 1.0f / dz;
-  const uint32_t oct = (idx < 0.0f ? 1u : 0u) | (idy < 0.0f ? 2u : 0u) | (idz < 0.0f ? 4u : 0u);
+// Byte k (0..3) of w as a float, exactly. (Measured on B200: the integer-to-float conversion is
+// slightly faster here than building 2^23 + byte with a byte-permute and subtracting 2^23, since
+// the traversal keeps the ALU and FMA pipes busier than the conversion pipe.)
+SWR_HD float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
 
-  hit.slot = 0xFFFFFFFFu;
-  hit.id = 0xFFFFFFFFu;
-  hit.rank = 0xFFFFFFFFu;
-  hit.obj = 0xFFFFFFFFu;
-  hit.t = INFINITY;
-  hit.d2 = INFINITY;
-  float tprune = INFINITY;
-
+// Resumable closest-hit traversal of one ray: init() sets the ray up, each step() expands at
+// most one wide node and tests the triangles of its hit leaves, and returns true once the ray is
+// finished (hit holds the result). The persistent kernels keep one Traversal per lane and refill
+// lanes whose ray finished; trace_closest() runs a single ray to completion.
+struct Traversal {
+  f3 o, d;
+  float idx, idy, idz;  // traversal reciprocal (zero components replaced by a tiny value)
+  uint32_t oct;
+  float tprune;
+  uint2 ng;  // node group: x = child_base, y = hits (bits 24..31, visit order) | imask (bits 0..7)
+  uint2 tg;  // triangle group: x = base, y = hit bits 0..23
+  Hit hit;
   GroupStack st;
-  st.shared = stack_shared;
-  st.stride = stack_stride;
-  st.sp = 0;
+  uint32_t host_turn;  // host build only: drives the alternating postponing decision
 
-  // node group: x = child_base, y = hits (bits 24..31, in visit order) | imask (bits 0..7)
-  uint2 ng = make_uint2(0u, (1u << (24 + oct)) | 1u);  // the root, as inner slot 0
-  uint2 tg = make_uint2(0u, 0u);                        // triangle group: base, hit bits 0..23
-  for (;;) {
-    if (ng.y & 0xFF000000u) {
+  SWR_HD void init(f3 o_, f3 d_, uint2* stack_shared, int stack_stride) {
+    o = o_;
+    d = d_;
+    host_turn = f2bits(o_.x) ^ f2bits(d_.y);
+    const float tiny = 1e-20f;
+    const float dx = (fabsf(d.x) < tiny) ? copysignf(tiny, d.x) : d.x;
+    const float dy = (fabsf(d.y) < tiny) ? copysignf(tiny, d.y) : d.y;
+    const float dz = (fabsf(d.z) < tiny) ? copysignf(tiny, d.z) : d.z;
+    idx = 1.0f / dx;
+    idy = 1.0f / dy;
+    idz = 1.0f / dz;
+    oct = (idx < 0.0f ? 1u : 0u) | (idy < 0.0f ? 2u : 0u) | (idz < 0.0f ? 4u : 0u);
+    hit.slot = 0xFFFFFFFFu;
+    hit.id = 0xFFFFFFFFu;
+    hit.rank = 0xFFFFFFFFu;
+    hit.obj = 0xFFFFFFFFu;
+    hit.t = INFINITY;
+    hit.d2 = INFINITY;
+    tprune = INFINITY;
+    st.shared = stack_shared;
+    st.stride = stack_stride;
+    st.sp = 0;
+    ng = make_uint2(0u, (1u << (24 + oct)) | 1u);  // the root, as inner slot 0
+    tg = make_uint2(0u, 0u);
+  }
+
+  // kPostpone: triangle postponing. While fewer than a fifth of the warp's active lanes have
+  // triangles to test, a lane that could still expand nodes parks its triangle group on its
+  // stack, so the warp runs one phase at a time. Without it a step expands one node and then
+  // tests all triangles of that node's hit leaves. (The visit order never changes the result:
+  // the closest hit is an arg-min over the same candidates.)
+  template <bool kStats, bool kPostpone = false>
+  SWR_HD bool step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                   const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
+                   TraceStats* stats) {
+    const bool has_nodes = (ng.y & 0xFF000000u) != 0;
+    bool tri_now = tg.y != 0;
+    if (kPostpone) {
+#if defined(__CUDA_ARCH__)
+      const unsigned act = __activemask();
+      const unsigned with_tris = __ballot_sync(act, tg.y != 0);
+      tri_now = tri_now && (!has_nodes || __popc(with_tris) * 5 >= __popc(act));
+#else
+      // host build: alternate the decision deterministically so both paths are exercised
+      tri_now = tri_now && (!has_nodes || ((host_turn++ * 2654435761u) >> 31) != 0);
+#endif
+    }
+    if (!tri_now && has_nodes) {
+      if (tg.y) {
+        st.push(make_uint2(tg.x | kTriGroup, tg.y));
+        tg.y = 0;
+      }
       const uint32_t k = (uint32_t)ffs(ng.y >> 24) - 1u;
       ng.y &= ~(1u << (24 + k));
       const uint32_t slot = k ^ oct;
@@ -147,12 +188,12 @@ SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __rest
       for (int i = 0; i < 8; ++i) {
         const int sh = (i & 3) * 8;
         const uint32_t m = ((i < 4 ? meta0 : meta1) >> sh) & 0xFFu;
-        const float qnx = (float)(((i < 4 ? nx0 : nx1) >> sh) & 0xFFu);
-        const float qny = (float)(((i < 4 ? ny0 : ny1) >> sh) & 0xFFu);
-        const float qnz = (float)(((i < 4 ? nz0 : nz1) >> sh) & 0xFFu);
-        const float qfx = (float)(((i < 4 ? fx0 : fx1) >> sh) & 0xFFu);
-        const float qfy = (float)(((i < 4 ? fy0 : fy1) >> sh) & 0xFFu);
-        const float qfz = (float)(((i < 4 ? fz0 : fz1) >> sh) & 0xFFu);
+        const float qnx = byte_f(i < 4 ? nx0 : nx1, i & 3);
+        const float qny = byte_f(i < 4 ? ny0 : ny1, i & 3);
+        const float qnz = byte_f(i < 4 ? nz0 : nz1, i & 3);
+        const float qfx = byte_f(i < 4 ? fx0 : fx1, i & 3);
+        const float qfy = byte_f(i < 4 ? fy0 : fy1, i & 3);
+        const float qfz = byte_f(i < 4 ? fz0 : fz1, i & 3);
         const float tnx = fmaf(qnx, ax, bx), tny = fmaf(qny, ay, by), tnz = fmaf(qnz, az, bz);
         const float tfx = fmaf(qfx, ax, bx), tfy = fmaf(qfy, ay, by), tfz = fmaf(qfz, az, bz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
@@ -165,9 +206,11 @@ SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __rest
       }
       ng = make_uint2(f2bits(n1.x), (inner << 24) | imask);
       tg = make_uint2(f2bits(n1.y), trih);
+      if (kPostpone) return false;
+      tri_now = true;
     }
 
-    while (tg.y) {
+    while (tri_now && tg.y) {
       const uint32_t j = (uint32_t)ffs(tg.y) - 1u;
       tg.y &= tg.y - 1u;
       const uint32_t s = tg.x + j;
@@ -180,6 +223,7 @@ SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __rest
       const uint32_t rank = f2bits(c.z);
       if (!(d2 < hit.d2 || (d2 == hit.d2 && rank < hit.rank))) continue;
       const uint32_t obj = f2bits(c.w);
+      const f3 inv = vinv(d);  // exact reciprocal of the reference's slab tests
       if (!ref_slab(tri_boxes + (size_t)s * 6, tri_boxes + (size_t)s * 6 + 3, o, inv)) continue;
       if (!ref_slab(obj_boxes + (size_t)obj * 6, obj_boxes + (size_t)obj * 6 + 3, o, inv)) continue;
       hit.slot = s;
@@ -191,11 +235,28 @@ SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __rest
       tprune = t * kPruneSlack;
     }
 
-    if (!(ng.y & 0xFF000000u)) {
-      if (st.sp == 0) break;
-      ng = st.pop();
+    if (!(ng.y & 0xFF000000u) && tg.y == 0) {
+      if (st.sp == 0) return true;
+      const uint2 g = st.pop();
+      if (g.x & kTriGroup) tg = make_uint2(g.x & ~kTriGroup, g.y);
+      else ng = g;
     }
+    return false;
   }
+};
+
+// Closest hit of ray (o, d), run to completion. obj_boxes/tri_boxes hold the reference's own
+// boxes (lo.xyz, hi.xyz) per object and per triangle record. Returns false on a miss.
+template <bool kStats, bool kPostpone = false>
+SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                          const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
+                          f3 o, f3 d, uint2* stack_shared, int stack_stride, Hit& hit,
+                          TraceStats* stats) {
+  Traversal tr;
+  tr.init(o, d, stack_shared, stack_stride);
+  while (!tr.template step<kStats, kPostpone>(nodes, tris, tri_boxes, obj_boxes, stats)) {
+  }
+  hit = tr.hit;
   return hit.slot != 0xFFFFFFFFu;
 }
 

@@ -55,7 +55,7 @@ class Twin:
             L.twin_depth.restype = ctypes.c_uint32
             L.twin_nodes.argtypes = [P]
             L.twin_nodes.restype = ctypes.c_uint32
-            L.twin_trace.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P]
+            L.twin_trace.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P, ctypes.c_int]
             L.twin_render.argtypes = [P, P] + [ctypes.c_uint32] * 4 + [ctypes.c_uint64, ctypes.c_uint32,
                                                                         ctypes.c_uint32, ctypes.c_float,
                                                                         ctypes.c_uint32, ctypes.c_uint32, P]
@@ -75,14 +75,14 @@ class Twin:
     def depth(self):
         return Twin._lib.twin_depth(self._h)
 
-    def trace(self, ro, rd, counts=False):
+    def trace(self, ro, rd, counts=False, postpone=False):
         n = ro.shape[0]
         tri = np.empty(n, np.uint32)
         d2 = np.empty(n, np.float32)
         t = np.empty(n, np.float32)
         c = np.empty((n, 2), np.uint32) if counts else None
         Twin._lib.twin_trace(self._h, ro.ctypes.data, rd.ctypes.data, n, tri.ctypes.data, d2.ctypes.data,
-                             t.ctypes.data, None if c is None else c.ctypes.data)
+                             t.ctypes.data, None if c is None else c.ctypes.data, 1 if postpone else 0)
         return (tri, d2, t, c) if counts else (tri, d2, t)
 
     def render(self, cam, W, H, spp, depth, seed, mode=0, rr_depth=0, rr_q=1.0, p0=0, p1=None):

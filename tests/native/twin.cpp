@@ -65,19 +65,31 @@ uint32_t twin_ref_tree(const float* boxes, uint32_t n, uint32_t* out) {
   return m;
 }
 
+// copies the packed wide-BVH node words (20 per node) into out (if not null); returns the count
+uint32_t twin_node_words(void* t, uint32_t* out) {
+  const auto& w = ((Twin*)t)->pk.nodes;
+  if (out) std::memcpy(out, w.data(), w.size() * 4);
+  return (uint32_t)w.size();
+}
+
 uint32_t twin_depth(void* t) { return ((Twin*)t)->pk.depth; }
 uint32_t twin_nodes(void* t) { return ((Twin*)t)->pk.num_nodes; }
 
 void twin_trace(void* tw, const float* ro, const float* rd, uint64_t n, uint32_t* tri, float* d2,
-                float* tt, uint32_t* counts) {
+                float* tt, uint32_t* counts, int postpone) {
   const swr::PackedScene& p = ((Twin*)tw)->pk;
   uint2 stack[swrx::kStackShared];
   for (uint64_t i = 0; i < n; ++i) {
     swrx::Hit h;
     swrx::TraceStats st{0, 0};
-    swrx::trace_closest<true>((const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(),
-                              p.obj_boxes.data(), swrx::mk(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]),
-                              swrx::mk(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]), stack, 1, h, &st);
+    const swrx::f3 o = swrx::mk(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]);
+    const swrx::f3 d = swrx::mk(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
+    if (postpone)
+      swrx::trace_closest<true, true>((const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(),
+                                      p.obj_boxes.data(), o, d, stack, 1, h, &st);
+    else
+      swrx::trace_closest<true, false>((const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(),
+                                       p.obj_boxes.data(), o, d, stack, 1, h, &st);
     tri[i] = h.id;
     d2[i] = h.d2;
     tt[i] = h.t;

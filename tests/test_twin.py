@@ -21,14 +21,14 @@ def test_twin_hits_match_reference_golden(name):
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
-@pytest.mark.parametrize("max_leaf", [1, 3])
-def test_twin_hits_match_oracle_random_rays(name, max_leaf):
+@pytest.mark.parametrize("max_leaf,postpone", [(1, False), (3, False), (3, True)])
+def test_twin_hits_match_oracle_random_rays(name, max_leaf, postpone):
     g = golden(name)
     sd = golden_scene(g)
     tw = Twin(sd, max_leaf=max_leaf)
     osc = O.OracleScene.from_scene_data(sd)
     ro, rd = rays_uniform(20000, sd.vpos.min(0) - 0.3, sd.vpos.max(0) + 0.3, seed=11)
-    tri, d2, t = tw.trace(ro, rd)
+    tri, d2, t = tw.trace(ro, rd, postpone=postpone)
     otri, od2, ot = osc.trace(ro, rd)
     assert np.array_equal(tri, otri)
     assert np.array_equal(d2.view(np.uint32), od2.view(np.uint32))
