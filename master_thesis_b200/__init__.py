@@ -2,8 +2,26 @@
 
 The compute path is the native library (master_thesis_b200/lib/libswr.so: C++ host surface +
 sm_100a CUDA kernels behind the C ABI in include/swr.h); this package is the Python tooling on
-top of it. Importing it loads the native library and fails if it has not been built.
+top of it. The native library is loaded on first use of any public name and its absence raises
+ImportError there: nothing falls back to another implementation. (Importing the build module,
+master_thesis_b200.build, does not load it, so a stale or missing library can be rebuilt.)
 """
-from ._native import (MODE_PHYSICAL, MODE_REFERENCE, SwrError)  # noqa: F401
-from .api import (Scene, SceneData, MAT_DTYPE, camera_arrays, load_camera, load_renderer,  # noqa: F401
-                  load_scene, quantize_rgb8, write_ppm)
+import importlib
+
+_EXPORTS = {
+    "MODE_PHYSICAL": "._native", "MODE_REFERENCE": "._native", "SwrError": "._native",
+    "Scene": ".api", "SceneData": ".api", "MAT_DTYPE": ".api", "camera_arrays": ".api",
+    "load_camera": ".api", "load_renderer": ".api", "load_scene": ".api", "quantize_rgb8": ".api",
+    "write_ppm": ".api",
+}
+
+__all__ = sorted(_EXPORTS)
+
+
+def __getattr__(name):
+    mod = _EXPORTS.get(name)
+    if mod is None:
+        raise AttributeError("module 'master_thesis_b200' has no attribute %r" % name)
+    value = getattr(importlib.import_module(mod, __name__), name)
+    globals()[name] = value
+    return value
