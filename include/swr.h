@@ -212,6 +212,22 @@ typedef struct swr_render_profile {
 int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                         float* rgb_out, float* samples_out, void* stream, swr_render_profile* prof);
 
+/* Allocation-free variant of swr_render. It has no counterpart in the reference (whose renderer
+ * is a host-thread loop): it exists for callers that must not have a library allocate device
+ * memory during the call, such as applications that give all device memory to their own pool
+ * up front, or frame loops that cannot afford the device-wide synchronisation a cudaMalloc or
+ * cudaFree can cause. It calls no allocator; its scratch is one 64 MiB file-scope device array
+ * that every device holds from the moment it loads the library until the process exits.
+ * Limits: rgb_out (and samples_out when SWR_RENDER_SAMPLES_OUT is set) must be device memory;
+ * spp <= 2^21; wave_size <= 65536 (0 = 65536); block_size 0 or 256; trace_blocks 0; no flag other
+ * than SWR_RENDER_SAMPLES_OUT; larger requests are rejected with SWR_ERR_UNSUPPORTED. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before capturing any stream on the device. All calls share the
+ * one array, so calls that overlap on the GPU (other streams or host threads) race on it and must
+ * be serialised by the caller. Results equal swr_render's for the same arguments. */
+int swr_render_noalloc(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
+                       float* rgb_out, float* samples_out, void* stream);
+
 /* Reference-style 8-bit quantisation (graphics_engine.cpp:90-95: clamp to [0,1], *255, truncate)
  * and P6 PPM writer (graphics_engine.cpp:32-40). Host memory. */
 int swr_quantize_rgb8(const float* rgb, uint32_t width, uint32_t height, uint8_t* out);

@@ -17,6 +17,7 @@
 // kernels advance themselves, so the host only launches kernels and polls completion.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "shading.cuh"
@@ -621,6 +622,164 @@ void free_workspace(swr_scene* s) {
   s->workspace = nullptr;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Allocation-free render (swr_render_noalloc).
+//
+// Some callers cannot let a library allocate device memory while they run: applications that
+// hand all device memory to their own pool up front and forbid allocation by plug-ins, and
+// latency-sensitive loops that must not pay for cudaMalloc/cudaFree, which can synchronise the
+// whole device. For them the wavefront's scratch (path queues, per-pixel camera records,
+// per-sample slots and the control block) lives in one file-scope device array of fixed size,
+// loaded with the library and held by every device that loads it until the process exits.
+// Every call uses the same array: calls that overlap on the GPU (different streams or threads)
+// race on it and must be serialised by the caller. Nothing in the array needs to start at zero:
+// each chunk overwrites the control block from the host and writes every camera record and
+// sample slot it later reads.
+constexpr size_t kNoAllocBytes = 64ull << 20;           // 64 MiB of device scratch
+constexpr uint32_t kNoAllocCap = 1u << 16;              // paths in flight
+constexpr uint64_t kNoAllocChunkSamples = 1ull << 21;   // samples per chunk
+constexpr uint64_t kNoAllocChunkPixels = 1ull << 18;    // pixels per chunk
+constexpr size_t kNoAllocQueueBytes = (size_t)kNoAllocCap * (4 * sizeof(float4) + sizeof(uint2));
+constexpr size_t kNoAllocCamOffset = 256 + 2 * kNoAllocQueueBytes;
+constexpr size_t kNoAllocContribOffset = kNoAllocCamOffset + kNoAllocChunkPixels * 2 * sizeof(float4);
+static_assert(kNoAllocContribOffset + kNoAllocChunkSamples * sizeof(float4) <= kNoAllocBytes,
+              "no-allocation scratch layout exceeds its array");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device. In host
+// code the array's name is only a stand-in for the symbol, never a device address.
+static int noalloc_scratch(int device, char** out) {
+  static std::mutex mu;
+  static char* addr[64] = {nullptr};
+  if (device < 0 || device >= 64) return set_error(SWR_ERR_UNSUPPORTED, "swr: device index above 63");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    addr[device] = (char*)p;
+  }
+  *out = addr[device];
+  return SWR_OK;
+}
+
+int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
+                        float* samples_out, void* stream_) {
+  if (!s || !cam || !o || !rgb_out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (o->width == 0 || o->height == 0 || o->spp == 0)
+    return set_error(SWR_ERR_INVALID, "swr: zero image size or samples");
+  if (o->max_depth == 0 || o->max_depth > 31)
+    return set_error(SWR_ERR_INVALID, "swr: max_depth must be 1..31");
+  if (o->mode > 1) return set_error(SWR_ERR_INVALID, "swr: unknown mode");
+  if (o->mode == 1 && o->rr_depth != 0 && !(o->rr_survive > 0.0f && o->rr_survive <= 1.0f))
+    return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+  if ((uint64_t)o->width * o->height >= (1ull << 32))
+    return set_error(SWR_ERR_INVALID, "swr: image too large");
+  if (o->flags & ~SWR_RENDER_SAMPLES_OUT)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: swr_render_noalloc accepts only SWR_RENDER_SAMPLES_OUT");
+  const bool want_samples = (o->flags & SWR_RENDER_SAMPLES_OUT) != 0;
+  if (want_samples && !samples_out)
+    return set_error(SWR_ERR_INVALID, "swr: SWR_RENDER_SAMPLES_OUT without a samples buffer");
+  if (o->spp > kNoAllocChunkSamples)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: swr_render_noalloc handles at most 2097152 samples per pixel "
+                                          "(its fixed scratch holds 2^21 sample slots)");
+  if (o->wave_size > kNoAllocCap)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: swr_render_noalloc keeps at most 65536 paths in flight");
+  if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  if (o->block_size && o->block_size != 256)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: swr_render_noalloc shades with 256-thread blocks");
+  if (o->trace_blocks) return set_error(SWR_ERR_UNSUPPORTED, "swr: swr_render_noalloc uses trace_blocks 0");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  if (is_host_pointer(rgb_out) || (want_samples && is_host_pointer(samples_out)))
+    return set_error(SWR_ERR_INVALID, "swr: swr_render_noalloc needs device output buffers (staging host "
+                                      "memory would need a device allocation)");
+  char* base = nullptr;
+  int rc = noalloc_scratch(s->device, &base);
+  if (rc) return rc;
+
+  const uint64_t npix_total = (uint64_t)o->width * o->height;
+  const uint64_t px_per_chunk =
+      std::max<uint64_t>(1, std::min<uint64_t>(std::min<uint64_t>(npix_total, kNoAllocChunkSamples / o->spp),
+                                                kNoAllocChunkPixels));
+  uint32_t cap = o->wave_size ? o->wave_size : kNoAllocCap;
+  cap = (uint32_t)std::min<uint64_t>(cap, px_per_chunk * o->spp);
+  cap = std::min<uint32_t>(kNoAllocCap, std::max<uint32_t>(32, (cap + 255u) & ~255u));
+
+  Ctrl* ctrl = (Ctrl*)base;
+  Queue Q[2];
+  {
+    char* b = base + 256;
+    for (int p = 0; p < 2; ++p) {
+      Q[p].o = (float4*)b; b += (size_t)kNoAllocCap * sizeof(float4);
+      Q[p].d = (float4*)b; b += (size_t)kNoAllocCap * sizeof(float4);
+      Q[p].c = (float4*)b; b += (size_t)kNoAllocCap * sizeof(float4);
+      Q[p].l = (float4*)b; b += (size_t)kNoAllocCap * sizeof(float4);
+      Q[p].hit = (uint2*)b; b += (size_t)kNoAllocCap * sizeof(uint2);
+    }
+  }
+  Frame F;
+  std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
+  std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
+  std::memcpy(F.org, cam->origin, sizeof(F.org));
+  F.W = o->width;
+  F.H = o->height;
+  F.spp = o->spp;
+  F.depth = o->max_depth;
+  F.mode = o->mode;
+  F.rr_depth = (o->mode == 1) ? o->rr_depth : 0;
+  F.rr_q = (o->mode == 1 && o->rr_depth) ? o->rr_survive : 1.0f;
+  F.seed = o->seed;
+  F.capacity = cap;
+  F.refill = o->refill ? o->refill : 8;
+  F.cam = (float4*)(base + kNoAllocCamOffset);
+  F.contrib = (float4*)(base + kNoAllocContribOffset);
+
+  int trace_per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, k_trace_dyn<false, 0, false>,
+                                                         kTraceBlock, 0));
+  const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
+  const unsigned shade_grid = (cap + 255) / 256;
+  for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
+    const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
+    F.pixel0 = (uint32_t)p0;
+    F.npix = np;
+    const uint64_t total = (uint64_t)np * o->spp;
+    Ctrl init;
+    std::memset(&init, 0, sizeof(init));
+    init.total = total;
+    init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, total);
+    init.injected = init.inj_n[0];
+    // pageable source: the copy has been taken when the call returns
+    SWR_CUDA(cudaMemcpyAsync(ctrl, &init, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ctrl);
+    SWR_CUDA(cudaGetLastError());
+    uint64_t k = 0;
+    const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
+    for (;;) {
+      if (k > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
+      for (int c = 0; c < 8; ++c, ++k) {
+        const int p = (int)(k & 1);
+        k_shade<256><<<shade_grid, 256, 0, stream>>>(s->dev, F, ctrl, Q[p], Q[p ^ 1], p);
+        k_trace_dyn<false, 0, false><<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ctrl, Q[p ^ 1], p);
+      }
+      SWR_CUDA(cudaGetLastError());
+      Ctrl h;
+      SWR_CUDA(cudaMemcpyAsync(&h, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+      SWR_CUDA(cudaStreamSynchronize(stream));
+      const int np_ = (int)(k & 1);
+      if (h.count[np_] == 0 && h.inj_n[np_] == 0 && h.injected == h.total) break;
+    }
+    k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, rgb_out);
+    SWR_CUDA(cudaGetLastError());
+    if (want_samples)
+      SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)p0 * o->spp * 4, F.contrib, (size_t)np * o->spp * sizeof(float4),
+                               cudaMemcpyDeviceToDevice, stream));
+  }
+  return SWR_OK;
+}
+
 }  // namespace swr
 
 extern "C" {
@@ -633,6 +792,11 @@ int swr_render(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, fl
 int swr_render_profiled(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
                         float* samples_out, void* stream, swr_render_profile* prof) {
   return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, prof);
+}
+
+int swr_render_noalloc(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
+                       float* samples_out, void* stream) {
+  return swr::render_noalloc_impl(s, cam, o, rgb_out, samples_out, stream);
 }
 
 }  // extern "C"
