@@ -115,8 +115,8 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """ncu DRAM bytes per launch of the bounce traversal kernel and the algorithmic bytes of the same
-    launch, from the committed summary of one capture (profiles/k_trace_terrain.json)."""
+    """DRAM bytes per traced ray of the bounce traversal kernel, from the committed summary of one
+    ncu capture of a full-queue launch on the terrain scene (profiles/k_trace_terrain.json)."""
     p = os.path.join(ROOT, "profiles", "k_trace_terrain.json")
     if not os.path.exists(p):
         return None
@@ -282,9 +282,9 @@ def main():
     peak, peak_kind = measured_peaks()
     tp = profile_traffic()
     traffic = None
-    if tp and tp.get("workload") == args.config:
-        # DRAM bytes per algorithmic byte of the captured launch, applied to this launch's bytes
-        traffic = per_launch_bytes * tp["dram_bytes"] / tp["algorithmic_bytes"]
+    if tp and tp.get("scene") == cfg["kind"]:
+        # the captured launch's DRAM bytes per ray, scaled to this run's rays per launch
+        traffic = tp["dram_bytes_per_ray"] * rays_per_step * args.steps / max(launches, 1)
     mrays = sum(p["rays"] for p in profs) / (sum(step_ms) / 1e3) / 1e6
     launches_total = sum(p["launches"] for p in profs)
 
@@ -315,6 +315,7 @@ def main():
                     "step_ms": {"min": min(e2e_ms), "median": statistics.median(e2e_ms), "max": max(e2e_ms)}},
             "mrays_per_s": mrays,
             "rays_per_sample": profs[-1]["rays"] / (W * H * spp),
+            "first_trace_rays": int(profs[-1]["first_trace_rays"]),
             "roofline": {"bound": "hbm", "kernel": "k_trace (bounce traversal)", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": per_launch_bytes,

@@ -204,6 +204,7 @@ typedef struct swr_render_profile {
   uint64_t iterations;      /* shade/trace rounds */
   uint64_t launches;        /* kernels launched by the call */
   uint64_t trace_launches;  /* launches of the bounce traversal kernel */
+  uint64_t first_trace_rays;  /* rays of its first non-empty launch (first chunk) */
   uint64_t h2d_bytes, d2h_bytes;  /* explicit host<->device copies made by the call */
   double trace_ms, shade_ms, camera_ms, resolve_ms;
 } swr_render_profile;

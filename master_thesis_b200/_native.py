@@ -73,7 +73,8 @@ class RenderOpts(ctypes.Structure):
 
 class RenderProfile(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ["rays", "bounce_rays", "node_visits", "tri_tests", "iterations",
-                                               "launches", "trace_launches", "h2d_bytes", "d2h_bytes"]] + \
+                                               "launches", "trace_launches", "first_trace_rays", "h2d_bytes",
+                                               "d2h_bytes"]] + \
                [(n, ctypes.c_double) for n in ["trace_ms", "shade_ms", "camera_ms", "resolve_ms"]]
 
     def as_dict(self):

@@ -37,7 +37,8 @@ struct Ctrl {
   unsigned int count[2];
   unsigned int cursor[2];
   unsigned int inj_n[2];
-  unsigned int pad0[2];
+  unsigned int first_n;  // rays of the first non-empty bounce-traversal launch of the chunk
+  unsigned int pad0;
   unsigned long long inj_base[2];
   unsigned long long injected;
   unsigned long long total;
@@ -216,6 +217,7 @@ __global__ void __launch_bounds__(kTraceBlock)
     ctrl->count[parity] = 0u;
     ctrl->rays += n;
     ctrl->bounce_rays += n;
+    if (ctrl->first_n == 0u) ctrl->first_n = n;
   }
   swrx::TraceStats st{0, 0};
   for (;;) {
@@ -266,6 +268,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     ctrl->count[parity] = 0u;
     ctrl->rays += n;
     ctrl->bounce_rays += n;
+    if (ctrl->first_n == 0u) ctrl->first_n = n;
   }
   const unsigned lane = lane_id();
   const unsigned lt = (1u << lane) - 1u;
@@ -572,6 +575,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       if (h.count[np_] == 0 && h.inj_n[np_] == 0 && h.injected == h.total) {
         P.rays += h.rays;
         P.bounce_rays += h.bounce_rays;
+        if (P.first_trace_rays == 0) P.first_trace_rays = h.first_n;
         P.node_visits += h.nodes;
         P.tri_tests += h.tris;
         P.iterations += k;
