@@ -213,6 +213,26 @@ typedef struct swr_render_profile {
 int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                         float* rgb_out, float* samples_out, void* stream, swr_render_profile* prof);
 
+/* Physical-mode parameters of a built scene (no rebuild): diffuse albedo per triangle
+ * ([num_triangles*3], by global triangle id) and emitted radiance L_e per object ([num_objects*3];
+ * only objects marked light_source emit). Device or host memory. No counterpart in the reference,
+ * whose materials are per object and fixed at load time. */
+int swr_scene_set_albedo(swr_scene* scene, const float* albedo, void* stream);
+int swr_scene_set_emission(swr_scene* scene, const float* emission, void* stream);
+
+/* Gradient of sum_p dl_dimage[p] . image[p] for the SWR_MODE_PHYSICAL image that swr_render
+ * produces with the same scene, camera and opts (same seed = the same sampled paths), with respect
+ * to the per-triangle albedo ([num_triangles*3] by triangle id) and the per-object emission
+ * ([num_objects*3]). Each camera path is re-traced from its random-number counters (path replay)
+ * instead of being stored by the primal render. Outputs are overwritten. Device buffers;
+ * max_depth <= 16. No counterpart in the reference (it has no differentiable renderer). */
+int swr_render_adjoint(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
+                       const float* dl_dimage, float* dl_dalbedo, float* dl_demission, void* stream);
+/* As swr_render_adjoint, also returning its device time in milliseconds (CUDA events). */
+int swr_render_adjoint_timed(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
+                             const float* dl_dimage, float* dl_dalbedo, float* dl_demission,
+                             void* stream, double* device_ms);
+
 /* Allocation-free variant of swr_render. It has no counterpart in the reference (whose renderer
  * is a host-thread loop): it exists for callers that must not have a library allocate device
  * memory during the call, such as applications that give all device memory to their own pool

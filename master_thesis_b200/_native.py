@@ -107,6 +107,11 @@ SIGNATURES = {
     "swr_render_profiled": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P,
                                 ctypes.POINTER(RenderProfile)]),
     "swr_render_noalloc": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P]),
+    "swr_scene_set_albedo": (I, [P, P, P]),
+    "swr_scene_set_emission": (I, [P, P, P]),
+    "swr_render_adjoint": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P, P]),
+    "swr_render_adjoint_timed": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P, P,
+                                     ctypes.POINTER(ctypes.c_double)]),
     "swr_quantize_rgb8": (I, [P, U32, U32, P]),
     "swr_write_ppm": (I, [ctypes.c_char_p, P, U32, U32]),
 }

@@ -190,6 +190,36 @@ class Scene:
         return (out, prof.as_dict()) if return_profile else out
 
 
+def _scene_set_albedo(self, albedo, stream=None):
+    """Per-triangle diffuse albedo [num_triangles, 3] (by triangle id) for the physical mode."""
+    check(N.lib.swr_scene_set_albedo(self._h, ptr(albedo), _stream_handle(stream)))
+
+
+def _scene_set_emission(self, emission, stream=None):
+    """Per-object emitted radiance [num_objects, 3] (only light-source objects emit)."""
+    check(N.lib.swr_scene_set_emission(self._h, ptr(emission), _stream_handle(stream)))
+
+
+def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=0, rr_depth=0, rr_survive=1.0,
+                          refill=0, stream=None, return_ms=False):
+    """Gradients (albedo [num_triangles,3], emission [num_objects,3]) of sum(dl_dimage * image) for
+    the physical-mode image rendered with the same arguments (path replay). Device tensors."""
+    import torch
+    dl = dl_dimage.contiguous()
+    ga = torch.empty((self.data.num_triangles, 3), dtype=torch.float32, device=dl.device)
+    ge = torch.empty((self.data.num_objects, 3), dtype=torch.float32, device=dl.device)
+    o = N.RenderOpts(width, height, spp, depth, seed, N.MODE_PHYSICAL, rr_depth, rr_survive, 0, 0, 0, refill, 0, 0)
+    ms = ctypes.c_double(0.0)
+    check(N.lib.swr_render_adjoint_timed(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(dl), ptr(ga), ptr(ge),
+                                         _stream_handle(stream), ctypes.byref(ms) if return_ms else None))
+    return (ga, ge, ms.value) if return_ms else (ga, ge)
+
+
+Scene.set_albedo = _scene_set_albedo
+Scene.set_emission = _scene_set_emission
+Scene.render_adjoint = _scene_render_adjoint
+
+
 def quantize_rgb8(img):
     img = np.ascontiguousarray(img, dtype=np.float32)
     h, w = img.shape[:2]

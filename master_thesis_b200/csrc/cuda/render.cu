@@ -315,6 +315,146 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Path-replay adjoint of the physical-mode image.
+//
+// Each lane carries one camera sample at a time: it re-creates the sample's path from its Philox
+// counters (the same hits, directions and throughputs as the primal render), keeping for each
+// scattering vertex the triangle slot, the throughput c_j before the vertex and the factor
+// gq_j the vertex applied besides the albedo (2 cos / q for a diffuse bounce, 1 / q otherwise).
+// A path that ends on an emitter seen from the front contributes L = c_e * Le; sweeping its
+// vertices backwards with S = Le, dL/dalbedo(tri_j) = c_j * gq_j * S_{j+1} and S_j = albedo_j *
+// gq_j * S_{j+1}; dL/dLe = c_e. Each term is weighted by dLoss/dImage of the pixel / spp and
+// added atomically to per-triangle / per-object gradients. Nothing of the primal pass is stored:
+// the path is replayed, which is the checkpointing scheme. Lanes that finish a sample take a new
+// one (refill as in the bounce traversal), and the traversal itself is the resumable Traversal.
+constexpr int kAdjMaxDepth = 16;
+
+__global__ void __launch_bounds__(kTraceBlock)
+    k_adjoint(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, const float* __restrict__ dl,
+              float* __restrict__ g_alb, float* __restrict__ g_em) {
+  __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned long long total = ctrl->total;
+  swrx::Traversal tr;
+  swrx::PathState st;
+  uint32_t pixel = 0, sample = 0;
+  uint32_t h_slot[kAdjMaxDepth];
+  float h_cx[kAdjMaxDepth], h_cy[kAdjMaxDepth], h_cz[kAdjMaxDepth], h_gq[kAdjMaxDepth];
+  uint32_t h_diff = 0;
+  int nv = 0;
+  bool active = false, tracing = false, exhausted = false;
+  uint32_t pend_slot = 0;
+  float pend_t = 0.0f;
+  const float inv_spp = 1.0f / (float)F.spp;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
+      unsigned long long base = 0;
+      // inj_base[0] serves as the sample cursor of the adjoint launch
+      if (lane == 0) base = atomicAdd(&ctrl->inj_base[0], (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) exhausted = true;
+      if (!active) {
+        const unsigned long long g = base + __popc(idle & lt);
+        if (g < total) {
+          pixel = (uint32_t)(g / F.spp);
+          sample = (uint32_t)(g % F.spp);
+          const float4 r0 = F.cam[2 * (size_t)pixel], r1 = F.cam[2 * (size_t)pixel + 1];
+          const uint32_t bits = __float_as_uint(r1.w);
+          if (bits != kDeadSlot) {
+            st.o = mk(r0.x, r0.y, r0.z);
+            st.d = mk(r1.x, r1.y, r1.z);
+            st.c = mk(1.0f, 1.0f, 1.0f);
+            st.L = mk(0.0f, 0.0f, 0.0f);
+            st.i = bits >> 27;
+            st.v = 0;
+            pend_slot = bits & 0x07FFFFFFu;
+            pend_t = r0.w;
+            nv = 0;
+            h_diff = 0;
+            tracing = false;
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+    if (tracing) {
+      if (!tr.step<false, false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, nullptr)) continue;
+      tracing = false;
+      if (tr.hit.slot == 0xFFFFFFFFu) {  // the path left the scene: no emitter, no gradient
+        active = false;
+        continue;
+      }
+      pend_slot = tr.hit.slot;
+      pend_t = tr.hit.t;
+    }
+    // shade the pending hit
+    swrx::ShadeParams P;
+    P.seed = F.seed;
+    P.pixel = F.pixel0 + pixel;
+    P.sample = sample;
+    P.depth = F.depth;
+    P.mode = 1;
+    P.rr_depth = F.rr_depth;
+    P.rr_q = F.rr_q;
+    const float cx = st.c.x, cy = st.c.y, cz = st.c.z;
+    swrx::AdjVertex av;
+    const uint32_t outcome =
+        swrx::shade_physical_adj(sc.tris, sc.shade, sc.mats, sc.albedo, pend_slot, pend_t, P, st, av);
+    // a vertex after which the path goes on is kept for the sweep; a path that ends without an
+    // emitter (depth reached, Russian roulette, escape) carries no radiance and no gradient
+    if (outcome == swrx::kContinue) {
+      h_slot[nv] = pend_slot;
+      h_cx[nv] = cx;
+      h_cy[nv] = cy;
+      h_cz[nv] = cz;
+      h_gq[nv] = av.gq;
+      if (av.diffuse) h_diff |= 1u << nv;
+      ++nv;
+    }
+    if (outcome == swrx::kContinue) {
+      tr.init(st.o, st.d, stack + threadIdx.x, kTraceBlock);
+      tracing = true;
+      continue;
+    }
+    if (av.emit_front) {
+      const float* dlp = dl + (size_t)(F.pixel0 + pixel) * 3;
+      const float wx = dlp[0] * inv_spp, wy = dlp[1] * inv_spp, wz = dlp[2] * inv_spp;
+      atomicAdd(&g_em[3 * (size_t)av.obj + 0], wx * cx);
+      atomicAdd(&g_em[3 * (size_t)av.obj + 1], wy * cy);
+      atomicAdd(&g_em[3 * (size_t)av.obj + 2], wz * cz);
+      const float4 le = __ldg(sc.mats + 3 * (size_t)av.obj + 2);
+      float sx = le.x, sy = le.y, sz = le.z;
+      for (int j = nv - 1; j >= 0; --j) {
+        const float gq = h_gq[j];
+        if (h_diff & (1u << j)) {
+          const uint32_t s = h_slot[j];
+          const uint32_t id = __float_as_uint(__ldg(sc.tris + 3 * (size_t)s + 2).y);
+          atomicAdd(&g_alb[3 * (size_t)id + 0], wx * h_cx[j] * gq * sx);
+          atomicAdd(&g_alb[3 * (size_t)id + 1], wy * h_cy[j] * gq * sy);
+          atomicAdd(&g_alb[3 * (size_t)id + 2], wz * h_cz[j] * gq * sz);
+          const float* a = sc.albedo + 3 * (size_t)s;
+          sx *= a[0] * gq;
+          sy *= a[1] * gq;
+          sz *= a[2] * gq;
+        } else {
+          sx *= gq;
+          sy *= gq;
+          sz *= gq;
+        }
+      }
+    }
+    active = false;
+  }
+}
+
 __global__ void k_resolve(Frame F, float* __restrict__ img) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= F.npix) return;
@@ -626,6 +766,84 @@ void free_workspace(swr_scene* s) {
   s->workspace = nullptr;
 }
 
+int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, const float* dl,
+                        float* g_alb, float* g_em, void* stream_, double* ms_out) {
+  if (!s || !cam || !o || !dl || !g_alb || !g_em) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (o->mode != SWR_MODE_PHYSICAL)
+    return set_error(SWR_ERR_INVALID, "swr: the adjoint is defined for SWR_MODE_PHYSICAL");
+  if (o->width == 0 || o->height == 0 || o->spp == 0)
+    return set_error(SWR_ERR_INVALID, "swr: zero image size or samples");
+  if (o->max_depth == 0 || o->max_depth > (uint32_t)kAdjMaxDepth)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: the adjoint supports max_depth 1..16");
+  if (o->rr_depth != 0 && !(o->rr_survive > 0.0f && o->rr_survive <= 1.0f))
+    return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+  if ((uint64_t)o->width * o->height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
+  if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  if (is_host_pointer(dl) || is_host_pointer(g_alb) || is_host_pointer(g_em))
+    return set_error(SWR_ERR_INVALID, "swr: the adjoint takes device buffers");
+  RenderWorkspace* ws = workspace_of(s);
+  const uint64_t npix_total = (uint64_t)o->width * o->height;
+  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
+  int rc;
+  if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
+  if (!ws->ctrl) {
+    SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
+  }
+  SWR_CUDA(cudaMemsetAsync(g_alb, 0, (size_t)s->dev.num_tris * 3 * sizeof(float), stream));
+  SWR_CUDA(cudaMemsetAsync(g_em, 0, (size_t)s->dev.num_objects * 3 * sizeof(float), stream));
+  Frame F;
+  std::memset(&F, 0, sizeof(F));
+  std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
+  std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
+  std::memcpy(F.org, cam->origin, sizeof(F.org));
+  F.W = o->width;
+  F.H = o->height;
+  F.spp = o->spp;
+  F.depth = o->max_depth;
+  F.mode = 1;
+  F.rr_depth = o->rr_depth;
+  F.rr_q = o->rr_depth ? o->rr_survive : 1.0f;
+  F.seed = o->seed;
+  F.refill = o->refill ? o->refill : 8;
+  F.cam = (float4*)ws->cam;
+  int per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, kTraceBlock, 0));
+  const unsigned grid = (unsigned)(s->num_sms * std::max(per_sm, 1));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms_out) {
+    SWR_CUDA(cudaEventCreate(&e0));
+    SWR_CUDA(cudaEventCreate(&e1));
+    SWR_CUDA(cudaEventRecord(e0, stream));
+  }
+  for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
+    const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
+    F.pixel0 = (uint32_t)p0;
+    F.npix = np;
+    Ctrl init;
+    std::memset(&init, 0, sizeof(init));
+    init.total = (uint64_t)np * o->spp;
+    SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
+    *ws->host_ctrl = init;
+    SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    k_adjoint<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, dl, g_alb, g_em);
+    SWR_CUDA(cudaGetLastError());
+  }
+  if (ms_out) {
+    SWR_CUDA(cudaEventRecord(e1, stream));
+    SWR_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    SWR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *ms_out = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  return SWR_OK;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Allocation-free render (swr_render_noalloc).
 //
@@ -796,6 +1014,17 @@ int swr_render(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, fl
 int swr_render_profiled(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
                         float* samples_out, void* stream, swr_render_profile* prof) {
   return swr::render_impl(s, cam, o, rgb_out, samples_out, stream, prof);
+}
+
+int swr_render_adjoint(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, const float* dl_dimage,
+                       float* dl_dalbedo, float* dl_demission, void* stream) {
+  return swr::render_adjoint_impl(s, cam, o, dl_dimage, dl_dalbedo, dl_demission, stream, nullptr);
+}
+
+int swr_render_adjoint_timed(swr_scene* s, const swr_camera* cam, const swr_render_opts* o,
+                             const float* dl_dimage, float* dl_dalbedo, float* dl_demission, void* stream,
+                             double* device_ms) {
+  return swr::render_adjoint_impl(s, cam, o, dl_dimage, dl_dalbedo, dl_demission, stream, device_ms);
 }
 
 int swr_render_noalloc(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,

@@ -41,6 +41,39 @@ int upload(void** dst, const std::vector<T>& v) {
 
 constexpr int kTraceBlock = 128;
 
+// albedo given per triangle id -> the per-slot array the kernels read
+__global__ void k_set_albedo(const uint32_t* __restrict__ slot_of, const float* __restrict__ by_id,
+                             float* __restrict__ by_slot, uint32_t n) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t s = slot_of[t];
+  by_slot[3 * (size_t)s + 0] = by_id[3 * (size_t)t + 0];
+  by_slot[3 * (size_t)s + 1] = by_id[3 * (size_t)t + 1];
+  by_slot[3 * (size_t)s + 2] = by_id[3 * (size_t)t + 2];
+}
+
+// emitted radiance per object -> the third record of each material
+__global__ void k_set_emission(float4* __restrict__ mats, const float* __restrict__ em, uint32_t n) {
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  float4 m = mats[3 * (size_t)o + 2];
+  m.x = em[3 * (size_t)o + 0];
+  m.y = em[3 * (size_t)o + 1];
+  m.z = em[3 * (size_t)o + 2];
+  mats[3 * (size_t)o + 2] = m;
+}
+
+// copies host input to a temporary device buffer when needed; returns the device pointer
+int device_input(const float* p, size_t bytes, cudaStream_t stream, void** tmp, const float** dev) {
+  *tmp = nullptr;
+  *dev = p;
+  if (!is_host_pointer(p)) return SWR_OK;
+  SWR_CUDA(cudaMallocAsync(tmp, bytes, stream));
+  SWR_CUDA(cudaMemcpyAsync(*tmp, p, bytes, cudaMemcpyHostToDevice, stream));
+  *dev = (const float*)*tmp;
+  return SWR_OK;
+}
+
 template <bool kStats>
 __global__ void __launch_bounds__(kTraceBlock)
     k_trace_closest(DevScene sc, const float4* __restrict__ ro, const float4* __restrict__ rd,
@@ -214,6 +247,36 @@ int swr_scene_stats(const swr_scene* s, uint64_t out[8]) {
   out[5] = s->dev.num_objects;
   out[6] = 80;
   out[7] = 48;
+  return SWR_OK;
+}
+
+int swr_scene_set_albedo(swr_scene* s, const float* albedo, void* stream_) {
+  if (!s || !albedo) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  void* tmp;
+  const float* dev;
+  const uint32_t n = s->dev.num_tris;
+  int rc = swr::device_input(albedo, (size_t)n * 3 * sizeof(float), stream, &tmp, &dev);
+  if (rc) return rc;
+  swr::k_set_albedo<<<(n + 255) / 256, 256, 0, stream>>>(s->dev.slot_of, dev, (float*)s->d_albedo, n);
+  SWR_CUDA(cudaGetLastError());
+  if (tmp) SWR_CUDA(cudaFreeAsync(tmp, stream));
+  return SWR_OK;
+}
+
+int swr_scene_set_emission(swr_scene* s, const float* emission, void* stream_) {
+  if (!s || !emission) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  void* tmp;
+  const float* dev;
+  const uint32_t n = s->dev.num_objects;
+  int rc = swr::device_input(emission, (size_t)n * 3 * sizeof(float), stream, &tmp, &dev);
+  if (rc) return rc;
+  swr::k_set_emission<<<(n + 255) / 256, 256, 0, stream>>>((float4*)s->d_mats, dev, n);
+  SWR_CUDA(cudaGetLastError());
+  if (tmp) SWR_CUDA(cudaFreeAsync(tmp, stream));
   return SWR_OK;
 }
 

@@ -179,6 +179,68 @@ SWR_HD uint32_t shade_vertex(const float4* tris, const float4* shade, const floa
   return (st.i < P.depth) ? kContinue : kEndDark;
 }
 
+// Physical-mode shading of one vertex for the adjoint replay: the same arithmetic as the
+// physical branch of shade_vertex (so the replayed path and throughput are the primal's), plus
+// what the backward sweep needs. On return: diffuse tells whether the throughput was multiplied
+// by albedo * gq (gq = 2 cos / q), else only by gq (gq = 1 / q); emitter / emit_front describe an
+// emitter hit (no scattering then).
+struct AdjVertex {
+  bool emitter, emit_front, diffuse;
+  float gq;
+  uint32_t obj;
+};
+
+SWR_HD uint32_t shade_physical_adj(const float4* tris, const float4* shade, const float4* mats,
+                                   const float* albedo, uint32_t slot, float t, const ShadeParams& P,
+                                   PathState& st, AdjVertex& av) {
+  const f3 p = hit_point(st.o, st.d, t);
+  const f3 n = shading_normal(tris, shade, slot, p);
+  const uint32_t obj = f2bits(ld4(tris + (size_t)slot * 3 + 2).w);
+  const Material m = load_material(mats, obj);
+  av.obj = obj;
+  av.diffuse = false;
+  av.gq = 1.0f;
+  const bool front = vdot(n, st.d) <= 0.0f;
+  av.emitter = f2bits(m.m1.w) != 0u;
+  av.emit_front = av.emitter && front;
+  if (av.emitter) {
+    if (front) {
+      st.L.x += st.c.x * m.m2.x;
+      st.L.y += st.c.y * m.m2.y;
+      st.L.z += st.c.z * m.m2.z;
+    }
+    return kEndLight;
+  }
+  const Uniforms U = vertex_uniforms(P.seed, P.pixel, P.sample, st.v, 0);
+  const float r = U.u[0];
+  f3 nd = st.d;
+  float w = 1.0f;
+  if (r <= m.m0.w) {
+    const f3 ns = front ? n : mk(-n.x, -n.y, -n.z);
+    nd = hemisphere_dir(ns, U.u[1], U.u[2]);
+    w = 2.0f * vdot(ns, nd);
+    const float* a = albedo + (size_t)slot * 3;
+    st.c = mk(st.c.x * a[0] * w, st.c.y * a[1] * w, st.c.z * a[2] * w);
+    av.diffuse = true;
+  } else if (r <= m.m1.x) {
+    nd = reflect_ref(st.d, n);
+  } else if (r <= m.m1.y) {
+    nd = custom_refract_ref(st.d, n, m.m1.z);
+  }
+  st.v += 1;
+  float inv = 1.0f;
+  if (P.rr_depth != 0 && st.v >= P.rr_depth) {
+    if (U.u[3] >= P.rr_q) return kEndDark;
+    inv = 1.0f / P.rr_q;
+    st.c = mk(st.c.x * inv, st.c.y * inv, st.c.z * inv);
+  }
+  av.gq = w * inv;
+  st.o = vadd(p, vscale(0.01f, nd));
+  st.d = nd;
+  st.i += 1;
+  return (st.i < P.depth) ? kContinue : kEndDark;
+}
+
 // Primary ray through the pixel centre (path_tracer.cpp:19-23)
 SWR_HD f3 primary_dir(const float* vi, const float* pi, uint32_t px, uint32_t py, uint32_t W,
                       uint32_t H) {

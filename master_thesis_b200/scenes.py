@@ -143,6 +143,80 @@ def cornell(seed, root):
     return dict(scene=scene, camera=cam, basepath=base)
 
 
+def grid_quad_mesh(n):
+    """The unit square of quad_mesh (plane x = 0, y and z in [-1, 1], normal +x) as an n x n grid of
+    cells, two triangles each."""
+    t = np.linspace(-1.0, 1.0, n + 1)
+    zz, yy = np.meshgrid(t, t, indexing="ij")
+    pos = np.stack([np.zeros_like(yy), yy, zz], -1).reshape(-1, 3)
+    nrm = np.tile([1.0, 0.0, 0.0], (pos.shape[0], 1))
+    faces = []
+    for i in range(n):
+        for j in range(n):
+            a = i * (n + 1) + j
+            faces += [(a, a + 1, a + n + 2), (a, a + n + 2, a + n + 1)]
+    return pos, nrm, faces
+
+
+def grid_cube_mesh(m):
+    """Cube [-1, 1]^3 with every face an m x m grid (flat outward normals)."""
+    pos, nrm, faces = [], [], []
+    t = np.linspace(-1.0, 1.0, m + 1)
+    for axis in range(3):
+        for sgn in (-1.0, 1.0):
+            u, v = (axis + 1) % 3, (axis + 2) % 3
+            base = len(pos)
+            for i in range(m + 1):
+                for j in range(m + 1):
+                    p = [0.0, 0.0, 0.0]
+                    p[axis] = sgn
+                    p[u] = t[i]
+                    p[v] = t[j]
+                    n = [0.0, 0.0, 0.0]
+                    n[axis] = sgn
+                    pos.append(p)
+                    nrm.append(n)
+            for i in range(m):
+                for j in range(m):
+                    a = base + i * (m + 1) + j
+                    b, c, d = a + m + 1, a + m + 2, a + 1
+                    faces += [(a, b, c), (a, c, d)] if sgn > 0 else [(a, c, b), (a, d, c)]
+    return pos, nrm, faces
+
+
+def cornell_tessellated(seed, root, wall_cells=48, box_cells=33):
+    """Cornell-style scene with tessellated walls and boxes (about 49k triangles with the defaults)
+    and two emissive ceiling quads; for the differentiable configuration. Returns dict(scene,
+    camera, basepath, triangles)."""
+    rng = np.random.default_rng(seed)
+    base = _layout(root)
+    write_obj(os.path.join(root, "res/obj/wall.obj"), *grid_quad_mesh(wall_cells))
+    write_obj(os.path.join(root, "res/obj/box.obj"), *grid_cube_mesh(box_cells))
+    write_obj(os.path.join(root, "res/obj/quad.obj"), *quad_mesh())
+    hp = math.pi / 2
+    walls = [((-1, 0, 0), None), ((0, -1, 0), (0, 0, 1, hp)), ((0, 1, 0), (0, 0, 1, -hp)),
+             ((0, 0, -1), (0, 1, 0, -hp)), ((0, 0, 1), (0, 1, 0, hp))]
+    s = ""
+    for pos, rot in walls:
+        kw = dict(color=(0.7, 0.7, 0.7))
+        if rot is not None:
+            kw["rotation"] = rot
+        s += _entry("wall.obj", pos, **kw)
+    for z in (-0.35, 0.35):
+        s += _entry("quad.obj", (0.1, 0.99, z), scale=(0.15, 0.15, 0.15), rotation=(0, 0, 1, -hp),
+                    color=(1, 1, 1), lightSource=8.0)
+    for pos, sc in (((0.4, -0.7, -0.4), (0.3, 0.3, 0.3)), ((-0.4, -0.4, 0.4), (0.3, 0.6, 0.3))):
+        ang = math.radians(rng.uniform(0.0, 30.0))
+        s += _entry("box.obj", pos, scale=sc, rotation=(0, 1, 0, ang), color=(0.7, 0.7, 0.7))
+    scene = os.path.join(root, "res/scene/cornell_tess_%d.scene" % seed)
+    with open(scene, "w") as f:
+        f.write(s)
+    cam = os.path.join(root, "res/camera/cornell.camera")
+    write_camera(cam, (3.4, 0, 0), (1, 0), fov=40)
+    ntri = 5 * 2 * wall_cells ** 2 + 2 * 12 * box_cells ** 2 + 4
+    return dict(scene=scene, camera=cam, basepath=base, triangles=ntri)
+
+
 def fbm_heights(n, seed, octaves=6, hmax=0.2):
     """(n+1, n+1) heights in [0, hmax] from seeded value-noise fBm."""
     rng = np.random.default_rng(seed)
