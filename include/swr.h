@@ -148,6 +148,10 @@ void swr_host_scene_free(swr_host_scene* hs);
  * reference's fixed pi/4. */
 int swr_camera_load(const char* camera_path, uint32_t width, uint32_t height, uint32_t use_fov_key,
                     swr_camera* out);
+/* Camera from values instead of a file: the same result as a .camera file with
+ * position(x, y, z) angle(angle_theta, angle_phi) and, when fov_deg > 0, fov(fov_deg) honoured. */
+int swr_camera_make(const float position[3], float angle_theta, float angle_phi, float fov_deg,
+                    uint32_t width, uint32_t height, swr_camera* out);
 /* Renderer file (main.cpp:62-66, path_tracer.cpp:13-16): accepts PathTracer; returns its
  * visionJumpCount and raysPerPixel. */
 int swr_renderer_load(const char* renderer_path, uint32_t* max_depth, uint32_t* spp);
@@ -212,6 +216,32 @@ typedef struct swr_render_profile {
 /* As swr_render, filling *prof (which may be NULL). */
 int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                         float* rgb_out, float* samples_out, void* stream, swr_render_profile* prof);
+
+/* Batched rendering: many independent jobs (scene, camera, options, output) in one shared
+ * wavefront, so that small images do not leave the GPU idle (no counterpart in the reference,
+ * which renders one image per process). Per-job results match swr_render's for the same job up to
+ * the order of the per-pixel float sums (the batch sums in 64-bit fixed point). */
+typedef struct swr_batch swr_batch;
+typedef struct swr_batch_job {
+  swr_scene* scene;       /* built scene (jobs may share one) */
+  swr_camera cam;
+  swr_render_opts opts;   /* width, height, spp, max_depth, seed, mode, rr_*; tuning fields ignored */
+  float* rgb_out;         /* [height*width*3] device */
+} swr_batch_job;
+typedef struct swr_batch_opts {
+  uint32_t wave_size;     /* paths in flight, 0 = 2^23 */
+  uint32_t refill;        /* as in swr_render_opts, 0 = 8 */
+  uint32_t flags;         /* SWR_BATCH_* */
+  uint32_t reserved;
+} swr_batch_opts;
+#define SWR_BATCH_NO_GRAPH 1u /* launch the shade/trace rounds directly instead of from a CUDA graph */
+
+/* A batch context owns the shared wavefront buffers and the captured CUDA graph; reuse it across
+ * calls. One host thread at a time. */
+int swr_batch_create(swr_batch** out);
+void swr_batch_destroy(swr_batch* batch);
+int swr_render_batch(swr_batch* batch, const swr_batch_job* jobs, uint32_t num_jobs,
+                     const swr_batch_opts* opts, void* stream);
 
 /* Physical-mode parameters of a built scene (no rebuild): diffuse albedo per triangle
  * ([num_triangles*3], by global triangle id) and emitted radiance L_e per object ([num_objects*3];

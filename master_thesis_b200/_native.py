@@ -81,6 +81,17 @@ class RenderProfile(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("cam", Camera), ("opts", RenderOpts), ("rgb_out", ctypes.c_void_p)]
+
+
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("wave_size", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+BATCH_NO_GRAPH = 1
+
 P = ctypes.c_void_p
 U32 = ctypes.c_uint32
 U64 = ctypes.c_uint64
@@ -97,6 +108,8 @@ SIGNATURES = {
     "swr_host_scene_free": (None, [P]),
     "swr_camera_load": (I, [ctypes.c_char_p, U32, U32, U32, ctypes.POINTER(Camera)]),
     "swr_renderer_load": (I, [ctypes.c_char_p, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+    "swr_camera_make": (I, [ctypes.POINTER(ctypes.c_float), ctypes.c_float, ctypes.c_float, ctypes.c_float, U32,
+                            U32, ctypes.POINTER(Camera)]),
     "swr_scene_derive": (I, [ctypes.POINTER(SceneDesc), P, P, P, P, P]),
     "swr_scene_create": (I, [ctypes.POINTER(SceneDesc), ctypes.POINTER(BuildOpts), ctypes.POINTER(P)]),
     "swr_scene_destroy": (None, [P]),
@@ -107,6 +120,9 @@ SIGNATURES = {
     "swr_render_profiled": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P,
                                 ctypes.POINTER(RenderProfile)]),
     "swr_render_noalloc": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P]),
+    "swr_batch_create": (I, [ctypes.POINTER(P)]),
+    "swr_batch_destroy": (None, [P]),
+    "swr_render_batch": (I, [P, ctypes.POINTER(BatchJob), U32, ctypes.POINTER(BatchOpts), P]),
     "swr_scene_set_albedo": (I, [P, P, P]),
     "swr_scene_set_emission": (I, [P, P, P]),
     "swr_render_adjoint": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P, P]),

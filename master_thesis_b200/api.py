@@ -98,6 +98,14 @@ def load_camera(camera_path, width, height, use_fov_key=False):
     return c
 
 
+def make_camera(position, angle, width, height, fov_deg=0.0):
+    """Camera from values, as a .camera file with position(...) angle(theta, phi) [fov(deg)]."""
+    c = N.Camera()
+    p = (ctypes.c_float * 3)(*[float(x) for x in position])
+    check(N.lib.swr_camera_make(p, float(angle[0]), float(angle[1]), float(fov_deg), width, height, ctypes.byref(c)))
+    return c
+
+
 def camera_arrays(cam):
     return (np.array(cam.view_inv, np.float32).reshape(4, 4),
             np.array(cam.proj_inv, np.float32).reshape(4, 4),
@@ -218,6 +226,46 @@ def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=
 Scene.set_albedo = _scene_set_albedo
 Scene.set_emission = _scene_set_emission
 Scene.render_adjoint = _scene_render_adjoint
+
+
+class Batch:
+    """Batch context (shared wavefront buffers + captured CUDA graph), reused across calls."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        check(N.lib.swr_batch_create(ctypes.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib.swr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, jobs, wave_size=0, refill=0, use_graph=True, stream=None):
+        """jobs: list of dicts with scene, cam, width, height, spp, depth and optional seed, mode,
+        rr_depth, rr_survive, out (torch cuda tensor [h, w, 3]). Returns the output tensors."""
+        import torch
+        arr = (N.BatchJob * len(jobs))()
+        outs = []
+        for k, j in enumerate(jobs):
+            out = j.get("out")
+            if out is None:
+                out = torch.empty((j["height"], j["width"], 3), dtype=torch.float32, device="cuda")
+            outs.append(out)
+            arr[k].scene = j["scene"].handle
+            arr[k].cam = j["cam"]
+            arr[k].opts = N.RenderOpts(j["width"], j["height"], j["spp"], j["depth"], j.get("seed", 0),
+                                       j.get("mode", N.MODE_REFERENCE), j.get("rr_depth", 0),
+                                       j.get("rr_survive", 1.0), 0, 0, 0, 0, 0, 0)
+            arr[k].rgb_out = out.data_ptr()
+        o = N.BatchOpts(wave_size, refill, 0 if use_graph else N.BATCH_NO_GRAPH, 0)
+        check(N.lib.swr_render_batch(self._h, arr, len(jobs), ctypes.byref(o), _stream_handle(stream)))
+        return outs
 
 
 def quantize_rgb8(img):

@@ -1,0 +1,487 @@
+// Batched rendering of many independent scenes in one wavefront (C ABI: swr_batch_create /
+// swr_batch_destroy / swr_render_batch).
+//
+// All jobs share one path queue. A job = (scene, camera, image size, samples, depth, mode, seed,
+// output). Global sample indices run over the jobs back to back (prefix sums in the job table);
+// injection finds a sample's job by binary search, every path carries its job id, and the
+// traversal reads that job's scene. Samples use the same random-number keys as a single-scene
+// render of the job (pixel index within the job's image, sample index), so each job's paths are
+// exactly those of swr_render for it. Radiance is summed per pixel in 64-bit fixed point with
+// integer atomics (scale 2^32): order-independent, hence deterministic, and it needs 24 bytes per
+// pixel instead of 16 bytes per sample (a 256-scene batch has ~2e9 samples). The final per-pixel
+// scale is the single-scene one. The shade/trace rounds are captured once into a CUDA graph (eight
+// rounds per graph) that the host replays until the queue has drained.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "shading.cuh"
+#include "swr_internal.cuh"
+
+namespace swr {
+namespace {
+
+using swrx::f3;
+using swrx::mk;
+
+constexpr uint32_t kDead = 0xFFFFFFFFu;
+constexpr int kTB = 128;
+constexpr double kFix = 4294967296.0;  // 2^32
+
+struct BJob {
+  float vi[16], pi[16];
+  float org[3];
+  uint32_t W, H, spp, depth, mode, rr_depth;
+  float rr_q;
+  uint32_t scene;
+  uint64_t seed;
+  uint64_t sample_base;  // first global sample index of the job
+  uint64_t pixel_base;   // first global pixel index of the job
+  float* out;            // [H*W*3] device
+};
+
+struct BCtrl {
+  unsigned int count[2];
+  unsigned int cursor[2];
+  unsigned int inj_n[2];
+  unsigned int pad[2];
+  unsigned long long inj_base[2];
+  unsigned long long injected;
+  unsigned long long total;
+  unsigned long long rays;
+};
+
+struct BQueue {
+  float4* o;  // origin | pixel (within the job)
+  float4* d;  // direction | sample
+  float4* c;  // throughput | job << 16 | i << 8 | v
+  float4* l;  // physical radiance so far
+  uint2* hit;
+};
+
+struct BArgs {
+  const BJob* jobs;
+  const DevScene* scenes;
+  uint32_t njobs;
+  uint64_t npix;  // total pixels
+  uint32_t capacity, refill;
+  float4* cam;                  // [npix*2]
+  unsigned long long* accum;    // [npix*3] fixed point
+};
+
+__device__ __forceinline__ unsigned lane() { return threadIdx.x & 31u; }
+
+// index of the job whose [base, next base) range holds v (bases ascending, first is 0)
+__device__ __forceinline__ uint32_t find_job(const BJob* jobs, uint32_t n, uint64_t v, bool by_pixel) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const uint64_t b = by_pixel ? jobs[mid].pixel_base : jobs[mid].sample_base;
+    if (b <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kTB) k_bcamera(BArgs A, BCtrl* __restrict__ ctrl) {
+  __shared__ uint2 stack[swrx::kStackShared * kTB];
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned traced = 0;
+  if (p < A.npix) {
+    const uint32_t j = find_job(A.jobs, A.njobs, p, true);
+    const BJob& J = A.jobs[j];
+    const DevScene& sc = A.scenes[J.scene];
+    const uint32_t pix = (uint32_t)(p - J.pixel_base);
+    f3 o = mk(J.org[0], J.org[1], J.org[2]);
+    const f3 d = swrx::primary_dir(J.vi, J.pi, pix % J.W, pix / J.W, J.W, J.H);
+    float4 r0 = make_float4(0, 0, 0, 0), r1 = make_float4(0, 0, 0, __uint_as_float(kDead));
+    for (uint32_t i = 0; i < J.depth; ++i) {
+      swrx::Hit h;
+      ++traced;
+      if (!swrx::trace_closest<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, o, d, stack + threadIdx.x,
+                                      kTB, h, nullptr))
+        break;
+      const f3 hp = swrx::hit_point(o, d, h.t);
+      const f3 n = swrx::shading_normal(sc.tris, sc.shade, h.slot, hp);
+      if (swrx::vdot(n, d) > 0.0f) {
+        o = swrx::vadd(hp, swrx::vscale(0.01f, d));
+        continue;
+      }
+      r0 = make_float4(o.x, o.y, o.z, h.t);
+      r1 = make_float4(d.x, d.y, d.z, __uint_as_float(h.slot | (i << 27)));
+      break;
+    }
+    A.cam[2 * p] = r0;
+    A.cam[2 * p + 1] = r1;
+  }
+  for (int off = 16; off > 0; off >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, off);
+  if (lane() == 0 && traced) atomicAdd(&ctrl->rays, (unsigned long long)traced);
+}
+
+__device__ __forceinline__ void accumulate(unsigned long long* acc, float r, float g, float b) {
+  atomicAdd(acc + 0, (unsigned long long)__double2ll_rn((double)r * kFix));
+  atomicAdd(acc + 1, (unsigned long long)__double2ll_rn((double)g * kFix));
+  atomicAdd(acc + 2, (unsigned long long)__double2ll_rn((double)b * kFix));
+}
+
+__global__ void __launch_bounds__(256) k_bshade(BArgs A, BCtrl* __restrict__ ctrl, BQueue in, BQueue out,
+                                                int parity) {
+  const uint32_t n_in = ctrl->count[parity];
+  const uint32_t n_inj = ctrl->inj_n[parity];
+  const unsigned long long inj_base = ctrl->inj_base[parity];
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
+  const uint32_t i = blockIdx.x * 256 + threadIdx.x;
+  if (blockIdx.x * 256 >= n_in + n_inj) return;
+  bool live = false, have = false;
+  swrx::PathState st;
+  uint32_t pixel = 0, sample = 0, job = 0, slot = kDead;
+  float t = 0.0f;
+  if (i < n_in) {
+    const float4 qo = in.o[i], qd = in.d[i], qc = in.c[i];
+    const uint2 h = in.hit[i];
+    pixel = __float_as_uint(qo.w);
+    sample = __float_as_uint(qd.w);
+    const uint32_t meta = __float_as_uint(qc.w);
+    job = meta >> 16;
+    st.o = mk(qo.x, qo.y, qo.z);
+    st.d = mk(qd.x, qd.y, qd.z);
+    st.c = mk(qc.x, qc.y, qc.z);
+    st.i = (meta >> 8) & 0xFFu;
+    st.v = meta & 0xFFu;
+    const float4 ql = in.l[i];
+    st.L = mk(ql.x, ql.y, ql.z);
+    slot = h.x;
+    t = __uint_as_float(h.y);
+    have = true;
+  } else if (i < n_in + n_inj) {
+    const unsigned long long g = inj_base + (i - n_in);
+    job = find_job(A.jobs, A.njobs, g, false);
+    const BJob& J = A.jobs[job];
+    const uint64_t local = g - J.sample_base;
+    pixel = (uint32_t)(local / J.spp);
+    sample = (uint32_t)(local % J.spp);
+    const uint64_t p = J.pixel_base + pixel;
+    const float4 r0 = A.cam[2 * p], r1 = A.cam[2 * p + 1];
+    const uint32_t bits = __float_as_uint(r1.w);
+    st.c = mk(1.0f, 1.0f, 1.0f);
+    st.L = mk(0.0f, 0.0f, 0.0f);
+    st.v = 0;
+    st.i = 0;
+    if (bits != kDead) {
+      st.o = mk(r0.x, r0.y, r0.z);
+      st.d = mk(r1.x, r1.y, r1.z);
+      st.i = bits >> 27;
+      slot = bits & 0x07FFFFFFu;
+      t = r0.w;
+    }
+    have = true;
+  }
+  if (have) {
+    const BJob& J = A.jobs[job];
+    uint32_t outcome = swrx::kEndDark;
+    if (slot != kDead) {
+      const DevScene& sc = A.scenes[J.scene];
+      swrx::ShadeParams P;
+      P.seed = J.seed;
+      P.pixel = pixel;
+      P.sample = sample;
+      P.depth = J.depth;
+      P.mode = J.mode;
+      P.rr_depth = J.rr_depth;
+      P.rr_q = J.rr_q;
+      outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
+    }
+    if (outcome == swrx::kContinue) {
+      live = true;
+    } else {
+      unsigned long long* acc = A.accum + 3 * (J.pixel_base + pixel);
+      if (J.mode == 0) {
+        if (outcome == swrx::kEndLight) accumulate(acc, st.c.x, st.c.y, st.c.z);
+      } else {
+        accumulate(acc, st.L.x, st.L.y, st.L.z);
+      }
+    }
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, live);
+  if (mask == 0u) return;
+  unsigned base = 0;
+  const unsigned leader = __ffs(mask) - 1;
+  if (lane() == leader) base = atomicAdd(&ctrl->count[parity ^ 1], (unsigned)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (live) {
+    const unsigned j = base + __popc(mask & ((1u << lane()) - 1u));
+    out.o[j] = make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel));
+    out.d[j] = make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample));
+    out.c[j] = make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((job << 16) | (st.i << 8) | st.v));
+    out.l[j] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+  }
+}
+
+// bounce traversal over the shared queue, refilling idle lanes (as the single-scene kernel)
+__global__ void __launch_bounds__(kTB) k_btrace(BArgs A, BCtrl* __restrict__ ctrl, BQueue q, int parity) {
+  __shared__ uint2 stack[swrx::kStackShared * kTB];
+  const int qp = parity ^ 1;
+  const unsigned n = ctrl->count[qp];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long rem = ctrl->total - ctrl->injected;
+    const unsigned long long room = (unsigned long long)A.capacity - n;
+    const unsigned long long m = rem < room ? rem : room;
+    ctrl->inj_base[qp] = ctrl->injected;
+    ctrl->inj_n[qp] = (unsigned)m;
+    ctrl->injected += m;
+    ctrl->count[parity] = 0u;
+    ctrl->rays += n;
+  }
+  const unsigned ln = lane();
+  const unsigned lt = (1u << ln) - 1u;
+  swrx::Traversal tr;
+  const DevScene* sc = nullptr;
+  bool active = false, exhausted = false;
+  unsigned ray = 0;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= A.refill) {
+      unsigned base = 0;
+      if (ln == 0) base = atomicAdd(&ctrl->cursor[qp], (unsigned)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) exhausted = true;
+      if (!active) {
+        const unsigned j = base + __popc(idle & lt);
+        if (j < n) {
+          const float4 o = q.o[j], d = q.d[j];
+          const uint32_t job = __float_as_uint(q.c[j].w) >> 16;
+          sc = &A.scenes[A.jobs[job].scene];
+          tr.init(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), stack + threadIdx.x, kTB);
+          ray = j;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active && tr.step<false, false>(sc->nodes, sc->tris, sc->tri_boxes, sc->obj_boxes, nullptr)) {
+      q.hit[ray] = make_uint2(tr.hit.slot, __float_as_uint(tr.hit.t));
+      active = false;
+    }
+  }
+}
+
+__global__ void k_bresolve(BArgs A) {
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.npix) return;
+  const uint32_t j = find_job(A.jobs, A.njobs, p, true);
+  const BJob& J = A.jobs[j];
+  const float inv = __fdiv_rn(1.0f, (float)J.spp);
+  const double s = (J.mode == 0) ? __dmul_rn(6.283185307179586, (double)inv) : (double)inv;
+  const unsigned long long* acc = A.accum + 3 * p;
+  float* o = J.out + (size_t)(p - J.pixel_base) * 3;
+  for (int k = 0; k < 3; ++k)
+    o[k] = __double2float_rn((double)(long long)acc[k] / kFix * s);
+}
+
+int ensure_bytes(void** p, size_t& have, size_t want) {
+  if (have >= want && *p) return SWR_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  have = 0;
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(want, 256));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(SWR_ERR_ALLOC, "CUDA: batch workspace allocation of " + std::to_string(want) + " bytes failed");
+  }
+  have = want;
+  return SWR_OK;
+}
+
+}  // namespace
+}  // namespace swr
+
+struct swr_batch {
+  void *qbuf = nullptr, *cam = nullptr, *accum = nullptr, *jobs = nullptr, *scenes = nullptr, *ctrl = nullptr;
+  size_t qbytes = 0, cambytes = 0, accbytes = 0, jobbytes = 0, scenebytes = 0, ctrlbytes = 0;
+  swr::BCtrl* host_ctrl = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<char> graph_key;
+  int device = -1;
+};
+
+using swr::set_error;
+
+extern "C" {
+
+int swr_batch_create(swr_batch** out) {
+  if (!out) return set_error(SWR_ERR_INVALID, "swr: null output handle");
+  std::unique_ptr<swr_batch> b(new swr_batch());
+  SWR_CUDA(cudaGetDevice(&b->device));
+  SWR_CUDA(cudaMallocHost(&b->host_ctrl, sizeof(swr::BCtrl)));
+  *out = b.release();
+  return SWR_OK;
+}
+
+void swr_batch_destroy(swr_batch* b) {
+  if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (void* p : {b->qbuf, b->cam, b->accum, b->jobs, b->scenes, b->ctrl})
+    if (p) cudaFree(p);
+  if (b->host_ctrl) cudaFreeHost(b->host_ctrl);
+  delete b;
+}
+
+int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const swr_batch_opts* bo,
+                     void* stream_) {
+  using namespace swr;
+  if (!b || !jobs || n == 0) return set_error(SWR_ERR_INVALID, "swr: empty batch");
+  if (n > 65535) return set_error(SWR_ERR_UNSUPPORTED, "swr: at most 65535 jobs per batch");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(b->device));
+  std::vector<BJob> hj(n);
+  std::vector<DevScene> hs;
+  std::vector<const swr_scene*> uniq;
+  uint64_t samples = 0, pixels = 0;
+  int num_sms = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    const swr_batch_job& J = jobs[k];
+    const swr_render_opts& o = J.opts;
+    if (!J.scene || !J.rgb_out) return set_error(SWR_ERR_INVALID, "swr: batch job without scene or output");
+    if (J.scene->device != b->device) return set_error(SWR_ERR_INVALID, "swr: batch jobs on another device");
+    if (o.width == 0 || o.height == 0 || o.spp == 0) return set_error(SWR_ERR_INVALID, "swr: zero image size");
+    if (o.max_depth == 0 || o.max_depth > 31) return set_error(SWR_ERR_INVALID, "swr: max_depth must be 1..31");
+    if (o.mode > 1) return set_error(SWR_ERR_INVALID, "swr: unknown mode");
+    if (o.mode == 1 && o.rr_depth && !(o.rr_survive > 0.0f && o.rr_survive <= 1.0f))
+      return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+    if (is_host_pointer(J.rgb_out)) return set_error(SWR_ERR_INVALID, "swr: batch outputs must be device memory");
+    uint32_t si = 0;
+    while (si < uniq.size() && uniq[si] != J.scene) ++si;
+    if (si == uniq.size()) {
+      uniq.push_back(J.scene);
+      hs.push_back(J.scene->dev);
+    }
+    num_sms = J.scene->num_sms;
+    BJob& d = hj[k];
+    std::memcpy(d.vi, J.cam.view_inv, sizeof(d.vi));
+    std::memcpy(d.pi, J.cam.proj_inv, sizeof(d.pi));
+    std::memcpy(d.org, J.cam.origin, sizeof(d.org));
+    d.W = o.width;
+    d.H = o.height;
+    d.spp = o.spp;
+    d.depth = o.max_depth;
+    d.mode = o.mode;
+    d.rr_depth = o.mode == 1 ? o.rr_depth : 0;
+    d.rr_q = (o.mode == 1 && o.rr_depth) ? o.rr_survive : 1.0f;
+    d.scene = si;
+    d.seed = o.seed;
+    d.sample_base = samples;
+    d.pixel_base = pixels;
+    d.out = J.rgb_out;
+    const uint64_t np = (uint64_t)o.width * o.height;
+    pixels += np;
+    samples += np * o.spp;
+  }
+  uint32_t cap = (bo && bo->wave_size) ? bo->wave_size : (1u << 23);
+  cap = (uint32_t)std::min<uint64_t>(cap, samples);
+  cap = std::max<uint32_t>(32, (cap + 255u) & ~255u);
+  const uint32_t refill = (bo && bo->refill) ? bo->refill : 8;
+  if (refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  int rc;
+  if ((rc = ensure_bytes(&b->qbuf, b->qbytes, (size_t)cap * (4 * sizeof(float4) + sizeof(uint2)) * 2))) return rc;
+  if ((rc = ensure_bytes(&b->cam, b->cambytes, pixels * 2 * sizeof(float4)))) return rc;
+  if ((rc = ensure_bytes(&b->accum, b->accbytes, pixels * 3 * sizeof(unsigned long long)))) return rc;
+  if ((rc = ensure_bytes(&b->jobs, b->jobbytes, n * sizeof(BJob)))) return rc;
+  if ((rc = ensure_bytes(&b->scenes, b->scenebytes, hs.size() * sizeof(DevScene)))) return rc;
+  if ((rc = ensure_bytes(&b->ctrl, b->ctrlbytes, sizeof(BCtrl)))) return rc;
+  SWR_CUDA(cudaMemcpyAsync(b->jobs, hj.data(), n * sizeof(BJob), cudaMemcpyHostToDevice, stream));
+  SWR_CUDA(cudaMemcpyAsync(b->scenes, hs.data(), hs.size() * sizeof(DevScene), cudaMemcpyHostToDevice, stream));
+  SWR_CUDA(cudaMemsetAsync(b->accum, 0, pixels * 3 * sizeof(unsigned long long), stream));
+  BQueue Q[2];
+  {
+    char* p = (char*)b->qbuf;
+    for (int k = 0; k < 2; ++k) {
+      Q[k].o = (float4*)p; p += (size_t)cap * sizeof(float4);
+      Q[k].d = (float4*)p; p += (size_t)cap * sizeof(float4);
+      Q[k].c = (float4*)p; p += (size_t)cap * sizeof(float4);
+      Q[k].l = (float4*)p; p += (size_t)cap * sizeof(float4);
+      Q[k].hit = (uint2*)p; p += (size_t)cap * sizeof(uint2);
+    }
+  }
+  BArgs A;
+  A.jobs = (const BJob*)b->jobs;
+  A.scenes = (const DevScene*)b->scenes;
+  A.njobs = n;
+  A.npix = pixels;
+  A.capacity = cap;
+  A.refill = refill;
+  A.cam = (float4*)b->cam;
+  A.accum = (unsigned long long*)b->accum;
+  BCtrl init;
+  std::memset(&init, 0, sizeof(init));
+  init.total = samples;
+  init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, samples);
+  init.injected = init.inj_n[0];
+  SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
+  *b->host_ctrl = init;
+  SWR_CUDA(cudaMemcpyAsync(b->ctrl, b->host_ctrl, sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
+  k_bcamera<<<(unsigned)((pixels + kTB - 1) / kTB), kTB, 0, stream>>>(A, (BCtrl*)b->ctrl);
+  SWR_CUDA(cudaGetLastError());
+  int per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_btrace, kTB, 0));
+  const unsigned tgrid = (unsigned)(num_sms * std::max(per_sm, 1));
+  const unsigned sgrid = (cap + 255) / 256;
+  const bool use_graph = !(bo && (bo->flags & SWR_BATCH_NO_GRAPH));
+  auto enqueue_rounds = [&](cudaStream_t st) {
+    for (int k = 0; k < 8; ++k) {
+      const int p = k & 1;
+      k_bshade<<<sgrid, 256, 0, st>>>(A, (BCtrl*)b->ctrl, Q[p], Q[p ^ 1], p);
+      k_btrace<<<tgrid, kTB, 0, st>>>(A, (BCtrl*)b->ctrl, Q[p ^ 1], p);
+    }
+  };
+  if (use_graph) {
+    // the eight-round chunk as one graph, rebuilt whenever an argument baked into it changes
+    std::vector<char> key(sizeof(A) + sizeof(Q) + 3 * sizeof(void*));
+    {
+      char* k = key.data();
+      std::memset(k, 0, key.size());
+      std::memcpy(k, &A, sizeof(A));
+      std::memcpy(k + sizeof(A), Q, sizeof(Q));
+      const void* extra[3] = {b->ctrl, (void*)(uintptr_t)sgrid, (void*)(uintptr_t)tgrid};
+      std::memcpy(k + sizeof(A) + sizeof(Q), extra, sizeof(extra));
+    }
+    if (!b->graph || key != b->graph_key) {
+      if (b->graph) cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+      cudaStream_t cs;
+      SWR_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      SWR_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      enqueue_rounds(cs);
+      SWR_CUDA(cudaStreamEndCapture(cs, &g));
+      SWR_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
+      cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      b->graph_key = key;
+    }
+  }
+  uint64_t rounds = 0;
+  uint32_t maxdepth = 0;
+  for (uint32_t k = 0; k < n; ++k) maxdepth = std::max(maxdepth, jobs[k].opts.max_depth);
+  const uint64_t max_rounds = (samples / cap + 2) * (uint64_t)(maxdepth + 2) + 64;
+  for (;;) {
+    if (rounds > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
+    if (use_graph) SWR_CUDA(cudaGraphLaunch(b->graph, stream));
+    else enqueue_rounds(stream);
+    rounds += 8;
+    SWR_CUDA(cudaGetLastError());
+    SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, b->ctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
+    SWR_CUDA(cudaStreamSynchronize(stream));
+    const BCtrl& h = *b->host_ctrl;
+    // after an even number of rounds the next shade reads parity 0
+    if (h.count[0] == 0 && h.inj_n[0] == 0 && h.injected == h.total) break;
+  }
+  k_bresolve<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(A);
+  SWR_CUDA(cudaGetLastError());
+  return SWR_OK;
+}
+
+}  // extern "C"

@@ -105,6 +105,36 @@ int swr_camera_load(const char* camera_path, uint32_t width, uint32_t height, ui
   }
 }
 
+int swr_camera_make(const float position[3], float angle_theta, float angle_phi, float fov_deg,
+                    uint32_t width, uint32_t height, swr_camera* out) {
+  if (!position || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (width == 0 || height == 0) return set_error(SWR_ERR_INVALID, "swr: zero image size");
+  try {
+    // the same entry a .camera file produces: position(x, y, z) angle(theta, phi) [fov(deg)]
+    swr::InputEntry e("Camera");
+    auto str = [](float v) {
+      char b[64];
+      std::snprintf(b, sizeof(b), "%.9g", (double)v);
+      return std::string(b);
+    };
+    e.insert("position", {str(position[0]), str(position[1]), str(position[2])});
+    e.insert("angle", {str(angle_theta), str(angle_phi)});
+    if (fov_deg > 0.0f) e.insert("fov", {str(fov_deg)});
+    swr::CameraParams c = swr::parse_camera(e);
+    swr::CameraFrame f = swr::camera_frame(c, width, height, fov_deg > 0.0f);
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) {
+        out->view_inv[i * 4 + j] = f.view_inv.m[i][j];
+        out->proj_inv[i * 4 + j] = f.proj_inv.m[i][j];
+      }
+    for (int k = 0; k < 3; ++k) out->origin[k] = f.origin[k];
+    out->reserved = 0.0f;
+    return SWR_OK;
+  } catch (const std::exception& ex) {
+    return set_error(SWR_ERR_INVALID, std::string("swr: ") + ex.what());
+  }
+}
+
 int swr_renderer_load(const char* renderer_path, uint32_t* max_depth, uint32_t* spp) {
   if (!renderer_path) return set_error(SWR_ERR_INVALID, "swr: null argument");
   try {

@@ -13,6 +13,7 @@ Scenes (shapes and sizes of the benchmark configurations):
                  [0, 0.2]) split into OBJ tiles, icospheres of subdivision 4 with log-uniform radii
                  in [0.01, 0.1] and albedo in [0.1, 0.9]^3, and emissive quads.
 """
+import functools
 import math
 import os
 
@@ -68,6 +69,12 @@ def cube_mesh():
 
 
 def icosphere_mesh(subdiv):
+    pos, nrm, faces = _icosphere(subdiv)
+    return pos.copy(), nrm.copy(), list(faces)
+
+
+@functools.lru_cache(maxsize=None)
+def _icosphere(subdiv):
     t = (1.0 + math.sqrt(5.0)) / 2.0
     verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t),
              (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
@@ -91,7 +98,7 @@ def icosphere_mesh(subdiv):
             nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
         faces = nf
     pos = np.array(verts, np.float32)
-    return pos, pos.copy(), faces
+    return pos, pos.copy(), tuple(faces)
 
 
 def _layout(root):
@@ -215,6 +222,87 @@ def cornell_tessellated(seed, root, wall_cells=48, box_cells=33):
     write_camera(cam, (3.4, 0, 0), (1, 0), fov=40)
     ntri = 5 * 2 * wall_cells ** 2 + 2 * 12 * box_cells ** 2 + 4
     return dict(scene=scene, camera=cam, basepath=base, triangles=ntri)
+
+
+def _vertex_normals(pos, faces):
+    p = np.asarray(pos, np.float64)
+    f = np.asarray(faces, np.int64)
+    fn = np.cross(p[f[:, 1]] - p[f[:, 0]], p[f[:, 2]] - p[f[:, 0]])
+    n = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(n, f[:, k], fn)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    return n
+
+
+def random_scene(seed, target_tris):
+    """World-space scene of about target_tris triangles built in memory: a ground quad, an emissive
+    quad above, and seeded displaced icospheres and stacks of boxes. Returns (SceneData, camera
+    dict(position, angle)) for the batched configuration."""
+    from .api import MAT_DTYPE, SceneData
+    rng = np.random.default_rng(seed)
+    objs = []  # (pos, nrm, faces, albedo, light_strength)
+    g = 4.0
+    objs.append((np.array([(-g, 0, -g), (g, 0, -g), (g, 0, g), (-g, 0, g)], np.float64),
+                 np.tile([0.0, 1.0, 0.0], (4, 1)), [(0, 2, 1), (0, 3, 2)], rng.uniform(0.3, 0.8, 3), 0.0))
+    objs.append((np.array([(-0.6, 2.5, -0.6), (0.6, 2.5, -0.6), (0.6, 2.5, 0.6), (-0.6, 2.5, 0.6)], np.float64),
+                 np.tile([0.0, -1.0, 0.0], (4, 1)), [(0, 1, 2), (0, 2, 3)], np.ones(3), 12.0))
+    remaining = max(0, int(target_tris) - 4)
+    while remaining >= 80:
+        s = 1
+        while 20 * 4 ** (s + 1) <= remaining and s < 7:
+            s += 1
+        p, _, f = icosphere_mesh(s)
+        p = p.astype(np.float64)
+        # displacement: a few seeded sinusoids of the direction
+        k = rng.normal(size=(4, 3)) * 3.0
+        ph = rng.uniform(0, 2 * np.pi, 4)
+        disp = 1.0 + 0.15 * np.sum(np.sin(p @ k.T + ph), axis=1) / 4.0
+        r = rng.uniform(0.15, 0.6)
+        c = np.array([rng.uniform(-2.5, 2.5), 0.0, rng.uniform(-2.5, 2.5)])
+        c[1] = r * 1.2
+        pos = p * (disp * r)[:, None] + c
+        objs.append((pos, _vertex_normals(pos, f), f, rng.uniform(0.1, 0.9, 3), 0.0))
+        remaining -= len(f)
+    cp, cn, cf = cube_mesh()
+    cp, cn = np.asarray(cp, np.float64), np.asarray(cn, np.float64)
+    while remaining >= 12:
+        n_box = min(remaining // 12, int(rng.integers(2, 8)))
+        base = np.array([rng.uniform(-3, 3), 0.0, rng.uniform(-3, 3)])
+        y = 0.0
+        for _ in range(n_box):
+            hs = rng.uniform(0.05, 0.25, 3)
+            ang = rng.uniform(0, np.pi)
+            rot = np.array([[np.cos(ang), 0, np.sin(ang)], [0, 1, 0], [-np.sin(ang), 0, np.cos(ang)]])
+            pos = (cp * hs) @ rot.T + base + np.array([0, y + hs[1], 0])
+            objs.append((pos, cn @ rot.T, cf, rng.uniform(0.1, 0.9, 3), 0.0))
+            y += 2 * hs[1]
+            remaining -= 12
+    vpos, vnrm, tri, tobj, ofv = [], [], [], [], [0]
+    mats = np.zeros(len(objs), MAT_DTYPE)
+    nv = 0
+    for o, (p, n, f, alb, le) in enumerate(objs):
+        vpos.append(np.asarray(p, np.float32))
+        vnrm.append(np.asarray(n, np.float32))
+        tri.append(np.asarray(f, np.int64) + nv)
+        tobj.append(np.full(len(f), o, np.uint32))
+        nv += len(p)
+        ofv.append(nv)
+        mats[o]["color"] = alb
+        mats[o]["diffuse_t"] = mats[o]["reflect_t"] = mats[o]["transparent_t"] = 1.0
+        mats[o]["refraction_index"] = 1.0
+        mats[o]["light_source"] = 1 if le > 0 else 0
+        mats[o]["light_strength"] = le
+    sd = SceneData(np.concatenate(vpos), np.concatenate(vnrm), np.concatenate(tri), np.concatenate(tobj),
+                   np.array(ofv, np.uint32), mats)
+    az = rng.uniform(-np.pi, np.pi)
+    el = rng.uniform(np.radians(20), np.radians(40))
+    dist = 6.5
+    pos = np.array([dist * np.cos(el) * np.cos(az), dist * np.sin(el), dist * np.cos(el) * np.sin(az)])
+    d = -pos / np.linalg.norm(pos)
+    theta, phi = np.arctan2(d[2], d[0]), np.arccos(d[1])
+    cam = dict(position=pos.tolist(), angle=(float(theta / np.pi), float((np.pi / 2 - phi) / (np.pi / 2))))
+    return sd, cam
 
 
 def fbm_heights(n, seed, octaves=6, hmax=0.2):
