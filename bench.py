@@ -38,6 +38,10 @@ CONFIGS = {
     # the terrain scene at a reduced image size, for profiler captures of single kernel launches
     "c2s": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=16,
                 depth=8, seed=2024),
+    # batched: 256 scenes, 1k-500k triangles (log-uniform), image sides {64..1024}, spp {4,16,64}, depth 6
+    "c3": dict(kind="batch", scenes=256, depth=6, seed=7),
+    # differentiable: tessellated Cornell (~49k triangles), 512x512, 32 spp primal + 32 spp adjoint, depth 6
+    "c4": dict(kind="diff", W=512, H=512, spp=32, depth=6, seed=11),
 }
 METRIC = "Msamples/s (camera paths per second)"
 
@@ -145,6 +149,108 @@ def cpu_reference(cfg, files, threads, budget_s, impl_bin):
     return res
 
 
+def _events_ms(fn, steps, flush):
+    import torch
+    total = 0.0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total / steps
+
+
+def run_batch(args, cfg):
+    """C3: all scenes in one batched wavefront vs one single-scene render call per scene."""
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import autotune, scenes
+    rng = np.random.default_rng(cfg["seed"])
+    jobs, t0 = [], time.time()
+    tris = 0
+    for k in range(cfg["scenes"]):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+        side = int(rng.choice([64, 128, 256, 512, 1024]))
+        spp = int(rng.choice([4, 16, 64]))
+        sd, cam = scenes.random_scene(cfg["seed"] * 100003 + k, n)
+        sc = swr.Scene(sd)
+        tris += sd.num_triangles
+        jobs.append(dict(scene=sc, cam=swr.make_camera(cam["position"], cam["angle"], side, side, fov_deg=40),
+                         width=side, height=side, spp=spp, depth=cfg["depth"], seed=k, mode=swr.MODE_PHYSICAL))
+    setup_s = time.time() - t0
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    outs = [torch.empty((j["height"], j["width"], 3), dtype=torch.float32, device="cuda") for j in jobs]
+    jobs = [dict(j, out=o) for j, o in zip(jobs, outs)]
+    batch = swr.Batch()
+    tuned = autotune.tune_batch(batch, jobs) if args.tune else {}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(args.warmup, 3)):
+        batch.render(jobs, **tuned)
+    b_ms = _events_ms(lambda: batch.render(jobs, **tuned), args.steps, flush)
+    batched = [o.clone() for o in outs]
+
+    def per_scene():
+        for j in jobs:
+            j["scene"].render(j["cam"], j["width"], j["height"], j["spp"], j["depth"], seed=j["seed"], mode=j["mode"],
+                              out=j["out"])
+    per_scene()
+    s_ms = _events_ms(per_scene, args.steps, flush)
+    diff = max(float((a - b).abs().max() / b.abs().max().clamp_min(1e-12)) for a, b in zip(batched, outs))
+    print(json.dumps({
+        "metric": "Msamples/s (batched, %d scenes)" % len(jobs), "value": samples / (b_ms / 1e3) / 1e6,
+        "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded in-memory scenes)",
+        "config": {"workload": "%d scenes, %d triangles, %d samples, depth %d, physical mode" %
+                   (len(jobs), tris, samples, cfg["depth"]), "tuned": tuned},
+        "per_scene_launches": {"value": samples / (s_ms / 1e3) / 1e6, "ms_per_step": s_ms},
+        "speedup_vs_per_scene": s_ms / b_ms, "max_rel_image_diff_vs_per_scene": diff, "setup_s": setup_s}))
+
+
+def run_diff(args, cfg):
+    """C4: physical-mode primal render vs the path-replay adjoint of an L2 image loss."""
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import scenes
+    tmp = args.scene_dir or tempfile.mkdtemp(prefix="swr_bench_c4_")
+    s = scenes.cornell_tessellated(cfg["seed"], tmp)
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    sc = swr.Scene(sd)
+    W, H, spp, depth = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
+    cam = swr.load_camera(s["camera"], W, H, use_fov_key=True)
+    rng = np.random.default_rng(cfg["seed"])
+    hidden = torch.from_numpy(rng.uniform(0.1, 0.9, (sd.num_triangles, 3)).astype(np.float32)).cuda()
+    guess = torch.from_numpy(rng.uniform(0.1, 0.9, (sd.num_triangles, 3)).astype(np.float32)).cuda()
+    sc.set_albedo(hidden)
+    target = sc.render(cam, W, H, spp, depth, seed=99, mode=swr.MODE_PHYSICAL)
+    sc.set_albedo(guess)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+
+    def primal():
+        sc.render(cam, W, H, spp, depth, seed=1, mode=swr.MODE_PHYSICAL, out=out)
+    for _ in range(max(args.warmup, 3)):
+        primal()
+    p_ms = _events_ms(primal, args.steps, flush)
+    dl = (2.0 * (out - target) / out.numel()).contiguous()
+
+    def adjoint():
+        sc.render_adjoint(cam, W, H, spp, depth, dl, seed=1)
+    for _ in range(max(args.warmup, 3)):
+        adjoint()
+    a_ms = _events_ms(adjoint, args.steps, flush)
+    print(json.dumps({
+        "metric": "Msamples/s (physical primal)", "value": W * H * spp / (p_ms / 1e3) / 1e6, "unit": "Msamples/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": p_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
+        "config": {"workload": "tessellated cornell %d triangles, %dx%d, %d spp, depth %d" %
+                   (sd.num_triangles, W, H, spp, depth)},
+        "adjoint_ms": a_ms, "adjoint_over_primal": a_ms / p_ms}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -155,8 +261,18 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scene-dir", default=None)
+    ap.add_argument("--tune", action="store_true", help="autotune the launch shape (cached) before timing")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if cfg["kind"] in ("batch", "diff"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or differentiable "
+                                                                  "renderer"}))
+            return
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        (run_batch if cfg["kind"] == "batch" else run_diff)(args, cfg)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -1,0 +1,93 @@
+"""Autotuner for the wavefront's launch shape.
+
+For a workload it times a small grid of the tunable knobs - paths in flight (wave size), the
+idle-lane refill threshold of the traversal, the shading block size and the traversal's register
+budget (for single-scene renders) - with CUDA events, keeps the fastest, and caches the choice in a
+JSON file keyed by the workload's shape and the GPU name. (The BVH node width is fixed at 8 in this
+build; the leaf size and the SAH leaf cost are build options measured separately.)
+
+    cfg = tune_render(scene, cam, width, height, spp, depth, mode=...)   # -> dict of render kwargs
+    cfg = tune_batch(batch, jobs)                                        # -> dict of batch kwargs
+"""
+import itertools
+import json
+import os
+import time
+
+import torch
+
+CACHE = os.environ.get("SWR_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "swr_b200", "tune.json"))
+
+RENDER_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23], refill=[4, 8, 16], block_size=[256], trace_blocks=[0])
+BATCH_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23], refill=[4, 8, 16])
+
+
+def _load():
+    try:
+        with open(CACHE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(db):
+    os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+    tmp = CACHE + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(db, f, indent=1, sort_keys=True)
+    os.replace(tmp, CACHE)
+
+
+def _time(fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def _search(key, grid, run, reps, force):
+    db = _load()
+    if key in db and not force:
+        return db[key]["best"]
+    names = sorted(grid)
+    results = []
+    for values in itertools.product(*[grid[n] for n in names]):
+        cfg = dict(zip(names, values))
+        results.append((_time(lambda: run(cfg), reps), cfg))
+    results.sort(key=lambda r: r[0])
+    db[key] = {"best": results[0][1], "ms": results[0][0], "tried": [[ms, c] for ms, c in results],
+               "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+    _store(db)
+    return results[0][1]
+
+
+def tune_render(scene, cam, width, height, spp, depth, mode=0, rr_depth=0, rr_survive=1.0, reps=2, force=False,
+                grid=None):
+    st = scene.stats()
+    key = "render|%s|tris=%d|px=%d|spp=%d|depth=%d|mode=%d" % (torch.cuda.get_device_name(), st["triangles"],
+                                                              width * height, spp, depth, mode)
+    out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+
+    def run(cfg):
+        scene.render(cam, width, height, spp, depth, mode=mode, rr_depth=rr_depth, rr_survive=rr_survive, out=out,
+                     **cfg)
+    return _search(key, grid or RENDER_GRID, run, reps, force)
+
+
+def tune_batch(batch, jobs, reps=1, force=False, grid=None):
+    tris = sum(j["scene"].stats()["triangles"] for j in jobs)
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    key = "batch|%s|jobs=%d|tris=%d|samples=%d" % (torch.cuda.get_device_name(), len(jobs), tris, samples)
+    outs = [torch.empty((j["height"], j["width"], 3), dtype=torch.float32, device="cuda") for j in jobs]
+    jj = [dict(j, out=o) for j, o in zip(jobs, outs)]
+
+    def run(cfg):
+        batch.render(jj, **cfg)
+    return _search(key, grid or BATCH_GRID, run, reps, force)

@@ -1,0 +1,40 @@
+"""Autotuner: the grid search keeps the fastest configuration and caches it per workload key."""
+import json
+
+import pytest
+
+from master_thesis_b200 import autotune
+
+
+def test_search_picks_fastest_and_caches(tmp_path, monkeypatch):
+    monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tune.json"))
+    cost = {(1, 4): 3.0, (1, 8): 1.0, (2, 4): 2.0, (2, 8): 5.0}
+    calls = []
+    monkeypatch.setattr(autotune, "_time", lambda fn, reps: (fn(), cost[calls[-1]])[1])
+
+    def run(cfg):
+        calls.append((cfg["wave_size"], cfg["refill"]))
+    best = autotune._search("k", dict(wave_size=[1, 2], refill=[4, 8]), run, 1, False)
+    assert best == dict(wave_size=1, refill=8)
+    db = json.loads((tmp_path / "tune.json").read_text())
+    assert db["k"]["best"] == best and len(db["k"]["tried"]) == 4
+    n = len(calls)
+    assert autotune._search("k", dict(wave_size=[1, 2], refill=[4, 8]), run, 1, False) == best
+    assert len(calls) == n  # served from the cache
+    autotune._search("k", dict(wave_size=[1, 2], refill=[4, 8]), run, 1, True)
+    assert len(calls) == 2 * n  # forced re-tune
+
+
+@pytest.mark.gpu
+def test_tune_render_on_gpu(tmp_path, monkeypatch):
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import scenes
+    monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tune.json"))
+    sd, cam = scenes.random_scene(3, 2000)
+    sc = swr.Scene(sd)
+    c = swr.make_camera(cam["position"], cam["angle"], 64, 48, fov_deg=40)
+    best = autotune.tune_render(sc, c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL,
+                                grid=dict(wave_size=[1 << 12, 1 << 14], refill=[8]))
+    assert best["wave_size"] in (1 << 12, 1 << 14) and best["refill"] == 8
+    img = sc.render(c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL, **best)
+    assert float(img.max()) > 0
