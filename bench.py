@@ -39,9 +39,16 @@ CONFIGS = {
     "c2s": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=16,
                 depth=8, seed=2024),
     # batched: 256 scenes, 1k-500k triangles (log-uniform), image sides {64..1024}, spp {4,16,64}, depth 6
-    "c3": dict(kind="batch", scenes=256, depth=6, seed=7),
+    "c3": dict(kind="batch", scenes=256, depth=6, seed=7, sides=[64, 128, 256, 512, 1024], spps=[4, 16, 64],
+               tris=[1e3, 5e5]),
+    # the same batch restricted to small jobs (64x64..128x128, 4-16 spp, 1k-50k triangles): launch-bound per scene
+    "c3s": dict(kind="batch", scenes=256, depth=6, seed=7, sides=[64, 128], spps=[4, 16], tris=[1e3, 5e4]),
     # differentiable: tessellated Cornell (~49k triangles), 512x512, 32 spp primal + 32 spp adjoint, depth 6
     "c4": dict(kind="diff", W=512, H=512, spp=32, depth=6, seed=11),
+    # batched inverse rendering: 64 scenes (5k-200k triangles, 128^2-512^2), 16 spp primal/adjoint, depth 5,
+    # per-triangle albedo from a seeded random start by 200 Adam steps (lr 1e-2)
+    "c5": dict(kind="inverse", scenes=64, tris=[5e3, 2e5], sides=[128, 256, 512], spp=16, depth=5, adam_steps=200,
+               lr=1e-2, target_spp=64, seed=13),
 }
 METRIC = "Msamples/s (camera paths per second)"
 
@@ -172,9 +179,9 @@ def run_batch(args, cfg):
     jobs, t0 = [], time.time()
     tris = 0
     for k in range(cfg["scenes"]):
-        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
-        side = int(rng.choice([64, 128, 256, 512, 1024]))
-        spp = int(rng.choice([4, 16, 64]))
+        n = int(np.exp(rng.uniform(np.log(cfg["tris"][0]), np.log(cfg["tris"][1]))))
+        side = int(rng.choice(cfg["sides"]))
+        spp = int(rng.choice(cfg["spps"]))
         sd, cam = scenes.random_scene(cfg["seed"] * 100003 + k, n)
         sc = swr.Scene(sd)
         tris += sd.num_triangles
@@ -251,6 +258,128 @@ def run_diff(args, cfg):
         "adjoint_ms": a_ms, "adjoint_over_primal": a_ms / p_ms}))
 
 
+def run_inverse(args, cfg):
+    """C5: per-triangle albedo of many scenes recovered by Adam through the batched autograd
+    Function (one primal batch launch and one adjoint batch launch per step)."""
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import scenes
+    from master_thesis_b200.diff import render_physical_batch
+    rng = np.random.default_rng(cfg["seed"])
+    jobs, hidden, emis = [], [], []
+    t0 = time.time()
+    for k in range(cfg["scenes"]):
+        n = int(np.exp(rng.uniform(np.log(cfg["tris"][0]), np.log(cfg["tris"][1]))))
+        side = int(rng.choice(cfg["sides"]))
+        sd, cam = scenes.random_scene(cfg["seed"] * 7919 + k, n)
+        sc = swr.Scene(sd)
+        jobs.append(dict(scene=sc, cam=swr.make_camera(cam["position"], cam["angle"], side, side, fov_deg=40),
+                         width=side, height=side, spp=cfg["spp"], depth=cfg["depth"], seed=0))
+        hidden.append(torch.from_numpy(rng.uniform(0.1, 0.9, (sd.num_triangles, 3)).astype(np.float32)).cuda())
+        emis.append(torch.from_numpy((sd.materials["color"] * sd.materials["light_strength"][:, None])
+                                     .astype(np.float32)).cuda())
+    setup_s = time.time() - t0
+    tris = sum(j["scene"].data.num_triangles for j in jobs)
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    batch = swr.Batch()
+    with torch.no_grad():  # targets: the hidden albedo rendered at higher spp with other seeds
+        for j, a, e in zip(jobs, hidden, emis):
+            j["scene"].set_albedo(a)
+            j["scene"].set_emission(e)
+        targets = batch.render([dict(j, spp=cfg["target_spp"], seed=10 ** 6 + k, mode=swr.MODE_PHYSICAL)
+                                for k, j in enumerate(jobs)])
+        targets = [t.clone() for t in targets]
+    init = [torch.from_numpy(np.random.default_rng(cfg["seed"] + 1 + k).uniform(0.1, 0.9, tuple(h.shape))
+                             .astype(np.float32)).cuda() for k, h in enumerate(hidden)]
+    params = [a.clone().requires_grad_() for a in init]
+    opt = torch.optim.Adam(params, lr=cfg["lr"])
+    seen = [torch.zeros(h.shape[0], dtype=torch.bool, device="cuda") for h in hidden]
+
+    def step(i):
+        for k, j in enumerate(jobs):
+            j["seed"] = 2 * (i * len(jobs) + k)
+        opt.zero_grad(set_to_none=True)
+        imgs = render_physical_batch(batch, jobs, params, emis, adjoint_seeds=[j["seed"] + 1 for j in jobs])
+        loss = sum(((im - t) ** 2).mean() for im, t in zip(imgs, targets))
+        loss.backward()
+        for s_, p in zip(seen, params):
+            s_ |= (p.grad != 0).any(dim=1)
+        opt.step()
+        with torch.no_grad():
+            for p in params:
+                p.clamp_(0.0, 1.0)
+        return loss
+
+    def rmse(only_seen):
+        num, den = 0.0, 0
+        for p, h, s_ in zip(params, hidden, seen):
+            d = (p.detach() - h)[s_] if only_seen else (p.detach() - h)
+            num += float((d.double() ** 2).sum())
+            den += d.numel()
+        return (num / max(den, 1)) ** 0.5
+
+    def coverage(j):
+        # pixels whose primary ray (pixel centre) hits each triangle first
+        vi, pi, org = swr.camera_arrays(j["cam"])
+        ys, xs = np.mgrid[0:j["height"], 0:j["width"]]
+        v = np.stack([(2 * (xs + 0.5) / j["width"] - 1).ravel(), (2 * (ys + 0.5) / j["height"] - 1).ravel(),
+                      np.ones(xs.size), np.ones(xs.size)], 1)
+        t = (v @ pi.astype(np.float64))[:, :3]
+        t /= np.linalg.norm(t, axis=1, keepdims=True)
+        d = (np.concatenate([t, np.zeros((len(t), 1))], 1) @ vi.astype(np.float64))[:, :3]
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        ro = np.zeros((len(d), 4), np.float32)
+        ro[:, :3] = org
+        rd = np.zeros((len(d), 4), np.float32)
+        rd[:, :3] = d
+        tri = j["scene"].trace(ro, rd)[:, 0]
+        tri = tri[tri != 0xFFFFFFFF].astype(np.int64)
+        return torch.from_numpy(np.bincount(tri, minlength=j["scene"].data.num_triangles)).cuda()
+    cover = [coverage(j) for j in jobs]
+
+    def rmse_covered(ps, min_px):
+        num, den = 0.0, 0
+        for p, h, c in zip(ps, hidden, cover):
+            d = (p.detach() - h)[c >= min_px]
+            num += float((d.double() ** 2).sum())
+            den += d.numel()
+        return (num / max(den, 1)) ** 0.5
+
+    warm = max(args.warmup, 3)
+    first = None
+    for i in range(warm):
+        loss = step(i)
+        first = float(loss.detach()) if first is None else first
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    last = None
+    for i in range(warm, cfg["adam_steps"]):
+        last = step(i)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    timed = cfg["adam_steps"] - warm
+    init_err = [float(((a - h).double() ** 2).sum()) for a, h in zip(init, hidden)]
+    init_seen = (sum(float((((a - h)[s_]).double() ** 2).sum()) for a, h, s_ in zip(init, hidden, seen)) /
+                 max(1, 3 * sum(int(s_.sum()) for s_ in seen))) ** 0.5
+    print(json.dumps({
+        "metric": "grad-steps/s (batched inverse rendering, %d scenes)" % len(jobs), "value": timed / (ms / 1e3),
+        "unit": "grad-steps/s", "n_gpus": 1, "steps": timed, "warmup": warm, "ms_per_step": ms / timed,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded in-memory scenes)",
+        "config": {"workload": "%d scenes, %d triangles, %d samples primal + %d adjoint per step, depth %d, "
+                               "Adam lr %g, %d steps" % (len(jobs), tris, samples, samples, cfg["depth"], cfg["lr"],
+                                                        cfg["adam_steps"])},
+        "loss_first_step": first, "loss_last_step": float(last.detach()),
+        "albedo_rmse": {"initial_all": (sum(init_err) / sum(h.numel() for h in hidden)) ** 0.5,
+                        "final_all": rmse(False), "initial_seen": init_seen, "final_seen": rmse(True),
+                        "seen_triangles": int(sum(int(s_.sum()) for s_ in seen)), "triangles": tris,
+                        "initial_covering_4px": rmse_covered(init, 4), "final_covering_4px": rmse_covered(params, 4),
+                        "triangles_covering_4px": int(sum(int((c >= 4).sum()) for c in cover))},
+        "msamples_per_s_primal_plus_adjoint": 2 * samples * timed / (ms / 1e3) / 1e6, "setup_s": setup_s}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -264,14 +393,14 @@ def main():
     ap.add_argument("--tune", action="store_true", help="autotune the launch shape (cached) before timing")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
-    if cfg["kind"] in ("batch", "diff"):
+    if cfg["kind"] in ("batch", "diff", "inverse"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or differentiable "
                                                                   "renderer"}))
             return
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        (run_batch if cfg["kind"] == "batch" else run_diff)(args, cfg)
+        {"batch": run_batch, "diff": run_diff, "inverse": run_inverse}[cfg["kind"]](args, cfg)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -263,6 +263,22 @@ int swr_render_adjoint_timed(swr_scene* scene, const swr_camera* cam, const swr_
                              const float* dl_dimage, float* dl_dalbedo, float* dl_demission,
                              void* stream, double* device_ms);
 
+/* Batched adjoint: swr_render_adjoint for many jobs in one persistent launch (after one camera
+ * launch over all jobs' pixels). Each job's gradients equal swr_render_adjoint's for that job up
+ * to the order of the float atomic sums. Every distinct gradient buffer is zeroed once; jobs that
+ * name the same buffers (the same scene rendered from several cameras) add into them. Only
+ * opts.refill of the batch options is used. No counterpart in the reference. */
+typedef struct swr_adjoint_job {
+  swr_scene* scene;
+  swr_camera cam;
+  swr_render_opts opts;       /* SWR_MODE_PHYSICAL, max_depth <= 16; tuning fields ignored */
+  const float* dl_dimage;     /* [height*width*3] device */
+  float* dl_dalbedo;          /* [num_triangles*3] device */
+  float* dl_demission;        /* [num_objects*3] device */
+} swr_adjoint_job;
+int swr_render_adjoint_batch(swr_batch* batch, const swr_adjoint_job* jobs, uint32_t num_jobs,
+                             const swr_batch_opts* opts, void* stream);
+
 /* Allocation-free variant of swr_render. It has no counterpart in the reference (whose renderer
  * is a host-thread loop): it exists for callers that must not have a library allocate device
  * memory during the call, such as applications that give all device memory to their own pool

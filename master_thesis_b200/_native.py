@@ -90,6 +90,11 @@ class BatchOpts(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class AdjointJob(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("cam", Camera), ("opts", RenderOpts), ("dl_dimage", ctypes.c_void_p),
+                ("dl_dalbedo", ctypes.c_void_p), ("dl_demission", ctypes.c_void_p)]
+
+
 BATCH_NO_GRAPH = 1
 
 P = ctypes.c_void_p
@@ -123,6 +128,7 @@ SIGNATURES = {
     "swr_batch_create": (I, [ctypes.POINTER(P)]),
     "swr_batch_destroy": (None, [P]),
     "swr_render_batch": (I, [P, ctypes.POINTER(BatchJob), U32, ctypes.POINTER(BatchOpts), P]),
+    "swr_render_adjoint_batch": (I, [P, ctypes.POINTER(AdjointJob), U32, ctypes.POINTER(BatchOpts), P]),
     "swr_scene_set_albedo": (I, [P, P, P]),
     "swr_scene_set_emission": (I, [P, P, P]),
     "swr_render_adjoint": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P, P]),

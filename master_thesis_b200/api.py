@@ -267,6 +267,36 @@ class Batch:
         check(N.lib.swr_render_batch(self._h, arr, len(jobs), ctypes.byref(o), _stream_handle(stream)))
         return outs
 
+    def render_adjoint(self, jobs, refill=0, stream=None):
+        """Path-replay adjoint of many physical-mode jobs in one launch. jobs: dicts as for render
+        plus dl_dimage (cuda tensor [h, w, 3]) and optionally grad_albedo / grad_emission (cuda
+        tensors [num_triangles, 3] / [num_objects, 3]; jobs of one scene may share them and then
+        add into them). Returns [(grad_albedo, grad_emission)] per job."""
+        import torch
+        arr = (N.AdjointJob * len(jobs))()
+        keep, grads = [], []
+        for k, j in enumerate(jobs):
+            dl = j["dl_dimage"].contiguous()
+            sd = j["scene"].data
+            ga = j.get("grad_albedo")
+            if ga is None:
+                ga = torch.empty((sd.num_triangles, 3), dtype=torch.float32, device=dl.device)
+            ge = j.get("grad_emission")
+            if ge is None:
+                ge = torch.empty((sd.num_objects, 3), dtype=torch.float32, device=dl.device)
+            keep.append(dl)
+            grads.append((ga, ge))
+            arr[k].scene = j["scene"].handle
+            arr[k].cam = j["cam"]
+            arr[k].opts = N.RenderOpts(j["width"], j["height"], j["spp"], j["depth"], j.get("seed", 0), N.MODE_PHYSICAL,
+                                       j.get("rr_depth", 0), j.get("rr_survive", 1.0), 0, 0, 0, 0, 0, 0)
+            arr[k].dl_dimage = dl.data_ptr()
+            arr[k].dl_dalbedo = ga.data_ptr()
+            arr[k].dl_demission = ge.data_ptr()
+        o = N.BatchOpts(0, refill, 0, 0)
+        check(N.lib.swr_render_adjoint_batch(self._h, arr, len(jobs), ctypes.byref(o), _stream_handle(stream)))
+        return grads
+
 
 def quantize_rgb8(img):
     img = np.ascontiguousarray(img, dtype=np.float32)

@@ -38,7 +38,10 @@ struct BJob {
   uint64_t seed;
   uint64_t sample_base;  // first global sample index of the job
   uint64_t pixel_base;   // first global pixel index of the job
-  float* out;            // [H*W*3] device
+  float* out;            // [H*W*3] device (primal)
+  const float* dl;       // [H*W*3] device dLoss/dImage (adjoint)
+  float* g_alb;          // [triangles*3] device (adjoint)
+  float* g_em;           // [objects*3] device (adjoint)
 };
 
 struct BCtrl {
@@ -269,6 +272,102 @@ __global__ void __launch_bounds__(kTB) k_btrace(BArgs A, BCtrl* __restrict__ ctr
   }
 }
 
+// Batched path-replay adjoint: the single-scene adjoint replay (render.cu, k_adjoint) over the
+// batch's global sample range. One persistent launch covers every job: lanes take the next
+// global samples (refilling idle lanes), find their job by binary search, start from the job's
+// per-pixel camera record and replay the path with the job's scene, seed and Russian roulette,
+// then sweep it into the job's gradient buffers. ctrl->injected is the sample cursor.
+__global__ void __launch_bounds__(kTB) k_badjoint(BArgs A, BCtrl* __restrict__ ctrl) {
+  __shared__ uint2 stack[swrx::kStackShared * kTB];
+  const unsigned ln = lane();
+  const unsigned lt = (1u << ln) - 1u;
+  const unsigned long long total = ctrl->total;
+  swrx::Traversal tr;
+  swrx::PathState st;
+  swrx::AdjointTape tape;
+  tape.reset();
+  const BJob* J = nullptr;
+  const DevScene* sc = nullptr;
+  uint32_t pixel = 0, sample = 0, pend_slot = 0;
+  float pend_t = 0.0f;
+  bool active = false, tracing = false, exhausted = false;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= A.refill) {
+      unsigned long long base = 0;
+      if (ln == 0) base = atomicAdd(&ctrl->injected, (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) exhausted = true;
+      if (!active) {
+        const unsigned long long g = base + __popc(idle & lt);
+        if (g < total) {
+          J = &A.jobs[find_job(A.jobs, A.njobs, g, false)];
+          const uint64_t local = g - J->sample_base;
+          pixel = (uint32_t)(local / J->spp);
+          sample = (uint32_t)(local % J->spp);
+          const uint64_t p = J->pixel_base + pixel;
+          const float4 r0 = A.cam[2 * p], r1 = A.cam[2 * p + 1];
+          const uint32_t bits = __float_as_uint(r1.w);
+          if (bits != kDead) {
+            sc = &A.scenes[J->scene];
+            st.o = mk(r0.x, r0.y, r0.z);
+            st.d = mk(r1.x, r1.y, r1.z);
+            st.c = mk(1.0f, 1.0f, 1.0f);
+            st.L = mk(0.0f, 0.0f, 0.0f);
+            st.i = bits >> 27;
+            st.v = 0;
+            pend_slot = bits & 0x07FFFFFFu;
+            pend_t = r0.w;
+            tape.reset();
+            tracing = false;
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+    if (tracing) {
+      if (!tr.step<false, false>(sc->nodes, sc->tris, sc->tri_boxes, sc->obj_boxes, nullptr)) continue;
+      tracing = false;
+      if (tr.hit.slot == 0xFFFFFFFFu) {  // the path left the scene: no emitter, no gradient
+        active = false;
+        continue;
+      }
+      pend_slot = tr.hit.slot;
+      pend_t = tr.hit.t;
+    }
+    swrx::ShadeParams P;
+    P.seed = J->seed;
+    P.pixel = pixel;
+    P.sample = sample;
+    P.depth = J->depth;
+    P.mode = 1;
+    P.rr_depth = J->rr_depth;
+    P.rr_q = J->rr_q;
+    const f3 c_before = st.c;
+    swrx::AdjVertex av;
+    const uint32_t outcome =
+        swrx::shade_physical_adj(sc->tris, sc->shade, sc->mats, sc->albedo, pend_slot, pend_t, P, st, av);
+    if (outcome == swrx::kContinue) {
+      tape.push(pend_slot, c_before, av);
+      tr.init(st.o, st.d, stack + threadIdx.x, kTB);
+      tracing = true;
+      continue;
+    }
+    if (av.emit_front) {
+      const float inv_spp = 1.0f / (float)J->spp;
+      const float* dlp = J->dl + (size_t)pixel * 3;
+      tape.sweep(sc->tris, sc->mats, sc->albedo, av.obj, c_before,
+                 mk(dlp[0] * inv_spp, dlp[1] * inv_spp, dlp[2] * inv_spp), J->g_alb, J->g_em);
+    }
+    active = false;
+  }
+}
+
 __global__ void k_bresolve(BArgs A) {
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.npix) return;
@@ -310,6 +409,51 @@ struct swr_batch {
 
 using swr::set_error;
 
+namespace swr {
+namespace {
+
+// Appends one job to the table (validating what the primal and the adjoint both need); uniq / hs
+// collect the distinct scenes, samples / pixels the running prefix sums.
+int add_job(int device, const swr_scene* scene, const swr_camera& cam, const swr_render_opts& o, BJob& d,
+            std::vector<const swr_scene*>& uniq, std::vector<DevScene>& hs, uint64_t& samples, uint64_t& pixels) {
+  if (!scene) return set_error(SWR_ERR_INVALID, "swr: batch job without scene");
+  if (scene->device != device) return set_error(SWR_ERR_INVALID, "swr: batch jobs on another device");
+  if (o.width == 0 || o.height == 0 || o.spp == 0) return set_error(SWR_ERR_INVALID, "swr: zero image size");
+  if ((uint64_t)o.width * o.height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
+  if (o.max_depth == 0 || o.max_depth > 31) return set_error(SWR_ERR_INVALID, "swr: max_depth must be 1..31");
+  if (o.mode > 1) return set_error(SWR_ERR_INVALID, "swr: unknown mode");
+  if (o.mode == 1 && o.rr_depth && !(o.rr_survive > 0.0f && o.rr_survive <= 1.0f))
+    return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+  uint32_t si = 0;
+  while (si < uniq.size() && uniq[si] != scene) ++si;
+  if (si == uniq.size()) {
+    uniq.push_back(scene);
+    hs.push_back(scene->dev);
+  }
+  std::memset(&d, 0, sizeof(d));
+  std::memcpy(d.vi, cam.view_inv, sizeof(d.vi));
+  std::memcpy(d.pi, cam.proj_inv, sizeof(d.pi));
+  std::memcpy(d.org, cam.origin, sizeof(d.org));
+  d.W = o.width;
+  d.H = o.height;
+  d.spp = o.spp;
+  d.depth = o.max_depth;
+  d.mode = o.mode;
+  d.rr_depth = o.mode == 1 ? o.rr_depth : 0;
+  d.rr_q = (o.mode == 1 && o.rr_depth) ? o.rr_survive : 1.0f;
+  d.scene = si;
+  d.seed = o.seed;
+  d.sample_base = samples;
+  d.pixel_base = pixels;
+  const uint64_t np = (uint64_t)o.width * o.height;
+  pixels += np;
+  samples += np * o.spp;
+  return SWR_OK;
+}
+
+}  // namespace
+}  // namespace swr
+
 extern "C" {
 
 int swr_batch_create(swr_batch** out) {
@@ -342,50 +486,20 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
   std::vector<const swr_scene*> uniq;
   uint64_t samples = 0, pixels = 0;
   int num_sms = 0;
+  int rc;
   for (uint32_t k = 0; k < n; ++k) {
     const swr_batch_job& J = jobs[k];
-    const swr_render_opts& o = J.opts;
-    if (!J.scene || !J.rgb_out) return set_error(SWR_ERR_INVALID, "swr: batch job without scene or output");
-    if (J.scene->device != b->device) return set_error(SWR_ERR_INVALID, "swr: batch jobs on another device");
-    if (o.width == 0 || o.height == 0 || o.spp == 0) return set_error(SWR_ERR_INVALID, "swr: zero image size");
-    if (o.max_depth == 0 || o.max_depth > 31) return set_error(SWR_ERR_INVALID, "swr: max_depth must be 1..31");
-    if (o.mode > 1) return set_error(SWR_ERR_INVALID, "swr: unknown mode");
-    if (o.mode == 1 && o.rr_depth && !(o.rr_survive > 0.0f && o.rr_survive <= 1.0f))
-      return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+    if (!J.rgb_out) return set_error(SWR_ERR_INVALID, "swr: batch job without output");
+    if ((rc = add_job(b->device, J.scene, J.cam, J.opts, hj[k], uniq, hs, samples, pixels))) return rc;
     if (is_host_pointer(J.rgb_out)) return set_error(SWR_ERR_INVALID, "swr: batch outputs must be device memory");
-    uint32_t si = 0;
-    while (si < uniq.size() && uniq[si] != J.scene) ++si;
-    if (si == uniq.size()) {
-      uniq.push_back(J.scene);
-      hs.push_back(J.scene->dev);
-    }
+    hj[k].out = J.rgb_out;
     num_sms = J.scene->num_sms;
-    BJob& d = hj[k];
-    std::memcpy(d.vi, J.cam.view_inv, sizeof(d.vi));
-    std::memcpy(d.pi, J.cam.proj_inv, sizeof(d.pi));
-    std::memcpy(d.org, J.cam.origin, sizeof(d.org));
-    d.W = o.width;
-    d.H = o.height;
-    d.spp = o.spp;
-    d.depth = o.max_depth;
-    d.mode = o.mode;
-    d.rr_depth = o.mode == 1 ? o.rr_depth : 0;
-    d.rr_q = (o.mode == 1 && o.rr_depth) ? o.rr_survive : 1.0f;
-    d.scene = si;
-    d.seed = o.seed;
-    d.sample_base = samples;
-    d.pixel_base = pixels;
-    d.out = J.rgb_out;
-    const uint64_t np = (uint64_t)o.width * o.height;
-    pixels += np;
-    samples += np * o.spp;
   }
   uint32_t cap = (bo && bo->wave_size) ? bo->wave_size : (1u << 23);
   cap = (uint32_t)std::min<uint64_t>(cap, samples);
   cap = std::max<uint32_t>(32, (cap + 255u) & ~255u);
   const uint32_t refill = (bo && bo->refill) ? bo->refill : 8;
   if (refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
-  int rc;
   if ((rc = ensure_bytes(&b->qbuf, b->qbytes, (size_t)cap * (4 * sizeof(float4) + sizeof(uint2)) * 2))) return rc;
   if ((rc = ensure_bytes(&b->cam, b->cambytes, pixels * 2 * sizeof(float4)))) return rc;
   if ((rc = ensure_bytes(&b->accum, b->accbytes, pixels * 3 * sizeof(unsigned long long)))) return rc;
@@ -480,6 +594,81 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
     if (h.count[0] == 0 && h.inj_n[0] == 0 && h.injected == h.total) break;
   }
   k_bresolve<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(A);
+  SWR_CUDA(cudaGetLastError());
+  return SWR_OK;
+}
+
+int swr_render_adjoint_batch(swr_batch* b, const swr_adjoint_job* jobs, uint32_t n, const swr_batch_opts* bo,
+                             void* stream_) {
+  using namespace swr;
+  if (!b || !jobs || n == 0) return set_error(SWR_ERR_INVALID, "swr: empty batch");
+  if (n > 65535) return set_error(SWR_ERR_UNSUPPORTED, "swr: at most 65535 jobs per batch");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(b->device));
+  std::vector<BJob> hj(n);
+  std::vector<DevScene> hs;
+  std::vector<const swr_scene*> uniq;
+  uint64_t samples = 0, pixels = 0;
+  int num_sms = 0;
+  int rc;
+  // distinct gradient buffers and their sizes in bytes (zeroed once each; jobs that share a
+  // buffer add into it)
+  std::vector<std::pair<float*, size_t>> zero;
+  auto note = [&](float* p, size_t bytes) -> int {
+    for (auto& z : zero)
+      if (z.first == p) {
+        if (z.second != bytes) return set_error(SWR_ERR_INVALID, "swr: a gradient buffer is shared by scenes of "
+                                                                 "different sizes");
+        return SWR_OK;
+      }
+    zero.emplace_back(p, bytes);
+    return SWR_OK;
+  };
+  for (uint32_t k = 0; k < n; ++k) {
+    const swr_adjoint_job& J = jobs[k];
+    if (!J.dl_dimage || !J.dl_dalbedo || !J.dl_demission) return set_error(SWR_ERR_INVALID, "swr: null argument");
+    if (J.opts.mode != SWR_MODE_PHYSICAL)
+      return set_error(SWR_ERR_INVALID, "swr: the adjoint is defined for SWR_MODE_PHYSICAL");
+    if (J.opts.max_depth > (uint32_t)swrx::kAdjMaxDepth)
+      return set_error(SWR_ERR_UNSUPPORTED, "swr: the adjoint supports max_depth 1..16");
+    if ((rc = add_job(b->device, J.scene, J.cam, J.opts, hj[k], uniq, hs, samples, pixels))) return rc;
+    if (is_host_pointer(J.dl_dimage) || is_host_pointer(J.dl_dalbedo) || is_host_pointer(J.dl_demission))
+      return set_error(SWR_ERR_INVALID, "swr: the adjoint takes device buffers");
+    hj[k].dl = J.dl_dimage;
+    hj[k].g_alb = J.dl_dalbedo;
+    hj[k].g_em = J.dl_demission;
+    if ((rc = note(J.dl_dalbedo, (size_t)J.scene->dev.num_tris * 3 * sizeof(float)))) return rc;
+    if ((rc = note(J.dl_demission, (size_t)J.scene->dev.num_objects * 3 * sizeof(float)))) return rc;
+    num_sms = J.scene->num_sms;
+  }
+  const uint32_t refill = (bo && bo->refill) ? bo->refill : 8;
+  if (refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  if ((rc = ensure_bytes(&b->cam, b->cambytes, pixels * 2 * sizeof(float4)))) return rc;
+  if ((rc = ensure_bytes(&b->jobs, b->jobbytes, n * sizeof(BJob)))) return rc;
+  if ((rc = ensure_bytes(&b->scenes, b->scenebytes, hs.size() * sizeof(DevScene)))) return rc;
+  if ((rc = ensure_bytes(&b->ctrl, b->ctrlbytes, sizeof(BCtrl)))) return rc;
+  SWR_CUDA(cudaMemcpyAsync(b->jobs, hj.data(), n * sizeof(BJob), cudaMemcpyHostToDevice, stream));
+  SWR_CUDA(cudaMemcpyAsync(b->scenes, hs.data(), hs.size() * sizeof(DevScene), cudaMemcpyHostToDevice, stream));
+  for (auto& z : zero) SWR_CUDA(cudaMemsetAsync(z.first, 0, z.second, stream));
+  BArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.jobs = (const BJob*)b->jobs;
+  A.scenes = (const DevScene*)b->scenes;
+  A.njobs = n;
+  A.npix = pixels;
+  A.refill = refill;
+  A.cam = (float4*)b->cam;
+  BCtrl init;
+  std::memset(&init, 0, sizeof(init));
+  init.total = samples;
+  SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
+  *b->host_ctrl = init;
+  SWR_CUDA(cudaMemcpyAsync(b->ctrl, b->host_ctrl, sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
+  k_bcamera<<<(unsigned)((pixels + kTB - 1) / kTB), kTB, 0, stream>>>(A, (BCtrl*)b->ctrl);
+  SWR_CUDA(cudaGetLastError());
+  int per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_badjoint, kTB, 0));
+  k_badjoint<<<(unsigned)(num_sms * std::max(per_sm, 1)), kTB, 0, stream>>>(A, (BCtrl*)b->ctrl);
   SWR_CUDA(cudaGetLastError());
   return SWR_OK;
 }

@@ -322,13 +322,10 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
 // counters (the same hits, directions and throughputs as the primal render), keeping for each
 // scattering vertex the triangle slot, the throughput c_j before the vertex and the factor
 // gq_j the vertex applied besides the albedo (2 cos / q for a diffuse bounce, 1 / q otherwise).
-// A path that ends on an emitter seen from the front contributes L = c_e * Le; sweeping its
-// vertices backwards with S = Le, dL/dalbedo(tri_j) = c_j * gq_j * S_{j+1} and S_j = albedo_j *
-// gq_j * S_{j+1}; dL/dLe = c_e. Each term is weighted by dLoss/dImage of the pixel / spp and
-// added atomically to per-triangle / per-object gradients. Nothing of the primal pass is stored:
-// the path is replayed, which is the checkpointing scheme. Lanes that finish a sample take a new
-// one (refill as in the bounce traversal), and the traversal itself is the resumable Traversal.
-constexpr int kAdjMaxDepth = 16;
+// The backward sweep is swrx::AdjointTape. Nothing of the primal pass is stored: the path is
+// replayed, which is the checkpointing scheme. Lanes that finish a sample take a new one (refill
+// as in the bounce traversal), and the traversal itself is the resumable Traversal.
+using swrx::kAdjMaxDepth;
 
 __global__ void __launch_bounds__(kTraceBlock)
     k_adjoint(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, const float* __restrict__ dl,
@@ -340,10 +337,8 @@ __global__ void __launch_bounds__(kTraceBlock)
   swrx::Traversal tr;
   swrx::PathState st;
   uint32_t pixel = 0, sample = 0;
-  uint32_t h_slot[kAdjMaxDepth];
-  float h_cx[kAdjMaxDepth], h_cy[kAdjMaxDepth], h_cz[kAdjMaxDepth], h_gq[kAdjMaxDepth];
-  uint32_t h_diff = 0;
-  int nv = 0;
+  swrx::AdjointTape tape;
+  tape.reset();
   bool active = false, tracing = false, exhausted = false;
   uint32_t pend_slot = 0;
   float pend_t = 0.0f;
@@ -372,8 +367,7 @@ __global__ void __launch_bounds__(kTraceBlock)
             st.v = 0;
             pend_slot = bits & 0x07FFFFFFu;
             pend_t = r0.w;
-            nv = 0;
-            h_diff = 0;
+            tape.reset();
             tracing = false;
             active = true;
           }
@@ -404,52 +398,22 @@ __global__ void __launch_bounds__(kTraceBlock)
     P.mode = 1;
     P.rr_depth = F.rr_depth;
     P.rr_q = F.rr_q;
-    const float cx = st.c.x, cy = st.c.y, cz = st.c.z;
+    const f3 c_before = st.c;
     swrx::AdjVertex av;
     const uint32_t outcome =
         swrx::shade_physical_adj(sc.tris, sc.shade, sc.mats, sc.albedo, pend_slot, pend_t, P, st, av);
     // a vertex after which the path goes on is kept for the sweep; a path that ends without an
     // emitter (depth reached, Russian roulette, escape) carries no radiance and no gradient
     if (outcome == swrx::kContinue) {
-      h_slot[nv] = pend_slot;
-      h_cx[nv] = cx;
-      h_cy[nv] = cy;
-      h_cz[nv] = cz;
-      h_gq[nv] = av.gq;
-      if (av.diffuse) h_diff |= 1u << nv;
-      ++nv;
-    }
-    if (outcome == swrx::kContinue) {
+      tape.push(pend_slot, c_before, av);
       tr.init(st.o, st.d, stack + threadIdx.x, kTraceBlock);
       tracing = true;
       continue;
     }
     if (av.emit_front) {
       const float* dlp = dl + (size_t)(F.pixel0 + pixel) * 3;
-      const float wx = dlp[0] * inv_spp, wy = dlp[1] * inv_spp, wz = dlp[2] * inv_spp;
-      atomicAdd(&g_em[3 * (size_t)av.obj + 0], wx * cx);
-      atomicAdd(&g_em[3 * (size_t)av.obj + 1], wy * cy);
-      atomicAdd(&g_em[3 * (size_t)av.obj + 2], wz * cz);
-      const float4 le = __ldg(sc.mats + 3 * (size_t)av.obj + 2);
-      float sx = le.x, sy = le.y, sz = le.z;
-      for (int j = nv - 1; j >= 0; --j) {
-        const float gq = h_gq[j];
-        if (h_diff & (1u << j)) {
-          const uint32_t s = h_slot[j];
-          const uint32_t id = __float_as_uint(__ldg(sc.tris + 3 * (size_t)s + 2).y);
-          atomicAdd(&g_alb[3 * (size_t)id + 0], wx * h_cx[j] * gq * sx);
-          atomicAdd(&g_alb[3 * (size_t)id + 1], wy * h_cy[j] * gq * sy);
-          atomicAdd(&g_alb[3 * (size_t)id + 2], wz * h_cz[j] * gq * sz);
-          const float* a = sc.albedo + 3 * (size_t)s;
-          sx *= a[0] * gq;
-          sy *= a[1] * gq;
-          sz *= a[2] * gq;
-        } else {
-          sx *= gq;
-          sy *= gq;
-          sz *= gq;
-        }
-      }
+      tape.sweep(sc.tris, sc.mats, sc.albedo, av.obj, c_before,
+                 mk(dlp[0] * inv_spp, dlp[1] * inv_spp, dlp[2] * inv_spp), g_alb, g_em);
     }
     active = false;
   }

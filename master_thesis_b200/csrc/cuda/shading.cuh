@@ -241,6 +241,64 @@ SWR_HD uint32_t shade_physical_adj(const float4* tris, const float4* shade, cons
   return (st.i < P.depth) ? kContinue : kEndDark;
 }
 
+#ifdef __CUDACC__
+// The per-path record of the adjoint replay and its backward sweep. A path that ends on an
+// emitter seen from the front contributes L = c_e * Le; sweeping its vertices backwards with
+// S = Le, dL/dalbedo(tri_j) = c_j * gq_j * S_{j+1} and S_j = albedo_j * gq_j * S_{j+1}; dL/dLe =
+// c_e. Each term is weighted by w = dLoss/dImage(pixel) / spp and added atomically.
+constexpr int kAdjMaxDepth = 16;
+
+struct AdjointTape {
+  uint32_t slot[kAdjMaxDepth];
+  float cx[kAdjMaxDepth], cy[kAdjMaxDepth], cz[kAdjMaxDepth], gq[kAdjMaxDepth];
+  uint32_t diff;
+  int nv;
+
+  __device__ __forceinline__ void reset() {
+    nv = 0;
+    diff = 0;
+  }
+  // a vertex after which the path goes on (c = throughput before the vertex)
+  __device__ __forceinline__ void push(uint32_t s, f3 c, const AdjVertex& av) {
+    slot[nv] = s;
+    cx[nv] = c.x;
+    cy[nv] = c.y;
+    cz[nv] = c.z;
+    gq[nv] = av.gq;
+    if (av.diffuse) diff |= 1u << nv;
+    ++nv;
+  }
+  // the path ended on the front of emitter object obj with throughput c before it
+  __device__ __forceinline__ void sweep(const float4* __restrict__ tris, const float4* __restrict__ mats,
+                                        const float* __restrict__ albedo, uint32_t obj, f3 c, f3 w,
+                                        float* __restrict__ g_alb, float* __restrict__ g_em) const {
+    atomicAdd(&g_em[3 * (size_t)obj + 0], w.x * c.x);
+    atomicAdd(&g_em[3 * (size_t)obj + 1], w.y * c.y);
+    atomicAdd(&g_em[3 * (size_t)obj + 2], w.z * c.z);
+    const float4 le = __ldg(mats + 3 * (size_t)obj + 2);
+    float sx = le.x, sy = le.y, sz = le.z;
+    for (int j = nv - 1; j >= 0; --j) {
+      const float g = gq[j];
+      if (diff & (1u << j)) {
+        const uint32_t s = slot[j];
+        const uint32_t id = __float_as_uint(__ldg(tris + 3 * (size_t)s + 2).y);
+        atomicAdd(&g_alb[3 * (size_t)id + 0], w.x * cx[j] * g * sx);
+        atomicAdd(&g_alb[3 * (size_t)id + 1], w.y * cy[j] * g * sy);
+        atomicAdd(&g_alb[3 * (size_t)id + 2], w.z * cz[j] * g * sz);
+        const float* a = albedo + 3 * (size_t)s;
+        sx *= a[0] * g;
+        sy *= a[1] * g;
+        sz *= a[2] * g;
+      } else {
+        sx *= g;
+        sy *= g;
+        sz *= g;
+      }
+    }
+  }
+};
+#endif
+
 // Primary ray through the pixel centre (path_tracer.cpp:19-23)
 SWR_HD f3 primary_dir(const float* vi, const float* pi, uint32_t px, uint32_t py, uint32_t W,
                       uint32_t H) {

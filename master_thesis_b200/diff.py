@@ -6,7 +6,8 @@ per-object emission [num_objects, 3]. The backward pass is the library's path-re
 (swr_render_adjoint): it re-traces every camera path from its random-number counters instead of
 keeping anything from the forward pass. With adjoint_seed = seed (the default) the gradient is the
 exact derivative of the rendered Monte Carlo estimate; a different adjoint seed gives an
-independent (decorrelated) gradient estimate.
+independent (decorrelated) gradient estimate. render_physical_batch does the same for many scenes
+at once through the batched primal (swr_render_batch) and adjoint (swr_render_adjoint_batch).
 """
 import torch
 
@@ -45,3 +46,47 @@ def render_physical(scene, cam, albedo, emission, width, height, spp, depth, see
     """Physical-mode image [height, width, 3], differentiable w.r.t. albedo and emission."""
     return _PhysicalRender.apply(albedo, emission, scene, cam, width, height, spp, depth, seed, rr_depth,
                                  rr_survive, adjoint_seed)
+
+
+class _PhysicalRenderBatch(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, batch, jobs, adjoint_seeds, *params):
+        params = [p.detach().contiguous() for p in params]
+        for k, j in enumerate(jobs):
+            j["scene"].set_albedo(params[2 * k])
+            j["scene"].set_emission(params[2 * k + 1])
+        imgs = batch.render([dict(j, mode=N.MODE_PHYSICAL) for j in jobs])
+        ctx.save_for_backward(*params)
+        ctx.batch, ctx.jobs, ctx.adjoint_seeds = batch, jobs, adjoint_seeds
+        return tuple(imgs)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        params = ctx.saved_tensors
+        adj = []
+        for k, j in enumerate(ctx.jobs):
+            j["scene"].set_albedo(params[2 * k])
+            j["scene"].set_emission(params[2 * k + 1])
+            g = grads[k]
+            if g is None:
+                g = torch.zeros((j["height"], j["width"], 3), dtype=torch.float32, device=params[2 * k].device)
+            seed = j.get("seed", 0) if ctx.adjoint_seeds is None else ctx.adjoint_seeds[k]
+            adj.append(dict(j, seed=seed, dl_dimage=g))
+        out = ctx.batch.render_adjoint(adj)
+        flat = []
+        for ga, ge in out:
+            flat += [ga, ge]
+        return (None, None, None, *flat)
+
+
+def render_physical_batch(batch, jobs, albedos, emissions, adjoint_seeds=None):
+    """Physical-mode images of many scenes, one primal batch launch forward and one batched
+    path-replay adjoint launch backward. jobs: dicts with scene, cam, width, height, spp, depth and
+    optional seed, rr_depth, rr_survive; each job its own scene. albedos / emissions: per-job
+    tensors [num_triangles, 3] / [num_objects, 3]. Returns a tuple of images [h, w, 3]."""
+    if len({id(j["scene"]) for j in jobs}) != len(jobs):
+        raise ValueError("render_physical_batch: each job needs its own scene")
+    params = []
+    for a, e in zip(albedos, emissions):
+        params += [a, e]
+    return _PhysicalRenderBatch.apply(batch, jobs, adjoint_seeds, *params)
