@@ -83,8 +83,9 @@ def build(verbose=False, ptxas_info=False):
     cli = os.path.join(LIB, "SoftwareRenderer")
     cli_src = os.path.join(CSRC, CLI_SRC)
     if os.path.exists(cli_src) and _stale(cli, [cli_src, so] + headers):
-        _run([CXX, "-O2", "-std=c++17", cli_src, "-o", cli, "-L" + LIB, "-lswr",
-              "-Wl,-rpath,$ORIGIN"], verbose)
+        _run([CXX, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include", cli_src,
+              "-o", cli, "-L" + LIB, "-lswr", "-L/usr/local/cuda/lib64", "-lcudart",
+              "-Wl,-rpath,$ORIGIN:" + LIB + ":/usr/local/cuda/lib64"], verbose)
     return so, "\n".join(logs)
 
 

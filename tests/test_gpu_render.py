@@ -81,3 +81,27 @@ def test_gpu_render_invalid_args():
         sc.render(golden_camera(g), 8, 8, 1, 0)
     with pytest.raises(swr.SwrError):
         sc.render(golden_camera(g), 8, 8, 1, 40)
+
+
+def test_gpu_converged_image_within_statistical_error_of_fp64(tmp_path):
+    """A 256-spp GPU image against an independent 4096-spp FP64 host accumulation (other seed):
+    per pixel and channel the difference must be consistent with the two estimates' standard
+    errors (z-scores: mean square near 1, almost none beyond 4.5 sigma)."""
+    s = scenes.cornell(5, str(tmp_path))
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    sc = swr.Scene(sd)
+    W, H, spp, hi = 24, 16, 256, 4096
+    cam = swr.load_camera(s["camera"], W, H, use_fov_key=True)
+    vi, pi, org = swr.camera_arrays(cam)
+    img = sc.render(cam, W, H, spp, 5, seed=1, mode=swr.MODE_PHYSICAL, rr_depth=3, rr_survive=0.8)
+    torch.cuda.synchronize()
+    m64, var64 = O.render_physical64(O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org), W, H, hi, 5, 2,
+                                     rr_depth=3, rr_q=0.8)
+    g = img.cpu().numpy().reshape(-1, 3).astype(np.float64)
+    sigma2 = var64 * (hi / spp) + var64  # variance of the GPU mean + of the FP64 mean
+    live = sigma2 > 0
+    z = (g - m64)[live] / np.sqrt(sigma2[live])
+    assert live.sum() > 0.5 * live.size
+    assert 0.6 < float(np.mean(z ** 2)) < 1.5, float(np.mean(z ** 2))
+    assert float(np.mean(np.abs(z) > 4.5)) < 2e-3
+    assert np.all(np.abs(g - m64)[~live] < 1e-6)
