@@ -107,7 +107,7 @@ typedef struct swr_render_opts {
   uint32_t flags;          /* SWR_RENDER_* */
   uint32_t refill;         /* bounce traversal: idle lanes (1..32) that trigger a refill, 0 = 8 */
   uint32_t trace_blocks;   /* bounce traversal: resident blocks per SM targeted by the register
-                              budget, one of 0 (compiler's choice), 8, 10, 12 */
+                              budget, one of 0 (compiler's choice), 9, 10 */
   uint32_t reserved;
 } swr_render_opts;
 

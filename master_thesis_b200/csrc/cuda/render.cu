@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(kBlock)
   float t = 0.0f;
   bool have = false;
   if (i < n_in) {
-    const float4 qo = in.o[i], qd = in.d[i], qc = in.c[i];
-    const uint2 h = in.hit[i];
+    const float4 qo = __ldcs(in.o + i), qd = __ldcs(in.d + i), qc = __ldcs(in.c + i);
+    const uint2 h = __ldcs(in.hit + i);
     pixel = __float_as_uint(qo.w);
     sample = __float_as_uint(qd.w);
     const uint32_t meta = __float_as_uint(qc.w);
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kBlock)
     st.i = (meta >> 8) & 0xFFu;
     st.v = meta & 0xFFu;
     if (F.mode == 1) {
-      const float4 ql = in.l[i];
+      const float4 ql = __ldcs(in.l + i);
       st.L = mk(ql.x, ql.y, ql.z);
     } else {
       st.L = mk(0, 0, 0);
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kBlock)
                                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       else
         r = make_float4(st.L.x, st.L.y, st.L.z, 1.0f);
-      F.contrib[(size_t)pixel * F.spp + sample] = r;
+      __stcs(F.contrib + (size_t)pixel * F.spp + sample, r);
     }
   }
   // warp-aggregated append of the live paths
@@ -193,10 +193,10 @@ __global__ void __launch_bounds__(kBlock)
   base = __shfl_sync(0xffffffffu, base, leader);
   if (live) {
     const unsigned j = base + __popc(mask & ((1u << lane_id()) - 1u));
-    out.o[j] = make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel));
-    out.d[j] = make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample));
-    out.c[j] = make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((st.i << 8) | st.v));
-    if (F.mode == 1) out.l[j] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+    __stcs(out.o + j, make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel)));
+    __stcs(out.d + j, make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample)));
+    __stcs(out.c + j, make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((st.i << 8) | st.v)));
+    if (F.mode == 1) __stcs(out.l + j, make_float4(st.L.x, st.L.y, st.L.z, 0.0f));
   }
 }
 
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
       if (!active) {
         const unsigned j = base + __popc(idle & lt);
         if (j < n) {
-          const float4 o = q.o[j], d = q.d[j];
+          const float4 o = __ldcs(q.o + j), d = __ldcs(q.d + j);
           tr.init(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), stack + threadIdx.x, kTraceBlock);
           ray = j;
           active = true;
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
       continue;
     }
     if (active && tr.template step<kStats, kPostpone>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, &st)) {
-      q.hit[ray] = make_uint2(tr.hit.slot, __float_as_uint(tr.hit.t));
+      __stcs(q.hit + ray, make_uint2(tr.hit.slot, __float_as_uint(tr.hit.t)));
       active = false;
     }
   }
@@ -613,11 +613,15 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 0, true> : k_trace_dyn<false, 0, true>)
                               : (count ? k_trace_dyn<true, 0, false> : k_trace_dyn<false, 0, false>);
       break;
+    case 9:
+      trace_kernel = postpone ? (count ? k_trace_dyn<true, 9, true> : k_trace_dyn<false, 9, true>)
+                              : (count ? k_trace_dyn<true, 9, false> : k_trace_dyn<false, 9, false>);
+      break;
     case 10:
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 10, true> : k_trace_dyn<false, 10, true>)
                               : (count ? k_trace_dyn<true, 10, false> : k_trace_dyn<false, 10, false>);
       break;
-    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0 or 10");
+    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0, 9 or 10");
   }
   if (static_fetch) trace_kernel = count ? k_trace<true> : k_trace<false>;
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");

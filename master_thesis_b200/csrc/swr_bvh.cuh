@@ -49,6 +49,14 @@ struct Hit {
   float d2;
 };
 
+// What the traversal carries while it runs (id and object are read from the record at the end).
+struct BestHit {
+  uint32_t slot;
+  uint32_t rank;
+  float t;
+  float d2;
+};
+
 struct TraceStats {
   uint32_t nodes;
   uint32_t tris;
@@ -60,18 +68,51 @@ struct TraceStats {
 constexpr uint32_t kTriGroup = 0x80000000u;
 
 struct GroupStack {
+#if defined(__CUDA_ARCH__)
+  uint32_t sbase;  // shared-memory address of this thread's entry 0
+  uint32_t sstride;  // bytes between consecutive entries
+#else
   uint2* shared;
   int stride;
+#endif
   int sp;
   uint2 local[kStackTotal - kStackShared];
+  SWR_HD void bind(uint2* p, int stride_entries) {
+#if defined(__CUDA_ARCH__)
+    sbase = (uint32_t)__cvta_generic_to_shared(p);
+    sstride = (uint32_t)stride_entries * (uint32_t)sizeof(uint2);
+#else
+    shared = p;
+    stride = stride_entries;
+#endif
+    sp = 0;
+  }
   SWR_HD void push(uint2 v) {
-    if (sp < kStackShared) shared[sp * stride] = v;
-    else local[sp - kStackShared] = v;
+    if (sp < kStackShared) {
+#if defined(__CUDA_ARCH__)
+      asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(sbase + (uint32_t)sp * sstride), "r"(v.x), "r"(v.y)
+                   : "memory");
+#else
+      shared[sp * stride] = v;
+#endif
+    } else {
+      local[sp - kStackShared] = v;
+    }
     ++sp;
   }
   SWR_HD uint2 pop() {
     --sp;
-    return (sp < kStackShared) ? shared[sp * stride] : local[sp - kStackShared];
+    if (sp < kStackShared) {
+#if defined(__CUDA_ARCH__)
+      uint2 v;
+      asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(sbase + (uint32_t)sp * sstride)
+                   : "memory");
+      return v;
+#else
+      return shared[sp * stride];
+#endif
+    }
+    return local[sp - kStackShared];
   }
 };
 
@@ -88,6 +129,26 @@ SWR_HD float4 ldg4(const float4* p) {
 // the traversal keeps the ALU and FMA pipes busier than the conversion pipe.)
 SWR_HD float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
 
+// max / min of three floats, NaN operands ignored as by fmaxf / fminf
+SWR_HD float fmax3(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fmaxf(fmaxf(a, b), c);
+#endif
+}
+SWR_HD float fmin3(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fminf(fminf(a, b), c);
+#endif
+}
+
 // Resumable closest-hit traversal of one ray: init() sets the ray up, each step() expands at
 // most one wide node and tests the triangles of its hit leaves, and returns true once the ray is
 // finished (hit holds the result). The persistent kernels keep one Traversal per lane and refill
@@ -99,7 +160,7 @@ struct Traversal {
   float tprune;
   uint2 ng;  // node group: x = child_base, y = hits (bits 24..31, visit order) | imask (bits 0..7)
   uint2 tg;  // triangle group: x = base, y = hit bits 0..23
-  Hit hit;
+  BestHit hit;
   GroupStack st;
   uint32_t host_turn;  // host build only: drives the alternating postponing decision
 
@@ -116,24 +177,20 @@ struct Traversal {
     idz = 1.0f / dz;
     oct = (idx < 0.0f ? 1u : 0u) | (idy < 0.0f ? 2u : 0u) | (idz < 0.0f ? 4u : 0u);
     hit.slot = 0xFFFFFFFFu;
-    hit.id = 0xFFFFFFFFu;
     hit.rank = 0xFFFFFFFFu;
-    hit.obj = 0xFFFFFFFFu;
     hit.t = INFINITY;
     hit.d2 = INFINITY;
     tprune = INFINITY;
-    st.shared = stack_shared;
-    st.stride = stack_stride;
-    st.sp = 0;
+    st.bind(stack_shared, stack_stride);
     ng = make_uint2(0u, (1u << (24 + oct)) | 1u);  // the root, as inner slot 0
     tg = make_uint2(0u, 0u);
   }
 
   // kPostpone: triangle postponing. While fewer than a fifth of the warp's active lanes have
   // triangles to test, a lane that could still expand nodes parks its triangle group on its
-  // stack, so the warp runs one phase at a time. Without it a step expands one node and then
-  // tests all triangles of that node's hit leaves. (The visit order never changes the result:
-  // the closest hit is an arg-min over the same candidates.)
+  // stack, so the warp runs one phase at a time. Without it a lane with pending triangles tests
+  // one of them per step and a lane without expands a node. (The visit order never changes the
+  // result: the closest hit is an arg-min over the same candidates.)
   template <bool kStats, bool kPostpone = false>
   SWR_HD bool step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
                    const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
@@ -196,8 +253,8 @@ struct Traversal {
         const float qfz = byte_f(i < 4 ? fz0 : fz1, i & 3);
         const float tnx = fmaf(qnx, ax, bx), tny = fmaf(qny, ay, by), tnz = fmaf(qnz, az, bz);
         const float tfx = fmaf(qfx, ax, bx), tfy = fmaf(qfy, ay, by), tfz = fmaf(qfz, az, bz);
-        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tprune));
+        const float tn = fmax3(tnx, tny, fmaxf(tnz, 0.0f));
+        const float tf = fmin3(tfx, tfy, fminf(tfz, tprune));
         const bool is_inner = (imask >> i) & 1u;
         if (tn <= tf && (is_inner || m != 0u)) {
           if (is_inner) inner |= 1u << (i ^ (int)oct);
@@ -210,7 +267,11 @@ struct Traversal {
       tri_now = true;
     }
 
-    while (tri_now && tg.y) {
+    // At most one triangle per step: a lane with many candidate triangles then holds the warp
+    // for one test per step while the other lanes go on expanding nodes (measured on the
+    // terrain workload: 24.5 ms per image against 28.4 ms when a step tests all of them).
+    do {
+      if (!(tri_now && tg.y)) break;
       const uint32_t j = (uint32_t)ffs(tg.y) - 1u;
       tg.y &= tg.y - 1u;
       const uint32_t s = tg.x + j;
@@ -218,22 +279,19 @@ struct Traversal {
       const float4* tp = tris + (size_t)s * kTriF4;
       const float4 a = ldg4(tp + 0), b = ldg4(tp + 1), c = ldg4(tp + 2);
       float t, d2;
-      if (!ref_intersect(o, d, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y), mk(b.z, b.w, c.x), t, d2))
-        continue;
+      if (!ref_intersect(o, d, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y), mk(b.z, b.w, c.x), t, d2)) break;
       const uint32_t rank = f2bits(c.z);
-      if (!(d2 < hit.d2 || (d2 == hit.d2 && rank < hit.rank))) continue;
+      if (!(d2 < hit.d2 || (d2 == hit.d2 && rank < hit.rank))) break;
       const uint32_t obj = f2bits(c.w);
       const f3 inv = vinv(d);  // exact reciprocal of the reference's slab tests
-      if (!ref_slab(tri_boxes + (size_t)s * 6, tri_boxes + (size_t)s * 6 + 3, o, inv)) continue;
-      if (!ref_slab(obj_boxes + (size_t)obj * 6, obj_boxes + (size_t)obj * 6 + 3, o, inv)) continue;
+      if (!ref_slab(tri_boxes + (size_t)s * 6, tri_boxes + (size_t)s * 6 + 3, o, inv)) break;
+      if (!ref_slab(obj_boxes + (size_t)obj * 6, obj_boxes + (size_t)obj * 6 + 3, o, inv)) break;
       hit.slot = s;
-      hit.id = f2bits(c.y);
       hit.rank = rank;
-      hit.obj = obj;
       hit.t = t;
       hit.d2 = d2;
       tprune = t * kPruneSlack;
-    }
+    } while (false);
 
     if (!(ng.y & 0xFF000000u) && tg.y == 0) {
       if (st.sp == 0) return true;
@@ -256,8 +314,16 @@ SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __rest
   tr.init(o, d, stack_shared, stack_stride);
   while (!tr.template step<kStats, kPostpone>(nodes, tris, tri_boxes, obj_boxes, stats)) {
   }
-  hit = tr.hit;
-  return hit.slot != 0xFFFFFFFFu;
+  hit.slot = tr.hit.slot;
+  hit.rank = tr.hit.rank;
+  hit.t = tr.hit.t;
+  hit.d2 = tr.hit.d2;
+  hit.id = hit.obj = 0xFFFFFFFFu;
+  if (hit.slot == 0xFFFFFFFFu) return false;
+  const float4 c = ldg4(tris + (size_t)hit.slot * kTriF4 + 2);
+  hit.id = f2bits(c.y);
+  hit.obj = f2bits(c.w);
+  return true;
 }
 
 }  // namespace swrx
