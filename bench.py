@@ -449,6 +449,7 @@ def main():
         dist = dist_mod
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import master_thesis_b200 as swr
+    from master_thesis_b200 import sharding
 
     t0 = time.time()
     sd = swr.load_scene(files["scene"], files["basepath"])
@@ -507,10 +508,8 @@ def main():
     barrier()
     clk = clocks.stop()
 
-    tot = torch.tensor([sum(step_ms), sum(e2e_ms)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    total_ms, total_e2e_ms = float(tot[0]), float(tot[1])
+    # the job's time is the slowest rank's (device time, each rank rendering its own images)
+    total_ms, total_e2e_ms = sharding.max_over_ranks([sum(step_ms), sum(e2e_ms)])
     samples = W * H * spp * world * args.steps
     value = samples / (total_ms / 1e3) / 1e6
     e2e_value = samples / (total_e2e_ms / 1e3) / 1e6
