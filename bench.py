@@ -33,7 +33,7 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # name: scene parameters, image, spp, depth
     "c2": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=64,
-               depth=8, seed=2024),
+               depth=8, seed=2024, microbench_rays=1 << 24),
     "c1": dict(kind="cornell", W=256, H=256, spp=16, depth=5, seed=1),
     # the terrain scene at a reduced image size, for profiler captures of single kernel launches
     "c2s": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=16,
@@ -154,6 +154,42 @@ def cpu_reference(cfg, files, threads, budget_s, impl_bin):
     res = run(pixels)
     res["load_s_probe"] = probe["load_s"]
     return res
+
+
+def traversal_microbench(scene, sd, n, steps, flush, stream):
+    """Closest-hit queries only (swr_trace_closest on device buffers): n rays with origins uniform
+    in the scene's bounding box and directions uniform on the sphere. Hit ids of these rays are
+    checked against the oracle by tests/test_gpu_trace.py."""
+    import torch
+    from master_thesis_b200 import scenes
+    ro, rd = scenes.uniform_rays(n, sd.vpos.min(0), sd.vpos.max(0), seed=16)
+    hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    counts = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    scene.trace(ro, rd, out=hits, counts=counts, stream=stream)  # node/triangle counts (untimed)
+    torch.cuda.synchronize()
+    nodes = float(counts[:, 0].double().mean())
+    tris = float(counts[:, 1].double().mean())
+    miss = float((hits[:, 0] == -1).double().mean())
+    for _ in range(3):
+        scene.trace(ro, rd, out=hits, stream=stream)
+    ms = []
+    for _ in range(max(steps, 1)):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        scene.trace(ro, rd, out=hits, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = sum(ms) / len(ms)
+    per_ray = 32 + 16 + 80 * nodes + 48 * tris
+    peak, peak_kind = measured_peaks()
+    achieved = n * per_ray / (t / 1e3) / 1e9
+    return {"rays": n, "mrays_per_s": n / (t / 1e3) / 1e6, "ms_per_launch": t, "miss_fraction": miss,
+            "node_visits_per_ray": nodes, "tri_tests_per_ray": tris,
+            "roofline": {"bound": "hbm", "kernel": "k_trace_closest", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_ray": per_ray}}
 
 
 def _events_ms(fn, steps, flush):
@@ -482,15 +518,23 @@ def main():
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     barrier()
-    step_ms, profs = [], []
+    step_ms, plain = [], []
     for _ in range(args.steps):
         flush.fill_(1.0)  # evict L2 between steps (256 MB > 126 MB L2)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        _, pr = render(out, profile=True)
+        _, pr = render(out)
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
+        plain.append(pr)
+    barrier()
+    # per-kernel device times: the same K renders again with CUDA events around every launch (on
+    # the launching stream); kept out of the steps above because the events cost a few us each
+    profs = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        _, pr = render(out, profile=True)
         profs.append(pr)
     barrier()
     # end to end: the same call with a pinned host output buffer
@@ -505,6 +549,10 @@ def main():
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
         e2e_prof.append(pr)
+    barrier()
+    micro = None
+    if cfg.get("microbench_rays"):
+        micro = traversal_microbench(scene, sd, cfg["microbench_rays"], args.steps, flush, stream)
     barrier()
     clk = clocks.stop()
 
@@ -529,8 +577,8 @@ def main():
     if tp and tp.get("scene") == cfg["kind"]:
         # the captured launch's DRAM bytes per ray, scaled to this run's rays per launch
         traffic = tp["dram_bytes_per_ray"] * rays_per_step * args.steps / max(launches, 1)
-    mrays = sum(p["rays"] for p in profs) / (sum(step_ms) / 1e3) / 1e6
-    launches_total = sum(p["launches"] for p in profs)
+    mrays = sum(p["rays"] for p in plain) / (sum(step_ms) / 1e3) / 1e6
+    launches_total = sum(p["launches"] for p in plain)
 
     if rank == 0:
         cpu = None
@@ -565,8 +613,10 @@ def main():
                          "algorithmic_bytes_per_launch": per_launch_bytes,
                          "node_visits_per_ray": cprof["node_visits"] / max(cprof["bounce_rays"], 1),
                          "tri_tests_per_ray": cprof["tri_tests"] / max(cprof["bounce_rays"], 1)},
+            "traversal_microbench": micro,
             "kernel_ms_per_step": {k: sum(p[k] for p in profs) / args.steps for k in
                                    ("trace_ms", "shade_ms", "camera_ms", "resolve_ms")},
+            "kernel_timing": "per-kernel CUDA events over K further renders of the same image",
             "gpu_launches": int(launches_total),
             "clocks": clk,
             "cpu_baseline": cpu,

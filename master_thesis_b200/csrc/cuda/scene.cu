@@ -74,28 +74,50 @@ int device_input(const float* p, size_t bytes, cudaStream_t stream, void** tmp, 
   return SWR_OK;
 }
 
+// Persistent closest-hit queries with per-lane refill: each lane keeps one ray's resumable
+// traversal; once at least kRefill lanes of a warp are idle the warp takes that many new rays
+// with one atomic on the cursor, so lanes stay busy while long rays are still walking the tree.
+constexpr unsigned kRefill = 8;
+
 template <bool kStats>
 __global__ void __launch_bounds__(kTraceBlock)
     k_trace_closest(DevScene sc, const float4* __restrict__ ro, const float4* __restrict__ rd,
                     uint64_t n, uint4* __restrict__ out, uint2* __restrict__ counts,
                     unsigned long long* __restrict__ cursor) {
   __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
-  const int lane = threadIdx.x & 31;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  swrx::Traversal tr;
+  swrx::TraceStats st{0, 0};
+  bool active = false, exhausted = false;
+  uint64_t ray = 0;
   for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(cursor, 32ull);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    const uint64_t i = base + lane;
-    if (i < n) {
-      const float4 o = ro[i], d = rd[i];
-      swrx::Hit h;
-      swrx::TraceStats st{0, 0};
-      swrx::trace_closest<kStats>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes,
-                                  swrx::mk(o.x, o.y, o.z), swrx::mk(d.x, d.y, d.z),
-                                  stack + threadIdx.x, kTraceBlock, h, &st);
-      out[i] = make_uint4(h.id, h.obj, __float_as_uint(h.d2), __float_as_uint(h.t));
-      if (kStats) counts[i] = make_uint2(st.nodes, st.tris);
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= kRefill) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(cursor, (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) exhausted = true;
+      if (!active) {
+        const uint64_t j = base + (unsigned)__popc(idle & lt);
+        if (j < n) {
+          const float4 o = ro[j], d = rd[j];
+          tr.init(swrx::mk(o.x, o.y, o.z), swrx::mk(d.x, d.y, d.z), stack + threadIdx.x, kTraceBlock);
+          st = swrx::TraceStats{0, 0};
+          ray = j;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active && tr.template step<kStats>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, &st)) {
+      const swrx::Hit h = tr.result(sc.tris);
+      out[ray] = make_uint4(h.id, h.obj, __float_as_uint(h.d2), __float_as_uint(h.t));
+      if (kStats) counts[ray] = make_uint2(st.nodes, st.tris);
+      active = false;
     }
   }
 }

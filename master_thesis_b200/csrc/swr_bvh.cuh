@@ -186,6 +186,22 @@ struct Traversal {
     tg = make_uint2(0u, 0u);
   }
 
+  // The finished ray's hit with its triangle id and object read from the triangle record.
+  SWR_HD Hit result(const float4* __restrict__ tris) const {
+    Hit h;
+    h.slot = hit.slot;
+    h.rank = hit.rank;
+    h.t = hit.t;
+    h.d2 = hit.d2;
+    h.id = h.obj = 0xFFFFFFFFu;
+    if (h.slot != 0xFFFFFFFFu) {
+      const float4 c = ldg4(tris + (size_t)h.slot * kTriF4 + 2);
+      h.id = f2bits(c.y);
+      h.obj = f2bits(c.w);
+    }
+    return h;
+  }
+
   // kPostpone: triangle postponing. While fewer than a fifth of the warp's active lanes have
   // triangles to test, a lane that could still expand nodes parks its triangle group on its
   // stack, so the warp runs one phase at a time. Without it a lane with pending triangles tests
@@ -314,16 +330,8 @@ SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __rest
   tr.init(o, d, stack_shared, stack_stride);
   while (!tr.template step<kStats, kPostpone>(nodes, tris, tri_boxes, obj_boxes, stats)) {
   }
-  hit.slot = tr.hit.slot;
-  hit.rank = tr.hit.rank;
-  hit.t = tr.hit.t;
-  hit.d2 = tr.hit.d2;
-  hit.id = hit.obj = 0xFFFFFFFFu;
-  if (hit.slot == 0xFFFFFFFFu) return false;
-  const float4 c = ldg4(tris + (size_t)hit.slot * kTriF4 + 2);
-  hit.id = f2bits(c.y);
-  hit.obj = f2bits(c.w);
-  return true;
+  hit = tr.result(tris);
+  return hit.slot != 0xFFFFFFFFu;
 }
 
 }  // namespace swrx

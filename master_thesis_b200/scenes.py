@@ -381,3 +381,25 @@ def terrain(seed, root, cells=1024, tile=16, spheres=64, sphere_subdiv=4, lights
     write_camera(cam, (0.0, 1.3, 2.2), (-0.5, -0.35))
     ntri = ntiles * ntiles * fi.shape[0] + spheres * len(sf) + 2 * lights
     return dict(scene=scene, camera=cam, basepath=base, triangles=ntri)
+
+
+def uniform_rays(n, lo, hi, seed, device="cuda"):
+    """Closest-hit microbenchmark rays as two (n, 4) float32 tensors: origins uniform in the box
+    [lo, hi], directions uniform on the unit sphere (z = 2u - 1, phi = 2 pi v, the mapping of the
+    reference's random direction, random.cpp:16-29). Seeded torch generator on `device`."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    u = torch.rand((n, 5), generator=g, device=device, dtype=torch.float32)
+    lo_t = torch.as_tensor(np.asarray(lo, np.float32), device=device)
+    hi_t = torch.as_tensor(np.asarray(hi, np.float32), device=device)
+    o = torch.zeros((n, 4), dtype=torch.float32, device=device)
+    o[:, :3] = lo_t + (hi_t - lo_t) * u[:, :3]
+    z = 2.0 * u[:, 3] - 1.0
+    r = torch.sqrt(torch.clamp(1.0 - z * z, min=0.0))
+    phi = (2.0 * math.pi) * u[:, 4]
+    d = torch.zeros((n, 4), dtype=torch.float32, device=device)
+    d[:, 0] = r * torch.cos(phi)
+    d[:, 1] = r * torch.sin(phi)
+    d[:, 2] = z
+    return o, d

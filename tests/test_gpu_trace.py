@@ -78,3 +78,23 @@ def test_gpu_trace_stats_counts():
     c = counts.cpu().numpy()
     assert np.array_equal(h.cpu().numpy().view(np.uint32)[:, 0], g["hit_id"])
     assert (c[:, 0] >= 1).all() and c[:, 1].mean() > 0
+
+
+def test_gpu_terrain_microbench_rays_vs_oracle(tmp_path):
+    """The default bench's closest-hit microbenchmark: the full terrain (2,424,840 triangles) and
+    16M rays from scenes.uniform_rays; every 64th ray's hit (262,144 rays spread over the whole
+    set) must be bit-identical to the oracle's."""
+    s = scenes.terrain(2024, str(tmp_path), cells=1024, tile=16, spheres=64, sphere_subdiv=4, lights=4)
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    assert sd.num_triangles == 2424840 and sd.ranks_exact
+    sc = swr.Scene(sd)
+    ro, rd = scenes.uniform_rays(1 << 24, sd.vpos.min(0), sd.vpos.max(0), seed=16)
+    h = sc.trace(ro, rd)
+    torch.cuda.synchronize()
+    h = h[::64].cpu().numpy().view(np.uint32)
+    osc = O.OracleScene.from_scene_data(sd)
+    otri, od2, ot = osc.trace(ro[::64].cpu().numpy(), rd[::64].cpu().numpy())
+    assert np.array_equal(h[:, 0], otri)
+    assert np.array_equal(h[:, 2], od2.view(np.uint32))
+    assert np.array_equal(h[:, 3], ot.view(np.uint32))
+    assert 0.05 < float((otri != 0xFFFFFFFF).mean()) < 0.95
