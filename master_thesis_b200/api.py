@@ -133,10 +133,12 @@ def _stream_handle(stream):
 class Scene:
     """Device scene (wide BVH + triangle records) built from SceneData."""
 
-    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0):
+    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0, builder="host", radius=0):
+        """builder: "host" (binned SAH on the host) or "device" (clustering + collapse on the GPU)."""
         self.data = data
         d = data.desc()
-        o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct)
+        b = {"host": N.BUILD_HOST, "device": N.BUILD_DEVICE}[builder]
+        o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius)
         self._h = ctypes.c_void_p()
         check(N.lib.swr_scene_create(ctypes.byref(d), ctypes.byref(o), ctypes.byref(self._h)))
 

@@ -26,7 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp
 
 HOST_SRC = ["host/surface.cpp", "host/ref_bvh.cpp", "host/wide_bvh.cpp", "host/derive.cpp",
             "host/capi_host.cpp", "host/scene_pack.cpp"]
-CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu", "cuda/batch.cu"]
+CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu", "cuda/batch.cu", "cuda/build.cu"]
 CLI_SRC = "cli/swr_main.cpp"
 
 

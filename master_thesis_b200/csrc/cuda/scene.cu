@@ -7,6 +7,7 @@
 
 #include "../host/capi_common.h"
 #include "../host/scene_pack.h"
+#include "build_device.h"
 #include "swr_internal.cuh"
 
 namespace swr {
@@ -36,6 +37,73 @@ int upload(void** dst, const std::vector<T>& v) {
                                         " bytes failed: " + cudaGetErrorString(e));
   }
   if (!v.empty()) SWR_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return SWR_OK;
+}
+
+// Triangle-id-ordered records -> leaf order of the device-built BVH.
+__global__ void k_permute(const uint32_t* __restrict__ order, uint32_t n, const float4* __restrict__ tris_in,
+                          const float4* __restrict__ shade_in, const float* __restrict__ box_in,
+                          const float* __restrict__ alb_in, float4* __restrict__ tris, float4* __restrict__ shade,
+                          float* __restrict__ boxes, float* __restrict__ alb, uint32_t* __restrict__ slot_of) {
+  const uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= n) return;
+  const uint32_t t = order[sl];
+  for (int k = 0; k < 3; ++k) tris[3 * (size_t)sl + k] = tris_in[3 * (size_t)t + k];
+  for (int k = 0; k < 4; ++k) shade[4 * (size_t)sl + k] = shade_in[4 * (size_t)t + k];
+  for (int k = 0; k < 6; ++k) boxes[6 * (size_t)sl + k] = box_in[6 * (size_t)t + k];
+  for (int k = 0; k < 3; ++k) alb[3 * (size_t)sl + k] = alb_in[3 * (size_t)t + k];
+  slot_of[t] = sl;
+}
+
+// Device BVH build (swr_build_opts.builder == SWR_BUILD_DEVICE): pk holds the records in
+// triangle-id order and the traversal boxes; the wide BVH is built on the GPU and the records
+// are permuted into its leaf order there.
+int device_pack(swr_scene* s, const swr_scene_desc* d, const swr_build_opts* opts, PackedScene& pk) {
+  const uint32_t n = d->num_triangles;
+  DeviceBuildOptions o;
+  if (opts) {
+    if (opts->max_leaf) o.max_leaf = opts->max_leaf;
+    if (opts->radius) o.radius = opts->radius;
+    if (opts->leaf_cost_pct) o.prim_cost = opts->leaf_cost_pct / 100.0;
+  }
+  cudaStream_t st = nullptr;
+  void *boxes = nullptr, *tris = nullptr, *shade = nullptr, *tboxes = nullptr, *alb = nullptr;
+  struct Free {
+    void** p[5];
+    ~Free() {
+      for (void** q : p)
+        if (*q) cudaFree(*q);
+    }
+  } fr{{&boxes, &tris, &shade, &tboxes, &alb}};
+  int rc;
+  if ((rc = upload(&boxes, pk.prim_boxes)) || (rc = upload(&tris, pk.tris)) || (rc = upload(&shade, pk.shade)) ||
+      (rc = upload(&tboxes, pk.tri_boxes)) || (rc = upload(&alb, pk.albedo)))
+    return rc;
+  DeviceBvh bvh;
+  rc = build_wide_bvh_device((const float*)boxes, n, o, bvh, st);
+  s->d_nodes = bvh.d_nodes;  // released with the scene on every path
+  struct FreeOrder {
+    uint32_t* p;
+    ~FreeOrder() {
+      if (p) cudaFree(p);
+    }
+  } fo{bvh.d_prim_order};
+  if (rc) return rc;
+  if (2 * bvh.depth + 2 > 64) return set_error(SWR_ERR_UNSUPPORTED, "swr: BVH deeper than the traversal stack");
+  SWR_CUDA(cudaMalloc(&s->d_tris, (size_t)n * 3 * sizeof(float4)));
+  SWR_CUDA(cudaMalloc(&s->d_shade, (size_t)n * 4 * sizeof(float4)));
+  SWR_CUDA(cudaMalloc(&s->d_tri_boxes, (size_t)n * 6 * sizeof(float)));
+  SWR_CUDA(cudaMalloc(&s->d_albedo, (size_t)n * 3 * sizeof(float)));
+  SWR_CUDA(cudaMalloc(&s->d_slot_of, (size_t)n * sizeof(uint32_t)));
+  k_permute<<<(n + 255) / 256, 256, 0, st>>>(bvh.d_prim_order, n, (const float4*)tris, (const float4*)shade,
+                                            (const float*)tboxes, (const float*)alb, (float4*)s->d_tris,
+                                            (float4*)s->d_shade, (float*)s->d_tri_boxes, (float*)s->d_albedo,
+                                            (uint32_t*)s->d_slot_of);
+  SWR_CUDA(cudaGetLastError());
+  pk.slot_to_id.resize(n);
+  SWR_CUDA(cudaMemcpy(pk.slot_to_id.data(), bvh.d_prim_order, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  pk.num_nodes = bvh.num_nodes;
+  pk.depth = bvh.depth;
   return SWR_OK;
 }
 
@@ -200,8 +268,12 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
   if (!out) return set_error(SWR_ERR_INVALID, "swr: null output handle");
   *out = nullptr;
   try {
+    const uint32_t builder = opts ? opts->builder : (uint32_t)SWR_BUILD_HOST;
+    if (builder != SWR_BUILD_HOST && builder != SWR_BUILD_DEVICE)
+      return set_error(SWR_ERR_INVALID, "swr: unknown builder");
+    const bool on_device = builder == SWR_BUILD_DEVICE;
     swr::PackedScene pk;
-    int rc = swr::pack_scene(d, opts, pk);
+    int rc = swr::pack_scene(d, opts, pk, !on_device);
     if (rc) return rc;
     std::unique_ptr<swr_scene> s(new swr_scene());
     SWR_CUDA(cudaGetDevice(&s->device));
@@ -212,14 +284,18 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
         if (p) swr_scene_destroy(p);
       }
     } guard{s.get()};
-    if ((rc = swr::upload(&s->d_nodes, pk.nodes))) return rc;
-    if ((rc = swr::upload(&s->d_tris, pk.tris))) return rc;
-    if ((rc = swr::upload(&s->d_shade, pk.shade))) return rc;
-    if ((rc = swr::upload(&s->d_tri_boxes, pk.tri_boxes))) return rc;
+    if (on_device) {
+      if ((rc = swr::device_pack(s.get(), d, opts, pk))) return rc;
+    } else {
+      if ((rc = swr::upload(&s->d_nodes, pk.nodes))) return rc;
+      if ((rc = swr::upload(&s->d_tris, pk.tris))) return rc;
+      if ((rc = swr::upload(&s->d_shade, pk.shade))) return rc;
+      if ((rc = swr::upload(&s->d_tri_boxes, pk.tri_boxes))) return rc;
+      if ((rc = swr::upload(&s->d_albedo, pk.albedo))) return rc;
+      if ((rc = swr::upload(&s->d_slot_of, pk.slot_of))) return rc;
+    }
     if ((rc = swr::upload(&s->d_obj_boxes, pk.obj_boxes))) return rc;
     if ((rc = swr::upload(&s->d_mats, pk.mats))) return rc;
-    if ((rc = swr::upload(&s->d_albedo, pk.albedo))) return rc;
-    if ((rc = swr::upload(&s->d_slot_of, pk.slot_of))) return rc;
     s->scratch_bytes = 256;
     SWR_CUDA(cudaMalloc(&s->d_scratch, s->scratch_bytes));
     SWR_CUDA(cudaMemset(s->d_scratch, 0, s->scratch_bytes));

@@ -20,7 +20,7 @@ static inline float ubits(uint32_t u) {
   return f;
 }
 
-int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene& out) {
+int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene& out, bool host_bvh) {
   int rc = validate_desc(d);
   if (rc) return rc;
   Derived dv;
@@ -59,10 +59,23 @@ int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene&
     if (opts->leaf_cost_pct) wo.prim_cost = opts->leaf_cost_pct / 100.0;
   }
   if (wo.max_leaf > 3) return set_error(SWR_ERR_INVALID, "swr: max_leaf must be 1..3");
-  WideBvh bvh = build_wide_bvh(prims, wo);
-  // a traversal keeps at most one node group and one postponed triangle group per level
-  if (2 * bvh.depth + 2 > kMaxStack)
-    return set_error(SWR_ERR_UNSUPPORTED, "swr: BVH deeper than the traversal stack");
+  if (opts && opts->radius > 256) return set_error(SWR_ERR_INVALID, "swr: radius must be 0..256");
+  WideBvh bvh;
+  if (host_bvh) {
+    bvh = build_wide_bvh(prims, wo);
+    // a traversal keeps at most one node group and one postponed triangle group per level
+    if (2 * bvh.depth + 2 > kMaxStack)
+      return set_error(SWR_ERR_UNSUPPORTED, "swr: BVH deeper than the traversal stack");
+  } else {
+    bvh.prim_order.resize(nt);
+    for (uint32_t t = 0; t < nt; ++t) bvh.prim_order[t] = t;
+    out.prim_boxes.resize((size_t)nt * 6);
+    for (uint32_t t = 0; t < nt; ++t)
+      for (int k = 0; k < 3; ++k) {
+        out.prim_boxes[6 * (size_t)t + k] = prims[t].lo[k];
+        out.prim_boxes[6 * (size_t)t + 3 + k] = prims[t].hi[k];
+      }
+  }
 
   const uint32_t ns = (uint32_t)bvh.prim_order.size();
   out.nodes = std::move(bvh.words);

@@ -21,10 +21,13 @@ struct PackedScene {
   std::vector<float> albedo;      // 3 per slot
   std::vector<uint32_t> slot_of;  // triangle id -> slot
   std::vector<uint32_t> slot_to_id;
+  std::vector<float> prim_boxes;  // without the host BVH: 6 per triangle, the traversal boxes
   uint32_t num_nodes = 0, depth = 0;
 };
 
-// Validates and packs; returns SWR_OK or an error code (message in swr_last_error).
-int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene& out);
+// Validates and packs; returns SWR_OK or an error code (message in swr_last_error). With
+// host_bvh false no BVH is built: the records are in triangle-id order (slot = id) and
+// prim_boxes holds the boxes for the caller's builder.
+int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene& out, bool host_bvh = true);
 
 }  // namespace swr
