@@ -48,23 +48,27 @@ void derive(const swr_scene_desc& d, Derived& out) {
   out.e1.resize(nt);
   out.den.resize(nt);
   out.tri_box.assign(nt, Box());
-  for (size_t t = 0; t < nt; ++t) {
-    const V3 a = P(d.tri_vertices[3 * t]), b = P(d.tri_vertices[3 * t + 1]),
-             c = P(d.tri_vertices[3 * t + 2]);
-    const V3 e0 = sub(b, a), e1 = sub(c, a);
-    const float d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
-    out.v0[t] = a;
-    out.e0[t] = e0;
-    out.e1[t] = e1;
-    out.den[t] = v4(d00, d01, d11, d00 * d11 - d01 * d01);
-    out.tri_box[t].add(a);
-    out.tri_box[t].add(b);
-    out.tri_box[t].add(c);
-  }
+  parallel_for(nt, [&](size_t t0, size_t t1) {
+    for (size_t t = t0; t < t1; ++t) {
+      const V3 a = P(d.tri_vertices[3 * t]), b = P(d.tri_vertices[3 * t + 1]),
+               c = P(d.tri_vertices[3 * t + 2]);
+      const V3 e0 = sub(b, a), e1 = sub(c, a);
+      const float d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
+      out.v0[t] = a;
+      out.e0[t] = e0;
+      out.e1[t] = e1;
+      out.den[t] = v4(d00, d01, d11, d00 * d11 - d01 * d01);
+      out.tri_box[t].add(a);
+      out.tri_box[t].add(b);
+      out.tri_box[t].add(c);
+    }
+  });
   out.obj_box.assign(no, Box());
-  for (size_t o = 0; o < no; ++o)
-    for (uint32_t v = d.object_first_vertex[o]; v < d.object_first_vertex[o + 1]; ++v)
-      out.obj_box[o].add(P(v));
+  parallel_for(no, [&](size_t o0, size_t o1) {
+    for (size_t o = o0; o < o1; ++o)
+      for (uint32_t v = d.object_first_vertex[o]; v < d.object_first_vertex[o + 1]; ++v)
+        out.obj_box[o].add(P(v));
+  });
 }
 
 }  // namespace swr

@@ -44,11 +44,13 @@ int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene&
     return set_error(SWR_ERR_INVALID, "swr: scene has non-finite vertex coordinates");
   const float eps = ext * (1.0f / 65536.0f) + mabs * (1.0f / 1048576.0f) + 1e-30f;
   std::vector<PrimBox> prims(nt);
-  for (uint32_t t = 0; t < nt; ++t)
-    for (int k = 0; k < 3; ++k) {
-      prims[t].lo[k] = dv.tri_box[t].lo[k] - eps;
-      prims[t].hi[k] = dv.tri_box[t].hi[k] + eps;
-    }
+  parallel_for(nt, [&](size_t t0, size_t t1) {
+    for (size_t t = t0; t < t1; ++t)
+      for (int k = 0; k < 3; ++k) {
+        prims[t].lo[k] = dv.tri_box[t].lo[k] - eps;
+        prims[t].hi[k] = dv.tri_box[t].hi[k] + eps;
+      }
+  });
   WideBvhOptions wo;
   if (opts) {
     if (opts->sah_bins) wo.sah_bins = opts->sah_bins;
@@ -89,29 +91,31 @@ int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene&
   out.mats.assign((size_t)no * 3, make_float4(0, 0, 0, 0));
   out.slot_of.assign(nt, 0u);
   out.slot_to_id.assign(ns, 0u);
-  for (uint32_t sl = 0; sl < ns; ++sl) {
-    const uint32_t t = bvh.prim_order[sl];
-    out.slot_of[t] = sl;
-    out.slot_to_id[sl] = t;
-    const uint32_t obj = d->tri_object[t];
-    const uint32_t rank = d->tri_rank ? d->tri_rank[t] : t;
-    const V3 &v0 = dv.v0[t], &e0 = dv.e0[t], &e1 = dv.e1[t];
-    out.tris[3 * (size_t)sl + 0] = make_float4(v0[0], v0[1], v0[2], e0[0]);
-    out.tris[3 * (size_t)sl + 1] = make_float4(e0[1], e0[2], e1[0], e1[1]);
-    out.tris[3 * (size_t)sl + 2] = make_float4(e1[2], ubits(t), ubits(rank), ubits(obj));
-    out.shade[4 * (size_t)sl] = make_float4(dv.den[t][0], dv.den[t][1], dv.den[t][2], dv.den[t][3]);
-    for (int c = 0; c < 3; ++c) {
-      const uint32_t vi = d->tri_vertices[3 * (size_t)t + c];
-      const float* nv = d->vertex_normal + 3 * (size_t)vi;
-      out.shade[4 * (size_t)sl + 1 + c] = make_float4(nv[0], nv[1], nv[2], 0.0f);
+  parallel_for(ns, [&](size_t s0, size_t s1) {
+    for (uint32_t sl = (uint32_t)s0; sl < (uint32_t)s1; ++sl) {
+      const uint32_t t = bvh.prim_order[sl];
+      out.slot_of[t] = sl;
+      out.slot_to_id[sl] = t;
+      const uint32_t obj = d->tri_object[t];
+      const uint32_t rank = d->tri_rank ? d->tri_rank[t] : t;
+      const V3 &v0 = dv.v0[t], &e0 = dv.e0[t], &e1 = dv.e1[t];
+      out.tris[3 * (size_t)sl + 0] = make_float4(v0[0], v0[1], v0[2], e0[0]);
+      out.tris[3 * (size_t)sl + 1] = make_float4(e0[1], e0[2], e1[0], e1[1]);
+      out.tris[3 * (size_t)sl + 2] = make_float4(e1[2], ubits(t), ubits(rank), ubits(obj));
+      out.shade[4 * (size_t)sl] = make_float4(dv.den[t][0], dv.den[t][1], dv.den[t][2], dv.den[t][3]);
+      for (int c = 0; c < 3; ++c) {
+        const uint32_t vi = d->tri_vertices[3 * (size_t)t + c];
+        const float* nv = d->vertex_normal + 3 * (size_t)vi;
+        out.shade[4 * (size_t)sl + 1 + c] = make_float4(nv[0], nv[1], nv[2], 0.0f);
+      }
+      for (int k = 0; k < 3; ++k) {
+        out.tri_boxes[6 * (size_t)sl + k] = dv.tri_box[t].lo[k];
+        out.tri_boxes[6 * (size_t)sl + 3 + k] = dv.tri_box[t].hi[k];
+        out.albedo[3 * (size_t)sl + k] =
+            d->tri_albedo ? d->tri_albedo[3 * (size_t)t + k] : d->materials[obj].color[k];
+      }
     }
-    for (int k = 0; k < 3; ++k) {
-      out.tri_boxes[6 * (size_t)sl + k] = dv.tri_box[t].lo[k];
-      out.tri_boxes[6 * (size_t)sl + 3 + k] = dv.tri_box[t].hi[k];
-      out.albedo[3 * (size_t)sl + k] =
-          d->tri_albedo ? d->tri_albedo[3 * (size_t)t + k] : d->materials[obj].color[k];
-    }
-  }
+  });
   for (uint32_t o = 0; o < no; ++o) {
     const swr_material& m = d->materials[o];
     for (int k = 0; k < 3; ++k) {

@@ -5,12 +5,16 @@
 #include "surface.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <exception>
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <thread>
+#include <unordered_map>
 
 #include "ref_bvh.h"
 
@@ -345,16 +349,14 @@ static bool ends_with(const std::string& v, const std::string& e) {
   return e.size() <= v.size() && std::equal(e.rbegin(), e.rend(), v.rbegin());
 }
 
-uint32_t SceneBuilder::add_mesh(const std::string& name, Mesh mesh) {
-  auto it = mesh_ids_.find(name);
-  if (it != mesh_ids_.end()) return it->second;
+void prepare_mesh(const std::string& name, Mesh& mesh, const LoadOptions& opt) {
   if (mesh.num_tris() == 0)
     throw SurfaceError(kErrInvalid, "MeshManager", "mesh \"" + name + "\" has no triangles");
   for (uint32_t i : mesh.idx)
     if (i >= mesh.pos.size())
       throw SurfaceError(kErrInvalid, "MeshManager", "mesh \"" + name + "\" has a bad index");
   // topology of the reference's object-space BVH over triangle boxes (mesh.cpp:24-37)
-  if (mesh.num_tris() <= opt_.max_exact_order) {
+  if (mesh.num_tris() <= opt.max_exact_order) {
     std::vector<Box> boxes(mesh.num_tris());
     for (size_t t = 0; t < mesh.num_tris(); ++t) {
       boxes[t].add(mesh.pos[mesh.idx[3 * t + 0]]);
@@ -363,6 +365,18 @@ uint32_t SceneBuilder::add_mesh(const std::string& name, Mesh mesh) {
     }
     mesh.dfs = ref_bvh_leaf_order(boxes);
   }
+}
+
+uint32_t SceneBuilder::add_mesh(const std::string& name, Mesh mesh) {
+  auto it = mesh_ids_.find(name);
+  if (it != mesh_ids_.end()) return it->second;
+  prepare_mesh(name, mesh, opt_);
+  return add_prepared_mesh(name, std::move(mesh));
+}
+
+uint32_t SceneBuilder::add_prepared_mesh(const std::string& name, Mesh mesh) {
+  auto it = mesh_ids_.find(name);
+  if (it != mesh_ids_.end()) return it->second;
   uint32_t id = (uint32_t)s_.meshes.size();
   s_.meshes.push_back(std::move(mesh));
   mesh_ids_[name] = id;
@@ -407,18 +421,19 @@ void SceneBuilder::add_object(uint32_t mesh_id, const V3& position, const V3& sc
   s_.objects.push_back(o);
 }
 
+Mesh load_mesh_file(const std::string& basepath, const std::string& name) {
+  if (ends_with(name, ".obj")) return load_obj(basepath, name);
+  if (ends_with(name, ".stl")) return load_stl(name);
+  throw SurfaceError(kErrParse, "MeshManager", "unknown mesh type \"" + name + "\"");
+}
+
 void SceneBuilder::add_entry(const InputEntry& e, const std::string& basepath) {
   if (e.name == "Probes") return;
-  uint32_t mid;
-  if (has_mesh(e.name)) {
-    mid = mesh_id(e.name);
-  } else if (ends_with(e.name, ".obj")) {
-    mid = add_mesh(e.name, load_obj(basepath, e.name));
-  } else if (ends_with(e.name, ".stl")) {
-    mid = add_mesh(e.name, load_stl(e.name));
-  } else {
-    throw SurfaceError(kErrParse, "MeshManager", "unknown mesh type \"" + e.name + "\"");
-  }
+  const uint32_t mid = has_mesh(e.name) ? mesh_id(e.name) : add_mesh(e.name, load_mesh_file(basepath, e.name));
+  add_entry_object(e, mid);
+}
+
+void SceneBuilder::add_entry_object(const InputEntry& e, uint32_t mid) {
   V3 pos = e.get_v3("position");
   V3 scl = v3(1.0f, 1.0f, 1.0f);
   Rot rot;
@@ -471,11 +486,47 @@ HostScene SceneBuilder::finish() {
   return s;
 }
 
+// The mesh files named by a scene are read and prepared (parse, checks, reference leaf order)
+// concurrently, one mesh per task; objects are then assembled in file order. A failure is
+// reported at the first block that uses the failing mesh, in file order, as a sequential load
+// (the reference's MeshManager) reports it.
 HostScene load_scene_file(const std::string& scene_path, const std::string& basepath,
                           const LoadOptions& opt) {
   std::vector<InputEntry> entries = parse_input_file(scene_path);
+  std::vector<std::string> names;
+  std::unordered_map<std::string, size_t> index;
+  for (const auto& e : entries)
+    if (e.name != "Probes" && index.emplace(e.name, names.size()).second) names.push_back(e.name);
+  std::vector<Mesh> meshes(names.size());
+  std::vector<std::exception_ptr> errors(names.size());
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    for (size_t i; (i = next.fetch_add(1)) < names.size();) {
+      try {
+        Mesh m = load_mesh_file(basepath, names[i]);
+        prepare_mesh(names[i], m, opt);
+        meshes[i] = std::move(m);
+      } catch (...) {
+        errors[i] = std::current_exception();
+      }
+    }
+  };
+  unsigned nt = opt.threads ? opt.threads : std::max(1u, std::thread::hardware_concurrency());
+  nt = (unsigned)std::min<size_t>(nt, names.size());
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
   SceneBuilder b(opt);
-  for (const auto& e : entries) b.add_entry(e, basepath);
+  for (const auto& e : entries) {
+    if (e.name == "Probes") continue;
+    const size_t i = index.at(e.name);
+    if (!b.has_mesh(e.name)) {
+      if (errors[i]) std::rethrow_exception(errors[i]);
+      b.add_prepared_mesh(e.name, std::move(meshes[i]));
+    }
+    b.add_entry_object(e, b.mesh_id(e.name));
+  }
   return b.finish();
 }
 

@@ -113,18 +113,28 @@ struct LoadOptions {
   // Meshes / object counts above this size do not get the reference's exact BVH leaf order
   // (the reference's own builder is cubic in this size); ties then go to the lower index.
   uint32_t max_exact_order = 1u << 15;
+  uint32_t threads = 0;  // mesh files parsed concurrently by load_scene_file; 0 = all cores
 };
+
+// Reads a mesh named in a .scene block: ".obj" from basepath + "../res/obj/", ".stl" from
+// "../res/stl/"; any other name is a parse error (mesh_manager.cpp:17-28).
+Mesh load_mesh_file(const std::string& basepath, const std::string& name);
+
+// Checks a mesh and computes its reference leaf order (mesh.cpp:24-37); throws SurfaceError.
+void prepare_mesh(const std::string& name, Mesh& mesh, const LoadOptions& opt);
 
 // Adds one object (already parsed mesh + entry keys) the way MeshManager + GraphicsObject do.
 class SceneBuilder {
  public:
   explicit SceneBuilder(const LoadOptions& opt = LoadOptions()) : opt_(opt) {}
   uint32_t add_mesh(const std::string& name, Mesh mesh);  // returns mesh id (cached by name)
+  uint32_t add_prepared_mesh(const std::string& name, Mesh mesh);  // after prepare_mesh
   bool has_mesh(const std::string& name) const { return mesh_ids_.count(name) > 0; }
   uint32_t mesh_id(const std::string& name) const { return mesh_ids_.at(name); }
   void add_object(uint32_t mesh_id, const V3& position, const V3& scl, const Rot& rot,
                   const Material& mat);
   void add_entry(const InputEntry& e, const std::string& basepath);  // a .scene block
+  void add_entry_object(const InputEntry& e, uint32_t mesh_id);      // its keys, mesh resolved
   HostScene finish();  // computes reference visit ranks
 
  private:

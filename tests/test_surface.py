@@ -155,6 +155,34 @@ def test_obj_parsing_and_bad_indices(tmp_path):
     assert e.value.code == 2
 
 
+def test_concurrent_mesh_loading_reports_first_failure_in_file_order(tmp_path):
+    """Mesh files are read concurrently, but a failure is reported for the first block (in file
+    order) that hits one, as a sequential load reports it."""
+    root = tmp_path
+    for d in ("res/obj", "res/scene", "bin"):
+        os.makedirs(root / d, exist_ok=True)
+    (root / "res/obj/q.obj").write_text("v 0 0 0\nv 1 0 0\nv 1 1 0\nvn 0 0 1\nf 1//1 2//1 3//1\n")
+    (root / "res/obj/bad.obj").write_text("v 0 0 0\nvn 0 0 1\nf 1//1 2//1 3//1\n")
+    base = str(root / "bin") + "/"
+    cases = [
+        ("q.obj\n\tposition(0, 0, 0)\nmissing.obj\n\tposition(0, 0, 0)\nbad.obj\n\tposition(0, 0, 0)\n", 1),
+        ("q.obj\n\tposition(0, 0, 0)\nbad.obj\n\tposition(0, 0, 0)\nmissing.obj\n\tposition(0, 0, 0)\n", 2),
+        ("q.obj\n\tcolor(1, 1, 1)\nmissing.obj\n\tposition(0, 0, 0)\n", 2),  # no position in block 1
+        ("q.obj\n\tposition(0, 0, 0)\nthing.xyz\n\tposition(0, 0, 0)\nmissing.obj\n\tposition(0, 0, 0)\n", 2),
+    ]
+    for k, (text, code) in enumerate(cases):
+        (root / "res/scene/m.scene").write_text(text)
+        with pytest.raises(swr.SwrError) as e:
+            swr.load_scene(str(root / "res/scene/m.scene"), base)
+        assert e.value.code == code, (k, str(e.value))
+    # many blocks sharing few meshes load to the same arrays as the blocks one by one
+    text = "".join("q.obj\n\tposition(%d, 0, 0)\n\tscale(%d, 1, 1)\n" % (i, 1 + i % 3) for i in range(40))
+    (root / "res/scene/many.scene").write_text(text)
+    D = swr.load_scene(str(root / "res/scene/many.scene"), base)
+    assert D.num_triangles == 40 and D.num_objects == 40
+    assert np.allclose(D.vpos[3::3][:, 0], np.arange(1, 40) * 1.0)
+
+
 def test_stl_synthetic(tmp_path, monkeypatch):
     """Binary STL (the reference's STL assets are not shipped): y/z swap and the 60-degree
     normal grouping into vertices."""
