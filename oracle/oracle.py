@@ -26,6 +26,9 @@ def _lib():
         [ctypes.c_uint32] * 2 + [P, P, ctypes.c_int]
     lib.swo_adjoint_physical64.argtypes = [P, P] + [ctypes.c_uint32] * 4 + [ctypes.c_uint64, ctypes.c_uint32,
                                                                             ctypes.c_double, P, P, P, ctypes.c_int]
+    lib.swo_render_bdpt.argtypes = [P, P] + [ctypes.c_uint32] * 6 + [ctypes.c_uint64] + [ctypes.c_uint32] * 2 + \
+        [P, P, ctypes.c_int]
+    lib.swo_render_bdpt.restype = ctypes.c_int
     return lib
 
 
@@ -42,7 +45,7 @@ def lib():
 class _Scene(ctypes.Structure):
     _fields_ = [("ntri", ctypes.c_uint32), ("nobj", ctypes.c_uint32)] + \
         [(n, ctypes.c_void_p) for n in ["v0", "e0", "e1", "den", "tri_box", "obj_box", "tri_obj",
-                                        "obj_first", "visit", "nrm", "mats", "albedo", "emission"]]
+                                        "obj_first", "visit", "nrm", "mats", "albedo", "emission", "vtx"]]
 
 
 class _Camera(ctypes.Structure):
@@ -60,16 +63,18 @@ def _threads():
 class OracleScene:
     """Arrays: v0/e0/e1 [n,3], den [n,4], tri_box [n,6], obj_box [m,6], tri_obj [n],
     rank [n] (visit order position), nrm [n,9] corner normals, mats [m,9]
-    (color rgb, dT, rT, tT, eta, light, strength), optional albedo [n,3], emission [m,3]."""
+    (color rgb, dT, rT, tT, eta, light, strength), optional albedo [n,3], emission [m,3],
+    vtx [n,9] corner positions (needed by the bidirectional tracer's light sampling)."""
 
     def __init__(self, v0, e0, e1, den, tri_box, obj_box, tri_obj, rank, nrm, mats, albedo=None,
-                 emission=None):
+                 emission=None, vtx=None):
         f = lambda a, c: np.ascontiguousarray(a, dtype=np.float32).reshape(-1, c)
         self.v0, self.e0, self.e1 = f(v0, 3), f(e0, 3), f(e1, 3)
         self.den, self.tri_box, self.obj_box = f(den, 4), f(tri_box, 6), f(obj_box, 6)
         self.nrm, self.mats = f(nrm, 9), f(mats, 9)
         self.albedo = None if albedo is None else f(albedo, 3)
         self.emission = None if emission is None else f(emission, 3)
+        self.vtx = None if vtx is None else f(vtx, 9)
         self.tri_obj = np.ascontiguousarray(tri_obj, dtype=np.uint32).reshape(-1)
         rank = np.asarray(rank, dtype=np.int64).reshape(-1)
         self.visit = np.ascontiguousarray(np.argsort(rank, kind="stable"), dtype=np.uint32)
@@ -79,7 +84,7 @@ class OracleScene:
         self.obj_first[1:] = np.cumsum(counts)
         self._s = _Scene(self.v0.shape[0], nobj, *[_p(a) for a in (
             self.v0, self.e0, self.e1, self.den, self.tri_box, self.obj_box, self.tri_obj,
-            self.obj_first, self.visit, self.nrm, self.mats, self.albedo, self.emission)])
+            self.obj_first, self.visit, self.nrm, self.mats, self.albedo, self.emission, self.vtx)])
 
     @staticmethod
     def from_scene_data(sd, albedo=None, emission=None):
@@ -96,7 +101,8 @@ class OracleScene:
         rank = sd.tri_rank if sd.tri_rank is not None else np.arange(sd.num_triangles)
         return OracleScene(sd.vpos[tri[:, 0]], dv["e0"], dv["e1"], dv["den"], dv["tri_box"],
                            dv["obj_box"], sd.tri_obj, rank, nrm, mats,
-                           albedo=albedo if albedo is not None else sd.tri_albedo, emission=emission)
+                           albedo=albedo if albedo is not None else sd.tri_albedo, emission=emission,
+                           vtx=sd.vpos[tri].reshape(-1, 9))
 
     @staticmethod
     def from_dump(R):
@@ -114,7 +120,8 @@ class OracleScene:
         om = R["obj_mat"].reshape(-1, 8)  # color3 dT rT tT eta strength
         mats = np.concatenate([om[:, :7], R["obj_light"][:, None].astype(np.float32), om[:, 7:8]], axis=1)
         return OracleScene(R["tri_v0"], R["tri_e0"], R["tri_e1"], R["tri_den"], R["tri_box"],
-                           R["obj_box"], R["tri_obj"], rank, nrm, mats)
+                           R["obj_box"], R["tri_obj"], rank, nrm, mats,
+                           vtx=R["vpos"].reshape(-1, 3)[tri].reshape(-1, 9))
 
     def trace(self, ro, rd, threads=None):
         ro = np.ascontiguousarray(ro, dtype=np.float32).reshape(-1, 4)
@@ -143,6 +150,20 @@ def render_reference(sc, cam, W, H, spp, depth, seed, p0=0, p1=None, threads=Non
     pp = np.empty((n, 3), np.float32)
     lib().swo_render_reference(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, depth, seed, p0, p1,
                                _p(ps), _p(pp), threads or _threads())
+    return ps, pp
+
+
+def render_bdpt(sc, cam, W, H, spp, vision_jumps, light_jumps, max_depth, seed, p0=0, p1=None, threads=None):
+    """BidirectionalPathTracer: per-sample contributions [n, spp, 4] (before the 2 pi / spp scale)
+    and per-pixel radiance [n, 3]."""
+    p1 = W * H if p1 is None else p1
+    n = p1 - p0
+    ps = np.empty((n, spp, 4), np.float32)
+    pp = np.empty((n, 3), np.float32)
+    rc = lib().swo_render_bdpt(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, vision_jumps, light_jumps,
+                               max_depth, seed, p0, p1, _p(ps), _p(pp), threads or _threads())
+    if rc != 0:
+        raise ValueError("oracle BDPT: %s" % ("no light source" if rc == -2 else "bad arguments"))
     return ps, pp
 
 

@@ -11,6 +11,11 @@
 //   ref_harness render <basepath> <scene> <camera> <W> <H> <spp> <depth> <seed> <p0> <p1> <out>
 //       PathTracer radiance for pixels [p0, p1) (row-major index), per sample and per pixel,
 //       with the Philox shim cursor set to (seed, pixel, sample) before each sample.
+//   ref_harness render_bdpt <basepath> <scene> <camera> <W> <H> <spp> <vision> <light> <maxdepth>
+//                           <seed> <p0> <p1> <out>
+//       BidirectionalPathTracer::renderPixel with one ray per pixel per call, the Philox shim
+//       cursor set to (seed, pixel, sample) before each call: per-sample values (with the
+//       reference's 2 pi scale for one sample).
 //   ref_harness tree   <boxes> <out>
 //       the reference BVH::init tree over the given boxes (for builder equivalence tests).
 //
@@ -39,6 +44,7 @@
 #define private public
 #include "camera.h"
 #include "graphic/graphics_engine.h"
+#include "graphic/bidirectional_path_tracer.h"
 #include "graphic/graphics_object.h"
 #include "graphic/path_tracer.h"
 #include "graphic/scene.h"
@@ -381,6 +387,62 @@ int cmd_render(char** a) {
   return 0;
 }
 
+int cmd_render_bdpt(char** a) {
+  std::string basepath = a[0], scene = a[1], camera = a[2];
+  unsigned W = (unsigned)std::atoi(a[3]), H = (unsigned)std::atoi(a[4]);
+  unsigned spp = (unsigned)std::atoi(a[5]);
+  unsigned vj = (unsigned)std::atoi(a[6]), lj = (unsigned)std::atoi(a[7]), md = (unsigned)std::atoi(a[8]);
+  uint64_t seed = std::strtoull(a[9], nullptr, 10);
+  uint32_t p0 = (uint32_t)std::atoi(a[10]), p1 = (uint32_t)std::atoi(a[11]);
+  Loaded L = load(basepath, scene);
+  Camera cam;
+  InputParser cp(camera);
+  cp.parse();
+  cam.parseInput(cp.getInputEntry(0));
+  Matrix4f vi = cam.getViewMatrix().inverseMatrix();
+  Matrix4f pi = cam.getProjectionMatrix(float(W) / float(H)).inverseMatrix();
+  Vector3f origin = cutVector(vi * Vector4f({0.0f, 0.0f, 0.0f, 1.0f}));
+  const uint32_t np = p1 - p0;
+  std::vector<float> per_sample((size_t)np * spp * 4);
+  unsigned nthreads = std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<uint32_t> next(0);
+  auto work = [&]() {
+    BidirectionalPathTracer bd;
+    bd.visionJumpCount = vj;
+    bd.lightJumpCount = lj;
+    bd.maxDepth = md;
+    bd.raysPerPixel = 1;
+    Renderer::PixelRenderData prd;
+    prd.scene = &L.engine->scene;
+    prd.objects = &L.engine->objects;
+    prd.lightSources = &L.engine->lightSources;
+    prd.imageSize = Vector2u({W, H});
+    prd.origin = origin;
+    prd.viewInverse = vi;
+    prd.projInverse = pi;
+    for (;;) {
+      uint32_t k = next.fetch_add(1);
+      if (k >= np) break;
+      uint32_t p = p0 + k;
+      prd.pixel[0] = p % W;
+      prd.pixel[1] = p / W;
+      for (unsigned s = 0; s < spp; ++s) {
+        swr_shim_set_cursor(seed, p, s);
+        Vector3f v = bd.renderPixel(prd);
+        float* o = &per_sample[((size_t)k * spp + s) * 4];
+        for (int c = 0; c < 3; ++c) o[c] = v[c];
+        o[3] = 1.0f;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nthreads; ++t) th.emplace_back(work);
+  for (auto& t : th) t.join();
+  Writer w(a[12]);
+  w.f32("per_sample", per_sample);
+  return 0;
+}
+
 int cmd_tree(char** a) {
   std::vector<uint8_t> raw = read_file(a[0]);
   const size_t n = raw.size() / 24;
@@ -413,6 +475,7 @@ int main(int argc, char** argv) {
     if (cmd == "trace" && argc == 6) return cmd_trace(argv + 2);
     if (cmd == "render" && argc == 13) return cmd_render(argv + 2);
     if (cmd == "tree" && argc == 4) return cmd_tree(argv + 2);
+    if (cmd == "render_bdpt" && argc == 15) return cmd_render_bdpt(argv + 2);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "harness error: %s\n", e.what());
     return 1;

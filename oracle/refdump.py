@@ -62,6 +62,11 @@ def render(basepath, scene, camera, width, height, spp, depth, seed, p0, p1, out
     return read(out)
 
 
+def render_bdpt(basepath, scene, camera, width, height, spp, vision, light, max_depth, seed, p0, p1, out):
+    run("render_bdpt", basepath, scene, camera, width, height, spp, vision, light, max_depth, seed, p0, p1, out)
+    return read(out)
+
+
 def tree(boxes6, out):
     boxes6 = np.ascontiguousarray(boxes6, dtype=np.float32).reshape(-1, 6)
     bpath = out + ".boxes"

@@ -370,6 +370,201 @@ void swo_render_reference(const swo_scene* s, const swo_camera* cam, uint32_t W,
 }
 
 /* ---------------------------------------------------------------------------------------------
+ * bidirectional path tracer (bidirectional_path_tracer.cpp:20-168, scene.cpp:58-83) */
+
+/* Scene::isOccluded: a candidate hit (the closest-hit rules) no farther than the end point */
+static int occluded(const swo_scene* s, v3f a, v3f b) {
+  v3f d = sub(b, a);
+  float dist2 = dot(d, d), t, d2;
+  uint32_t tri;
+  d = normalize(d);
+  tri = closest(s, a, d, &t, &d2);
+  return tri != 0xFFFFFFFFu && d2 <= dist2;
+}
+
+typedef struct {
+  v3f pos, nrm, col;
+  int light_hit;
+} hitpoint_t;
+
+/* BidirectionalPathTracer::traceSinglePath for slots [start, end); returns the path depth */
+static uint32_t bdpt_trace(const swo_scene* s, hitpoint_t* path, v3f o, v3f d, uint32_t start, uint32_t end,
+                           int light_ray, uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t* draws) {
+  v3f c = mk(1.0f, 1.0f, 1.0f);
+  uint32_t depth = 0, i;
+  int backface = !light_ray;
+  for (i = start; i < end; ++i) {
+    float t, d2, u[4], r;
+    uint32_t tri = closest(s, o, d, &t, &d2), obj;
+    v3f p, n, nd, prev;
+    const float* m;
+    if (tri == 0xFFFFFFFFu) break;
+    p = add(o, scl(t, d));
+    n = shading_normal(s, tri, p);
+    if (backface && dot(n, d) > 0.0f) {
+      o = add(p, scl(0.01f, d));
+      continue;
+    }
+    backface = 0;
+    depth = i + 1;
+    swo_vertex_uniforms(seed, pixel, sample, (*draws)++, 0, u);
+    r = u[0];
+    obj = s->tri_obj[tri];
+    m = s->mats + 9 * (size_t)obj;
+    prev = d;
+    nd = d;
+    if (r <= m[3]) nd = hemisphere(n, u[1], u[2]);
+    else if (r <= m[4]) nd = reflect_f(d, n);
+    else if (r <= m[5]) nd = custom_refract_f(d, n, m[6]);
+    o = add(p, scl(0.01f, nd));
+    d = nd;
+    if (r <= m[3]) {
+      float cs = dot(n, light_ray ? prev : d);
+      c = mk(c.x * (m[0] * cs), c.y * (m[1] * cs), c.z * (m[2] * cs));
+    }
+    path[i].pos = p;
+    path[i].nrm = n;
+    path[i].col = c;
+    path[i].light_hit = 0;
+    if (m[7] != 0.0f && dot(n, prev) <= 0.0f) {
+      path[i].light_hit = 1;
+      break;
+    }
+  }
+  return depth;
+}
+
+/* one sample of BidirectionalPathTracer::renderPixel before the 2 pi / spp scale; returns 1 when
+ * the sample added anything (a light hit or a connection pass) */
+static v3f bdpt_sample(const swo_scene* s, v3f org, v3f dir, uint32_t vj, uint32_t lj, uint32_t md,
+                       const uint32_t* lights, uint32_t nlights, uint64_t seed, uint32_t pixel,
+                       uint32_t sample) {
+  hitpoint_t V[32], L[32];
+  uint32_t draws = 0, dv, dl, vi, li, light, ti, nt;
+  float u[4], sr1, r2, b0, b1, b2;
+  v3f color = mk(0.0f, 0.0f, 0.0f), lp, ln, ld;
+  const float *vt, *nn;
+  memset(V, 0, sizeof(V));  /* the reference's value-initialised hit points */
+  memset(L, 0, sizeof(L));
+  dv = bdpt_trace(s, V, org, dir, 0, vj, 0, seed, pixel, sample, &draws);
+  if (dv == 0) return color;
+  if (V[dv - 1].light_hit) return V[dv - 1].col;
+  /* getRandomLightSourcePoint (bidirectional_path_tracer.cpp:140-168) */
+  swo_vertex_uniforms(seed, pixel, sample, draws++, 0, u);
+  light = (uint32_t)(u[0] * (float)nlights);
+  if (light >= nlights) light = nlights - 1;
+  swo_vertex_uniforms(seed, pixel, sample, draws++, 0, u);
+  sr1 = sqrtf(u[0]);
+  swo_vertex_uniforms(seed, pixel, sample, draws++, 0, u);
+  r2 = u[0];
+  swo_vertex_uniforms(seed, pixel, sample, draws++, 0, u);
+  nt = s->obj_first[lights[light] + 1] - s->obj_first[lights[light]];
+  ti = (uint32_t)(u[0] * (float)nt);
+  if (ti >= nt) ti = nt - 1;
+  ti += s->obj_first[lights[light]];
+  b0 = 1.0f - sr1;
+  b1 = sr1 * (1.0f - r2);
+  b2 = sr1 * r2;
+  vt = s->vtx + 9 * (size_t)ti;
+  nn = s->nrm + 9 * (size_t)ti;
+  lp = add(add(scl(b0, ld3(vt)), scl(b1, ld3(vt + 3))), scl(b2, ld3(vt + 6)));
+  ln = mk(0.0f, 0.0f, 0.0f);
+  ln = add(ln, scl(b0, ld3(nn)));
+  ln = add(ln, scl(b1, ld3(nn + 3)));
+  ln = add(ln, scl(b2, ld3(nn + 6)));
+  ln = normalize(ln);
+  ld = hemisphere(ln, u[1], u[2]);
+  L[0].pos = lp;
+  L[0].nrm = ln;
+  L[0].col = ld3(s->mats + 9 * (size_t)lights[light]);
+  dl = bdpt_trace(s, L, lp, ld, 1, lj, 1, seed, pixel, sample, &draws);
+  for (vi = 0; vi < dv; ++vi)
+    for (li = 0; li < dl; ++li) {
+      v3f a, b, d;
+      float cs;
+      if (vi + li > md) continue;
+      a = add(V[vi].pos, scl(0.01f, V[vi].nrm));
+      b = add(L[li].pos, scl(0.01f, L[li].nrm));
+      if (occluded(s, a, b)) continue;
+      d = normalize(sub(b, a));
+      cs = dot(d, V[vi].nrm);
+      color = add(color, mk(V[vi].col.x * L[li].col.x * cs, V[vi].col.y * L[li].col.y * cs,
+                            V[vi].col.z * L[li].col.z * cs));
+    }
+  return scl(1.0f / (float)md, color);
+}
+
+typedef struct {
+  const swo_scene* s;
+  const swo_camera* cam;
+  uint32_t W, H, spp, vj, lj, md, p0;
+  uint64_t seed;
+  const uint32_t* lights;
+  uint32_t nlights;
+  float *per_sample, *per_pixel;
+} bdpt_ctx;
+
+static void bdpt_range(void* c_, uint64_t b, uint64_t e) {
+  bdpt_ctx* c = (bdpt_ctx*)c_;
+  uint64_t k;
+  for (k = b; k < e; ++k) {
+    uint32_t pix = c->p0 + (uint32_t)k, smp;
+    v3f d = primary_dir(c->cam, pix % c->W, pix / c->W, c->W, c->H);
+    v3f o = ld3(c->cam->org);
+    v3f f = mk(0.0f, 0.0f, 0.0f);
+    double sc;
+    for (smp = 0; smp < c->spp; ++smp) {
+      v3f col = bdpt_sample(c->s, o, d, c->vj, c->lj, c->md, c->lights, c->nlights, c->seed, pix, smp);
+      float* ps = c->per_sample ? c->per_sample + (k * c->spp + smp) * 4 : NULL;
+      f = add(f, col);
+      if (ps) {
+        ps[0] = col.x;
+        ps[1] = col.y;
+        ps[2] = col.z;
+        ps[3] = 1.0f;
+      }
+    }
+    sc = 2.0 * M_PI * (double)(1.0f / (float)c->spp);
+    c->per_pixel[3 * k + 0] = (float)((double)f.x * sc);
+    c->per_pixel[3 * k + 1] = (float)((double)f.y * sc);
+    c->per_pixel[3 * k + 2] = (float)((double)f.z * sc);
+  }
+}
+
+int swo_render_bdpt(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H, uint32_t spp,
+                    uint32_t vision_jumps, uint32_t light_jumps, uint32_t max_depth, uint64_t seed,
+                    uint32_t p0, uint32_t p1, float* per_sample, float* per_pixel, int threads) {
+  bdpt_ctx c;
+  uint32_t* lights;
+  uint32_t o, n = 0;
+  if (!s->vtx || vision_jumps > 32 || light_jumps > 32 || max_depth == 0) return -1;
+  lights = (uint32_t*)malloc(sizeof(uint32_t) * (s->nobj ? s->nobj : 1));
+  for (o = 0; o < s->nobj; ++o)
+    if (s->mats[9 * (size_t)o + 7] != 0.0f) lights[n++] = o;
+  if (n == 0) {
+    free(lights);
+    return -2;
+  }
+  c.s = s;
+  c.cam = cam;
+  c.W = W;
+  c.H = H;
+  c.spp = spp;
+  c.vj = vision_jumps;
+  c.lj = light_jumps;
+  c.md = max_depth;
+  c.p0 = p0;
+  c.seed = seed;
+  c.lights = lights;
+  c.nlights = n;
+  c.per_sample = per_sample;
+  c.per_pixel = per_pixel;
+  parallel_for(p1 - p0, 4, threads, bdpt_range, &c);
+  free(lights);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------------------------
  * physical mode in double. Hits are chosen with the reference's float rules (the same triangle
  * the renderer finds); positions, normals, directions, throughput and sums are carried in double. */
 typedef struct {

@@ -24,6 +24,7 @@ typedef struct swo_scene {
   const float* mats;      /* [nobj*9] color.rgb dT rT tT eta light strength */
   const float* albedo;    /* [ntri*3] physical-mode albedo (NULL: object color) */
   const float* emission;  /* [nobj*3] physical-mode emission (NULL: color * strength) */
+  const float* vtx;       /* [ntri*9] corner positions v0 v1 v2 (light-point sampling) */
 } swo_scene;
 
 typedef struct swo_camera {
@@ -53,6 +54,12 @@ void swo_adjoint_physical64(const swo_scene* s, const swo_camera* cam, uint32_t 
                             uint32_t spp, uint32_t depth, uint64_t seed, uint32_t rr_depth,
                             double rr_q, const float* dl_dimg, double* g_albedo, double* g_emission,
                             int threads);
+
+/* BidirectionalPathTracer radiance for pixels [p0, p1): per sample (the contribution before the
+ * 2 pi / spp scale; r g b 1) and per pixel. Returns -2 for a scene without light sources. */
+int swo_render_bdpt(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H, uint32_t spp,
+                    uint32_t vision_jumps, uint32_t light_jumps, uint32_t max_depth, uint64_t seed,
+                    uint32_t p0, uint32_t p1, float* per_sample, float* per_pixel, int threads);
 
 #ifdef __cplusplus
 }

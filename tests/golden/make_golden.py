@@ -4,8 +4,8 @@ harness in oracle/_ref/, built from the reference sources by oracle/Makefile).
 For each case it stores, from the reference: the world-space scene exactly as its
 GraphicsObject::init produced it (vertices, normals, triangles, materials, the tie-break visit
 ranks from its BVHs), the camera matrices of GraphicsEngine::render, the closest hits of
-Scene::traceRay for a seeded ray set, and PathTracer radiance per sample (Philox shim) for a
-small image. Run from the repository root:  python tests/golden/make_golden.py
+Scene::traceRay for a seeded ray set, and PathTracer and BidirectionalPathTracer radiance per
+sample (Philox shim) for a small image. Run from the repository root:  python tests/golden/make_golden.py
 """
 import os
 import sys
@@ -24,6 +24,7 @@ from helpers import rays_uniform  # noqa: E402
 REF = "/root/reference"
 OUT = os.path.dirname(os.path.abspath(__file__))
 W, H, SPP, DEPTH, SEED = 32, 24, 4, 5, 20240601
+BD_VISION, BD_LIGHT, BD_MAX = 5, 5, 5  # res/renderer/SoftwareRendererBidirectionalPathTracer.renderer
 NRAYS = 4096
 
 
@@ -46,6 +47,8 @@ def make(name, scene, camera, basepath, tmp):
     ro, rd = rays_uniform(NRAYS, lo, hi, seed=17)
     hits = refdump.trace(basepath, scene, np.concatenate([ro[:, :3], rd[:, :3]], 1), os.path.join(tmp, name + ".hits"))
     rend = refdump.render(basepath, scene, camera, W, H, SPP, DEPTH, SEED, 0, W * H, os.path.join(tmp, name + ".rend"))
+    bd = refdump.render_bdpt(basepath, scene, camera, W, H, SPP, BD_VISION, BD_LIGHT, BD_MAX, SEED, 0, W * H,
+                             os.path.join(tmp, name + ".bdpt"))
     om = R["obj_mat"].reshape(-1, 8)
     np.savez_compressed(
         os.path.join(OUT, name + ".npz"),
@@ -59,7 +62,9 @@ def make(name, scene, camera, basepath, tmp):
         cam_origin=R["camera"][32:35], ray_o=ro, ray_d=rd, hit_id=hits["hit_id"], hit_obj=hits["hit_obj"],
         hit_d2=hits["hit_d2"], hit_pos=hits["hit_pos"].reshape(-1, 3), hit_nrm=hits["hit_nrm"].reshape(-1, 3),
         per_sample=rend["per_sample"].reshape(W * H, SPP, 4), per_pixel=rend["per_pixel"].reshape(W * H, 3),
-        params=np.array([W, H, SPP, DEPTH, SEED], np.uint64))
+        params=np.array([W, H, SPP, DEPTH, SEED], np.uint64),
+        bdpt_per_sample=bd["per_sample"].reshape(W * H, SPP, 4),
+        bdpt_params=np.array([W, H, SPP, BD_VISION, BD_LIGHT, BD_MAX, SEED], np.uint64))
     print(name, R["tri_obj"].shape[0], "triangles")
 
 

@@ -51,7 +51,8 @@ def _oracle_scene(name):
     mats = np.concatenate([g["mat_color"], g["mat_thresholds"], g["mat_eta"][:, None],
                            g["mat_light"][:, None].astype(np.float32), g["mat_strength"][:, None]], 1)
     sc = O.OracleScene(R["tri_v0"], R["tri_e0"], R["tri_e1"], R["tri_den"], R["tri_box"], R["obj_box"],
-                       R["tri_obj"], g["tri_rank"], nrm, mats)
+                       R["tri_obj"], g["tri_rank"], nrm, mats,
+                       vtx=g["vpos"][g["tri"].astype(np.int64)].reshape(-1, 9))
     return g, sc
 
 
@@ -73,6 +74,23 @@ def test_oracle_radiance_matches_reference(name):
     assert np.array_equal(ps.view(np.uint32), g["per_sample"].view(np.uint32))
     assert np.array_equal(pp.view(np.uint32), g["per_pixel"].view(np.uint32))
     assert np.array_equal(ref_pixel_from_samples(ps, spp).view(np.uint32), g["per_pixel"].view(np.uint32))
+
+
+def bdpt_reference_values(per_sample):
+    """What the reference's BidirectionalPathTracer::renderPixel returns for one sample: the
+    contribution scaled by 2 pi (in double, stored to float)."""
+    return (per_sample[..., :3].astype(np.float64) * (2.0 * np.pi)).astype(np.float32)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_bdpt_matches_reference(name):
+    g, sc = _oracle_scene(name)
+    W, H, spp, vj, lj, md, seed = [int(x) for x in g["bdpt_params"]]
+    cam = O.camera(g["cam_view_inv"], g["cam_proj_inv"], g["cam_origin"])
+    ps, pp = O.render_bdpt(sc, cam, W, H, spp, vj, lj, md, seed)
+    ref = g["bdpt_per_sample"][..., :3]
+    assert np.array_equal(bdpt_reference_values(ps).view(np.uint32), ref.view(np.uint32))
+    assert (np.abs(ref).sum(-1) > 0).mean() > 0.05
 
 
 @pytest.mark.reference
