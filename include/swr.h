@@ -159,6 +159,18 @@ int swr_camera_make(const float position[3], float angle_theta, float angle_phi,
 /* Renderer file (main.cpp:62-66, path_tracer.cpp:13-16): accepts PathTracer; returns its
  * visionJumpCount and raysPerPixel. */
 int swr_renderer_load(const char* renderer_path, uint32_t* max_depth, uint32_t* spp);
+/* Renderer file with either renderer of the reference (main.cpp:22-26): PathTracer
+ * (path_tracer.cpp:13-16) or BidirectionalPathTracer (bidirectional_path_tracer.cpp:13-18). */
+enum { SWR_RENDERER_PATH_TRACER = 0, SWR_RENDERER_BIDIRECTIONAL = 1 };
+typedef struct swr_renderer_params {
+  uint32_t kind;          /* SWR_RENDERER_* */
+  uint32_t vision_jumps;  /* visionJumpCount */
+  uint32_t light_jumps;   /* lightJumpCount (bidirectional) */
+  uint32_t max_depth;     /* maxDepth (bidirectional) */
+  uint32_t spp;           /* raysPerPixel */
+  uint32_t reserved[3];
+} swr_renderer_params;
+int swr_renderer_load_params(const char* renderer_path, swr_renderer_params* out);
 
 /* Derived per-triangle data exactly as the reference's Triangle / GraphicsObject compute them
  * (triangle.cpp:4-17, graphics_object.cpp:25): edges e0 = v1-v0, e1 = v2-v0 [3*ntri each],
@@ -220,6 +232,21 @@ typedef struct swr_render_profile {
 /* As swr_render, filling *prof (which may be NULL). */
 int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                         float* rgb_out, float* samples_out, void* stream, swr_render_profile* prof);
+
+/* Bidirectional path tracer (replaces BidirectionalPathTracer, bidirectional_path_tracer.cpp:20-168,
+ * with Scene::isOccluded, scene.cpp:58-83, as its occlusion query). opts->max_depth is
+ * visionJumpCount (1..16), opts->mode must be SWR_MODE_REFERENCE; bdpt->light_jumps is
+ * lightJumpCount (0..16) and bdpt->max_depth the reference's maxDepth (connections with
+ * vision index + light index <= maxDepth; the sum is divided by it). The light sources are the
+ * scene's light_source objects in object order; the scene needs at least one. samples_out (with
+ * SWR_RENDER_SAMPLES_OUT) receives per sample the contribution before the 2*pi/spp scale. */
+typedef struct swr_bdpt_opts {
+  uint32_t light_jumps;
+  uint32_t max_depth;
+  uint32_t reserved[2];
+} swr_bdpt_opts;
+int swr_render_bdpt(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
+                    const swr_bdpt_opts* bdpt, float* rgb_out, float* samples_out, void* stream);
 
 /* Batched rendering: many independent jobs (scene, camera, options, output) in one shared
  * wavefront, so that small images do not leave the GPU idle (no counterpart in the reference,

@@ -95,6 +95,19 @@ class BatchOpts(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class BdptOpts(ctypes.Structure):
+    _fields_ = [("light_jumps", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2)]
+
+
+class RendererParams(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("vision_jumps", ctypes.c_uint32), ("light_jumps", ctypes.c_uint32),
+                ("max_depth", ctypes.c_uint32), ("spp", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
+
+
+RENDERER_PATH_TRACER = 0
+RENDERER_BIDIRECTIONAL = 1
+
+
 class AdjointJob(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_void_p), ("cam", Camera), ("opts", RenderOpts), ("dl_dimage", ctypes.c_void_p),
                 ("dl_dalbedo", ctypes.c_void_p), ("dl_demission", ctypes.c_void_p)]
@@ -139,6 +152,8 @@ SIGNATURES = {
     "swr_render_adjoint": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P, P]),
     "swr_render_adjoint_timed": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), P, P, P, P,
                                      ctypes.POINTER(ctypes.c_double)]),
+    "swr_render_bdpt": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), ctypes.POINTER(BdptOpts), P, P, P]),
+    "swr_renderer_load_params": (I, [ctypes.c_char_p, ctypes.POINTER(RendererParams)]),
     "swr_quantize_rgb8": (I, [P, U32, U32, P]),
     "swr_write_ppm": (I, [ctypes.c_char_p, P, U32, U32]),
 }

@@ -118,6 +118,15 @@ def load_renderer(renderer_path):
     return depth.value, spp.value
 
 
+def load_renderer_params(renderer_path):
+    """Renderer file of either reference renderer: dict(kind "PathTracer" or
+    "BidirectionalPathTracer", vision_jumps, light_jumps, max_depth, spp)."""
+    r = N.RendererParams()
+    check(N.lib.swr_renderer_load_params(os.fsencode(renderer_path), ctypes.byref(r)))
+    return dict(kind="PathTracer" if r.kind == N.RENDERER_PATH_TRACER else "BidirectionalPathTracer",
+                vision_jumps=r.vision_jumps, light_jumps=r.light_jumps, max_depth=r.max_depth, spp=r.spp)
+
+
 def _stream_handle(stream):
     if stream is None:
         try:
@@ -225,6 +234,22 @@ def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=
     return (ga, ge, ms.value) if return_ms else (ga, ge)
 
 
+def _scene_render_bdpt(self, cam, width, height, spp, vision_jumps, light_jumps, max_depth, seed=0, out=None,
+                       samples=None, refill=0, stream=None):
+    """BidirectionalPathTracer image (height, width, 3) into `out` (torch cuda tensor or numpy
+    array); `samples` (optional, (height*width, spp, 4)) receives the per-sample contributions."""
+    flags = N.RENDER_SAMPLES_OUT if samples is not None else 0
+    o = N.RenderOpts(width, height, spp, vision_jumps, seed, N.MODE_REFERENCE, 0, 1.0, 0, 0, flags, refill, 0, 0)
+    b = N.BdptOpts(light_jumps, max_depth)
+    if out is None:
+        import torch
+        out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+    check(N.lib.swr_render_bdpt(self._h, ctypes.byref(cam), ctypes.byref(o), ctypes.byref(b), ptr(out), ptr(samples),
+                                _stream_handle(stream)))
+    return out
+
+
+Scene.render_bdpt = _scene_render_bdpt
 Scene.set_albedo = _scene_set_albedo
 Scene.set_emission = _scene_set_emission
 Scene.render_adjoint = _scene_render_adjoint

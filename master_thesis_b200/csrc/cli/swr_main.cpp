@@ -1,6 +1,7 @@
 // SoftwareRenderer command-line drop-in (software_renderer/main.cpp:28-87): the same positional
-// arguments, the same base-path rule for mesh files and the same P6 output, with the image
-// rendered on the GPU through the C ABI instead of by host threads.
+// arguments, the same renderer files (PathTracer and BidirectionalPathTracer), the same base-path
+// rule for mesh files and the same P6 output, with the image rendered on the GPU through the C
+// ABI instead of by host threads.
 //
 //   SoftwareRenderer renderer scene image_width image_height thread_count camera resultimage
 //
@@ -59,8 +60,8 @@ int main(int argc, char* argv[]) {
   const uint64_t seed = seed_env ? std::strtoull(seed_env, nullptr, 10) : 0;
 
   auto t0 = std::chrono::steady_clock::now();
-  uint32_t depth = 0, spp = 0;
-  if (swr_renderer_load(renderer_path, &depth, &spp)) return fail("renderer");
+  swr_renderer_params rp;
+  if (swr_renderer_load_params(renderer_path, &rp)) return fail("renderer");
   swr_host_scene* hs = nullptr;
   if (swr_host_scene_load(scene_path, basepath.c_str(), &hs)) return fail("scene");
   swr_camera cam;
@@ -83,12 +84,19 @@ int main(int argc, char* argv[]) {
   swr_render_opts ro = {};
   ro.width = width;
   ro.height = height;
-  ro.spp = spp;
-  ro.max_depth = depth;
+  ro.spp = rp.spp;
+  ro.max_depth = rp.vision_jumps;
   ro.seed = seed;
   ro.mode = SWR_MODE_REFERENCE;
   std::vector<float> rgb((size_t)width * height * 3);
-  if (swr_render(scene, &cam, &ro, rgb.data(), nullptr, nullptr)) return fail("render");
+  if (rp.kind == SWR_RENDERER_BIDIRECTIONAL) {
+    swr_bdpt_opts bd = {};
+    bd.light_jumps = rp.light_jumps;
+    bd.max_depth = rp.max_depth;
+    if (swr_render_bdpt(scene, &cam, &ro, &bd, rgb.data(), nullptr, nullptr)) return fail("render");
+  } else {
+    if (swr_render(scene, &cam, &ro, rgb.data(), nullptr, nullptr)) return fail("render");
+  }
   if (swr_sync(nullptr)) return fail("render");
   const double t_render = seconds_since(t0);
   std::cout << "100% done" << std::endl;

@@ -419,6 +419,228 @@ __global__ void __launch_bounds__(kTraceBlock)
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Bidirectional path tracer (BidirectionalPathTracer, bidirectional_path_tracer.cpp:20-168).
+//
+// Each lane carries one camera sample through the reference's three stages: the vision path
+// (starting from the per-pixel camera record, which already holds the back-face-skipping prefix
+// and the first front hit), a light subpath from a sampled point on a light source, and the
+// connections of every vision vertex with every light vertex (vi + li <= maxDepth) through
+// occlusion queries (Scene::isOccluded, scene.cpp:58-83). Every trace, closest hit or occlusion,
+// is the resumable Traversal, so lanes in different stages share the traversal loop; a lane that
+// finishes a sample takes a new one. Random numbers: the sample's k-th draw of the reference
+// (one per scattering vertex, four for the light point) is Philox vertex k of the sample.
+// The vision slots of the skipped prefix hold the reference's zero-initialised hit points: their
+// connections add exactly zero, so their occlusion queries are not run.
+constexpr int kBdptMax = 16;
+
+struct BdptArgs {
+  uint32_t vj, lj, md, pad;
+};
+
+enum BdptPhase : uint32_t { kVision = 0, kVisionDone = 1, kLight = 2, kConnectNext = 3, kConnectResult = 4 };
+
+__global__ void __launch_bounds__(kTraceBlock)
+    k_bdpt(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, BdptArgs B) {
+  __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned long long total = ctrl->total;
+  swrx::Traversal tr;
+  f3 vpos[kBdptMax], vnrm[kBdptMax], vcol[kBdptMax];
+  f3 lpos[kBdptMax], lnrm[kBdptMax], lcol[kBdptMax];
+  uint32_t pixel = 0, sample = 0, phase = kVision, i = 0, draws = 0, vfirst = 0, dv = 0, dl = 0, vi = 0, li = 0;
+  bool active = false, tracing = false, exhausted = false, vlight = false;
+  f3 o = mk(0, 0, 0), d = mk(0, 0, 0), c = mk(1, 1, 1), acc = mk(0, 0, 0), dn = mk(0, 0, 0);
+  uint32_t hslot = 0;
+  float ht = 0.0f;
+  const float inv_md = 1.0f / (float)B.md;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
+      unsigned long long base = 0;
+      // inj_base[0] serves as the sample cursor of this launch
+      if (lane == 0) base = atomicAdd(&ctrl->inj_base[0], (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) exhausted = true;
+      if (!active) {
+        const unsigned long long g = base + __popc(idle & lt);
+        if (g < total) {
+          pixel = (uint32_t)(g / F.spp);
+          sample = (uint32_t)(g % F.spp);
+          const float4 r0 = F.cam[2 * (size_t)pixel], r1 = F.cam[2 * (size_t)pixel + 1];
+          const uint32_t bits = __float_as_uint(r1.w);
+          if (bits == kDeadSlot) {  // no front hit within visionJumpCount: the sample adds nothing
+            F.contrib[(size_t)pixel * F.spp + sample] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          } else {
+            o = mk(r0.x, r0.y, r0.z);
+            d = mk(r1.x, r1.y, r1.z);
+            i = bits >> 27;
+            vfirst = i;
+            hslot = bits & 0x07FFFFFFu;
+            ht = r0.w;
+            draws = 0;
+            dv = dl = 0;
+            vlight = false;
+            c = mk(1.0f, 1.0f, 1.0f);
+            phase = kVision;
+            tracing = false;
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+    if (tracing) {
+      if (!tr.step<false, false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, nullptr)) continue;
+      tracing = false;
+      hslot = tr.hit.slot;
+      ht = tr.hit.t;
+    }
+    const uint32_t gpix = F.pixel0 + pixel;
+    // advance the sample until it needs a trace or is finished
+    while (active && !tracing) {
+      if (phase == kVision || phase == kLight) {
+        const bool vision = phase == kVision;
+        if (hslot == 0xFFFFFFFFu) {
+          phase = vision ? (uint32_t)kVisionDone : (uint32_t)kConnectNext;
+          vi = vfirst;
+          li = 0;
+          acc = mk(0.0f, 0.0f, 0.0f);
+          continue;
+        }
+        const f3 p = swrx::hit_point(o, d, ht);
+        const f3 n = swrx::shading_normal(sc.tris, sc.shade, hslot, p);
+        const uint32_t obj = __float_as_uint(__ldg(sc.tris + 3 * (size_t)hslot + 2).w);
+        const swrx::Material m = swrx::load_material(sc.mats, obj);
+        if (vision) dv = i + 1;
+        else dl = i + 1;
+        const swrx::Uniforms U = swrx::vertex_uniforms(F.seed, gpix, sample, draws++, 0);
+        const float r = U.u[0];
+        const f3 prev = d;
+        f3 nd = d;
+        if (r <= m.m0.w) nd = swrx::hemisphere_dir(n, U.u[1], U.u[2]);
+        else if (r <= m.m1.x) nd = swrx::reflect_ref(d, n);
+        else if (r <= m.m1.y) nd = swrx::custom_refract_ref(d, n, m.m1.z);
+        o = swrx::vadd(p, swrx::vscale(0.01f, nd));
+        d = nd;
+        if (r <= m.m0.w) {
+          const float cs = swrx::vdot(n, vision ? nd : prev);
+          c = swrx::vmul(c, mk(__fmul_rn(m.m0.x, cs), __fmul_rn(m.m0.y, cs), __fmul_rn(m.m0.z, cs)));
+        }
+        if (vision) {
+          vpos[i] = p;
+          vnrm[i] = n;
+          vcol[i] = c;
+        } else {
+          lpos[i] = p;
+          lnrm[i] = n;
+          lcol[i] = c;
+        }
+        const bool light_hit = __float_as_uint(m.m1.w) != 0u && swrx::vdot(n, prev) <= 0.0f;
+        ++i;
+        if (light_hit || i >= (vision ? B.vj : B.lj)) {
+          if (vision) {
+            vlight = light_hit;
+            phase = kVisionDone;
+          } else {
+            phase = kConnectNext;
+            vi = vfirst;
+            li = 0;
+            acc = mk(0.0f, 0.0f, 0.0f);
+          }
+          continue;
+        }
+        tr.init(o, d, stack + threadIdx.x, kTraceBlock);
+        tracing = true;
+      } else if (phase == kVisionDone) {
+        if (vlight) {
+          F.contrib[(size_t)pixel * F.spp + sample] = make_float4(vcol[dv - 1].x, vcol[dv - 1].y, vcol[dv - 1].z, 1.0f);
+          active = false;
+          continue;
+        }
+        // getRandomLightSourcePoint (bidirectional_path_tracer.cpp:140-168)
+        swrx::Uniforms U = swrx::vertex_uniforms(F.seed, gpix, sample, draws++, 0);
+        uint32_t light = __float2uint_rz(__fmul_rn(U.u[0], (float)sc.num_lights));
+        light = min(light, sc.num_lights - 1u);
+        U = swrx::vertex_uniforms(F.seed, gpix, sample, draws++, 0);
+        const float sr1 = __fsqrt_rn(U.u[0]);
+        U = swrx::vertex_uniforms(F.seed, gpix, sample, draws++, 0);
+        const float r2 = U.u[0];
+        U = swrx::vertex_uniforms(F.seed, gpix, sample, draws++, 0);
+        const uint4 L = sc.lights[light];
+        uint32_t ti = __float2uint_rz(__fmul_rn(U.u[0], (float)L.y));
+        ti = min(ti, L.y - 1u);
+        const float b0 = __fsub_rn(1.0f, sr1), b1 = __fmul_rn(sr1, __fsub_rn(1.0f, r2)), b2 = __fmul_rn(sr1, r2);
+        const float4* q = sc.light_tris + 5 * (size_t)(L.x + ti);
+        const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        const f3 v0 = mk(q0.x, q0.y, q0.z), v1 = mk(q0.w, q1.x, q1.y), v2 = mk(q1.z, q1.w, q2.x);
+        const f3 n0 = mk(q2.y, q2.z, q2.w), n1 = mk(q3.x, q3.y, q3.z), n2 = mk(q3.w, q4.x, q4.y);
+        const f3 lp = swrx::vadd(swrx::vadd(swrx::vscale(b0, v0), swrx::vscale(b1, v1)), swrx::vscale(b2, v2));
+        f3 ln = swrx::vadd(mk(0.0f, 0.0f, 0.0f), swrx::vscale(b0, n0));
+        ln = swrx::vadd(ln, swrx::vscale(b1, n1));
+        ln = swrx::vadd(ln, swrx::vscale(b2, n2));
+        ln = swrx::vnormalize(ln);
+        const float4 lc = __ldg(sc.mats + 3 * (size_t)L.z);
+        lpos[0] = lp;
+        lnrm[0] = ln;
+        lcol[0] = mk(lc.x, lc.y, lc.z);
+        o = lp;
+        d = swrx::hemisphere_dir(ln, U.u[1], U.u[2]);
+        c = mk(1.0f, 1.0f, 1.0f);
+        i = 1;
+        if (B.lj > 1) {
+          phase = kLight;
+          tr.init(o, d, stack + threadIdx.x, kTraceBlock);
+          tracing = true;
+        } else {
+          phase = kConnectNext;
+          vi = vfirst;
+          li = 0;
+          acc = mk(0.0f, 0.0f, 0.0f);
+        }
+      } else if (phase == kConnectNext) {
+        if (vi >= dv) {
+          const f3 r = swrx::vscale(inv_md, acc);
+          F.contrib[(size_t)pixel * F.spp + sample] = make_float4(r.x, r.y, r.z, 1.0f);
+          active = false;
+          continue;
+        }
+        if (li >= dl) {
+          ++vi;
+          li = 0;
+          continue;
+        }
+        if (vi + li > B.md) {
+          ++li;
+          continue;
+        }
+        const f3 a = swrx::vadd(vpos[vi], swrx::vscale(0.01f, vnrm[vi]));
+        const f3 b = swrx::vadd(lpos[li], swrx::vscale(0.01f, lnrm[li]));
+        const f3 dd = swrx::vsub(b, a);
+        const float dist2 = swrx::vdot(dd, dd);
+        dn = swrx::vnormalize(dd);
+        tr.init_occlusion(a, dn, dist2, stack + threadIdx.x, kTraceBlock);
+        tracing = true;
+        phase = kConnectResult;
+      } else {  // kConnectResult
+        if (hslot == 0xFFFFFFFFu) {  // not occluded
+          const float cs = swrx::vdot(dn, vnrm[vi]);
+          const f3 vc = vcol[vi], lc = lcol[li];
+          acc = swrx::vadd(acc, mk(__fmul_rn(__fmul_rn(vc.x, lc.x), cs), __fmul_rn(__fmul_rn(vc.y, lc.y), cs),
+                                   __fmul_rn(__fmul_rn(vc.z, lc.z), cs)));
+        }
+        ++li;
+        phase = kConnectNext;
+      }
+    }
+  }
+}
+
 __global__ void k_resolve(Frame F, float* __restrict__ img) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= F.npix) return;
@@ -812,6 +1034,90 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   return SWR_OK;
 }
 
+int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, const swr_bdpt_opts* b,
+                     float* rgb_out, float* samples_out, void* stream_) {
+  if (!s || !cam || !o || !b || !rgb_out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (o->mode != SWR_MODE_REFERENCE)
+    return set_error(SWR_ERR_INVALID, "swr: the bidirectional tracer renders SWR_MODE_REFERENCE");
+  if (o->width == 0 || o->height == 0 || o->spp == 0)
+    return set_error(SWR_ERR_INVALID, "swr: zero image size or samples");
+  if (o->max_depth == 0 || o->max_depth > (uint32_t)kBdptMax || b->light_jumps > (uint32_t)kBdptMax)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: the bidirectional tracer supports 1..16 vision and 0..16 light jumps");
+  if (b->max_depth == 0) return set_error(SWR_ERR_INVALID, "swr: bidirectional maxDepth must be positive");
+  if ((uint64_t)o->width * o->height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
+  if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  if (s->dev.num_lights == 0)
+    return set_error(SWR_ERR_INVALID, "swr: the bidirectional tracer needs a light source in the scene");
+  const bool want_samples = (o->flags & SWR_RENDER_SAMPLES_OUT) != 0;
+  if (want_samples && !samples_out)
+    return set_error(SWR_ERR_INVALID, "swr: SWR_RENDER_SAMPLES_OUT without a samples buffer");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  RenderWorkspace* ws = workspace_of(s);
+  if (!ws) return set_error(SWR_ERR_ALLOC, "swr: workspace");
+  const uint64_t npix_total = (uint64_t)o->width * o->height;
+  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
+  int rc;
+  if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
+  if ((rc = ensure(&ws->contrib, ws->contrib_n, px_per_chunk * o->spp, sizeof(float4)))) return rc;
+  if (!ws->ctrl) {
+    SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
+  }
+  float* img = rgb_out;
+  const bool host_img = is_host_pointer(rgb_out);
+  if (host_img) {
+    if ((rc = ensure(&ws->stage, ws->stage_n, npix_total * 3, sizeof(float)))) return rc;
+    img = (float*)ws->stage;
+  }
+  const bool host_samples = want_samples && is_host_pointer(samples_out);
+  Frame F;
+  std::memset(&F, 0, sizeof(F));
+  std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
+  std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
+  std::memcpy(F.org, cam->origin, sizeof(F.org));
+  F.W = o->width;
+  F.H = o->height;
+  F.spp = o->spp;
+  F.depth = o->max_depth;
+  F.mode = 0;
+  F.rr_q = 1.0f;
+  F.seed = o->seed;
+  F.refill = o->refill ? o->refill : 8;
+  F.cam = (float4*)ws->cam;
+  F.contrib = (float4*)ws->contrib;
+  BdptArgs B;
+  B.vj = o->max_depth;
+  B.lj = b->light_jumps;
+  B.md = b->max_depth;
+  B.pad = 0;
+  int per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bdpt, kTraceBlock, 0));
+  const unsigned grid = (unsigned)(s->num_sms * std::max(per_sm, 1));
+  for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
+    const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
+    F.pixel0 = (uint32_t)p0;
+    F.npix = np;
+    Ctrl init;
+    std::memset(&init, 0, sizeof(init));
+    init.total = (uint64_t)np * o->spp;
+    SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
+    *ws->host_ctrl = init;
+    SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    k_bdpt<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
+    k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
+    SWR_CUDA(cudaGetLastError());
+    if (want_samples)
+      SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)p0 * o->spp * 4, F.contrib, (size_t)np * o->spp * sizeof(float4),
+                               host_samples ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream));
+  }
+  if (host_img)
+    SWR_CUDA(cudaMemcpyAsync(rgb_out, img, npix_total * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+  if (host_img || host_samples) SWR_CUDA(cudaStreamSynchronize(stream));
+  return SWR_OK;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Allocation-free render (swr_render_noalloc).
 //
@@ -987,6 +1293,11 @@ int swr_render_profiled(swr_scene* s, const swr_camera* cam, const swr_render_op
 int swr_render_adjoint(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, const float* dl_dimage,
                        float* dl_dalbedo, float* dl_demission, void* stream) {
   return swr::render_adjoint_impl(s, cam, o, dl_dimage, dl_dalbedo, dl_demission, stream, nullptr);
+}
+
+int swr_render_bdpt(swr_scene* s, const swr_camera* cam, const swr_render_opts* opts, const swr_bdpt_opts* bdpt,
+                    float* rgb_out, float* samples_out, void* stream) {
+  return swr::render_bdpt_impl(s, cam, opts, bdpt, rgb_out, samples_out, stream);
 }
 
 int swr_render_adjoint_timed(swr_scene* s, const swr_camera* cam, const swr_render_opts* o,

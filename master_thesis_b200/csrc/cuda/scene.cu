@@ -296,6 +296,8 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
     }
     if ((rc = swr::upload(&s->d_obj_boxes, pk.obj_boxes))) return rc;
     if ((rc = swr::upload(&s->d_mats, pk.mats))) return rc;
+    if ((rc = swr::upload(&s->d_lights, pk.lights))) return rc;
+    if ((rc = swr::upload(&s->d_light_tris, pk.light_tris))) return rc;
     s->scratch_bytes = 256;
     SWR_CUDA(cudaMalloc(&s->d_scratch, s->scratch_bytes));
     SWR_CUDA(cudaMemset(s->d_scratch, 0, s->scratch_bytes));
@@ -308,6 +310,9 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
     ds.mats = (const float4*)s->d_mats;
     ds.albedo = (const float*)s->d_albedo;
     ds.slot_of = (const uint32_t*)s->d_slot_of;
+    ds.lights = (const uint4*)s->d_lights;
+    ds.light_tris = (const float4*)s->d_light_tris;
+    ds.num_lights = (uint32_t)(pk.lights.size() / 4);
     ds.num_nodes = pk.num_nodes;
     ds.num_slots = (uint32_t)pk.slot_to_id.size();
     ds.num_objects = d->num_objects;
@@ -330,7 +335,7 @@ void swr_scene_destroy(swr_scene* s) {
   if (!s) return;
   swr::free_workspace(s);
   for (void* p : {s->d_nodes, s->d_tris, s->d_shade, s->d_tri_boxes, s->d_obj_boxes, s->d_mats,
-                  s->d_albedo, s->d_slot_of, s->d_scratch})
+                  s->d_albedo, s->d_slot_of, s->d_scratch, s->d_lights, s->d_light_tris})
     if (p) cudaFree(p);
   delete s;
 }

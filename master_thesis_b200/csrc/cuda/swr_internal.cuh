@@ -24,7 +24,9 @@ struct DevScene {
   const float4* mats;       // [num_objects * 3] (rgb dT) (rT tT eta light) (Le.rgb strength)
   const float* albedo;      // [num_slots * 3]   physical-mode diffuse albedo per triangle slot
   const uint32_t* slot_of;  // [num_tris]        triangle id -> slot
-  uint32_t num_nodes, num_slots, num_objects, num_tris;
+  const uint4* lights;      // [num_lights]      first light triangle, count, object, 0
+  const float4* light_tris; // [5 per triangle]  corners v0 v1 v2 and corner normals n0 n1 n2
+  uint32_t num_nodes, num_slots, num_objects, num_tris, num_lights;
 };
 
 }  // namespace swr
@@ -40,6 +42,8 @@ struct swr_scene {
   void* d_mats = nullptr;
   void* d_albedo = nullptr;
   void* d_slot_of = nullptr;
+  void* d_lights = nullptr;
+  void* d_light_tris = nullptr;
   void* d_scratch = nullptr;  // small per-scene scratch (work counters)
   size_t scratch_bytes = 0;
   uint32_t depth = 0;

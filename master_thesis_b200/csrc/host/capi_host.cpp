@@ -138,11 +138,29 @@ int swr_camera_make(const float position[3], float angle_theta, float angle_phi,
 int swr_renderer_load(const char* renderer_path, uint32_t* max_depth, uint32_t* spp) {
   if (!renderer_path) return set_error(SWR_ERR_INVALID, "swr: null argument");
   try {
-    swr::RendererParams r = swr::load_renderer_file(renderer_path);
+    swr::RendererParams r = swr::load_renderer_file(renderer_path, false);
     if (r.name != "PathTracer")
       return set_error(SWR_ERR_UNSUPPORTED, "swr: renderer \"" + r.name + "\" is not provided");
     if (max_depth) *max_depth = r.vision_jump_count;
     if (spp) *spp = r.rays_per_pixel;
+    return SWR_OK;
+  } catch (const swr::SurfaceError& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SWR_ERR_PARSE, std::string("swr: ") + e.what());
+  }
+}
+
+int swr_renderer_load_params(const char* renderer_path, swr_renderer_params* out) {
+  if (!renderer_path || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  try {
+    swr::RendererParams r = swr::load_renderer_file(renderer_path);
+    std::memset(out, 0, sizeof(*out));
+    out->kind = r.name == "PathTracer" ? SWR_RENDERER_PATH_TRACER : SWR_RENDERER_BIDIRECTIONAL;
+    out->vision_jumps = r.vision_jump_count;
+    out->light_jumps = r.light_jump_count;
+    out->max_depth = r.max_depth;
+    out->spp = r.rays_per_pixel;
     return SWR_OK;
   } catch (const swr::SurfaceError& e) {
     return set_error(e.code, e.what());

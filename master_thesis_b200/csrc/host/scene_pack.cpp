@@ -116,6 +116,28 @@ int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene&
       }
     }
   });
+  {
+    // triangles of each object are contiguous in id order (tri_object is non-decreasing)
+    std::vector<uint32_t> first(no + 1, 0);
+    for (uint32_t t = 0; t < nt; ++t) first[d->tri_object[t] + 1]++;
+    for (uint32_t o = 0; o < no; ++o) first[o + 1] += first[o];
+    for (uint32_t o = 0; o < no; ++o) {
+      if (!d->materials[o].light_source) continue;
+      const uint32_t n = first[o + 1] - first[o];
+      out.lights.insert(out.lights.end(), {(uint32_t)(out.light_tris.size() / 5), n, o, 0u});
+      for (uint32_t t = first[o]; t < first[o + 1]; ++t) {
+        float w[20] = {0};
+        for (int c = 0; c < 3; ++c) {
+          const uint32_t vi = d->tri_vertices[3 * (size_t)t + c];
+          for (int k = 0; k < 3; ++k) {
+            w[3 * c + k] = d->vertex_pos[3 * (size_t)vi + k];
+            w[9 + 3 * c + k] = d->vertex_normal[3 * (size_t)vi + k];
+          }
+        }
+        for (int q = 0; q < 5; ++q) out.light_tris.push_back(make_float4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
+      }
+    }
+  }
   for (uint32_t o = 0; o < no; ++o) {
     const swr_material& m = d->materials[o];
     for (int k = 0; k < 3; ++k) {

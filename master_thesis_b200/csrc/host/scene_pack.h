@@ -22,6 +22,11 @@ struct PackedScene {
   std::vector<uint32_t> slot_of;  // triangle id -> slot
   std::vector<uint32_t> slot_to_id;
   std::vector<float> prim_boxes;  // without the host BVH: 6 per triangle, the traversal boxes
+  // light sources in object order (the reference's lightSources list, mesh_manager.cpp:52-56):
+  // 4 words each (first light triangle, triangle count, object, 0), and per light triangle in
+  // triangle-id order its corners v0 v1 v2 and corner normals n0 n1 n2 (20 floats, 18 used)
+  std::vector<uint32_t> lights;
+  std::vector<float4> light_tris;
   uint32_t num_nodes = 0, depth = 0;
 };
 

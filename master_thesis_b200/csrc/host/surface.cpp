@@ -577,15 +577,20 @@ CameraFrame camera_frame(const CameraParams& c, uint32_t width, uint32_t height,
   return f;
 }
 
-RendererParams load_renderer_file(const std::string& path) {
+RendererParams load_renderer_file(const std::string& path, bool bdpt_keys) {
   auto entries = parse_input_file(path);
   if (entries.empty()) throw SurfaceError(kErrParse, "Renderer", "no entry in \"" + path + "\"");
   RendererParams r;
   r.name = entries[0].name;
   if (r.name != "PathTracer" && r.name != "BidirectionalPathTracer")
     throw SurfaceError(kErrInvalid, "getRenderer not found", r.name);
-  if (r.name == "PathTracer") {
+  if (r.name == "PathTracer") {  // path_tracer.cpp:13-16
     r.vision_jump_count = entries[0].get_uint("visionJumpCount");
+    r.rays_per_pixel = entries[0].get_uint("raysPerPixel");
+  } else if (bdpt_keys) {  // bidirectional_path_tracer.cpp:13-18
+    r.vision_jump_count = entries[0].get_uint("visionJumpCount");
+    r.light_jump_count = entries[0].get_uint("lightJumpCount");
+    r.max_depth = entries[0].get_uint("maxDepth");
     r.rays_per_pixel = entries[0].get_uint("raysPerPixel");
   }
   return r;

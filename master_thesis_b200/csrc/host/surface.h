@@ -172,7 +172,10 @@ struct RendererParams {
   std::string name;
   unsigned vision_jump_count = 0;
   unsigned rays_per_pixel = 0;
+  unsigned light_jump_count = 0;  // BidirectionalPathTracer only
+  unsigned max_depth = 0;         // BidirectionalPathTracer only
 };
-RendererParams load_renderer_file(const std::string& path);
+// Renderer file; the bidirectional tracer's keys are read (and required) only with bdpt_keys.
+RendererParams load_renderer_file(const std::string& path, bool bdpt_keys = true);
 
 }  // namespace swr

@@ -161,6 +161,7 @@ struct Traversal {
   uint2 ng;  // node group: x = child_base, y = hits (bits 24..31, visit order) | imask (bits 0..7)
   uint2 tg;  // triangle group: x = base, y = hit bits 0..23
   BestHit hit;
+  uint32_t any;  // occlusion query: stop at the first accepted candidate
   GroupStack st;
   uint32_t host_turn;  // host build only: drives the alternating postponing decision
 
@@ -181,9 +182,22 @@ struct Traversal {
     hit.t = INFINITY;
     hit.d2 = INFINITY;
     tprune = INFINITY;
+    any = 0u;
     st.bind(stack_shared, stack_stride);
     ng = make_uint2(0u, (1u << (24 + oct)) | 1u);  // the root, as inner slot 0
     tg = make_uint2(0u, 0u);
+  }
+
+  // Occlusion query (Scene::isOccluded, scene.cpp:58-83): finished at the first candidate whose
+  // squared distance is <= dist2; hit.slot stays 0xFFFFFFFF when there is none. The candidate
+  // rule is the closest-hit one started from a best of (dist2, no rank), whose first acceptance is
+  // exactly "d2 <= dist2"; nodes beyond sqrt(dist2) (with the pruning slack) are skipped, which
+  // keeps every such candidate because d is of unit length.
+  SWR_HD void init_occlusion(f3 o_, f3 d_, float dist2, uint2* stack_shared, int stack_stride) {
+    init(o_, d_, stack_shared, stack_stride);
+    hit.d2 = dist2;
+    tprune = sqrtf(dist2) * kPruneSlack;
+    any = 1u;
   }
 
   // The finished ray's hit with its triangle id and object read from the triangle record.
@@ -307,6 +321,11 @@ struct Traversal {
       hit.t = t;
       hit.d2 = d2;
       tprune = t * kPruneSlack;
+      if (any) {  // occluded: drop the remaining work so the pop below ends the query
+        ng.y = 0u;
+        tg.y = 0u;
+        st.sp = 0;
+      }
     } while (false);
 
     if (!(ng.y & 0xFF000000u) && tg.y == 0) {

@@ -32,11 +32,11 @@ def _setup(tmp_path, spp=8, depth=5):
 def test_cli_rejects_unknown_renderer(tmp_path):
     s, exe, _ = _setup(tmp_path)
     bad = tmp_path / "B.renderer"
-    bad.write_text("BidirectionalPathTracer\n\tvisionJumpCount(5)\n\tlightJumpCount(5)\n\traysPerPixel(4)\n")
+    bad.write_text("PhotonMapper\n\tvisionJumpCount(5)\n\traysPerPixel(4)\n")
     p = subprocess.run([exe, str(bad), s["scene"], "8", "8", "2", s["camera"], str(tmp_path / "o.ppm")],
                        capture_output=True, text=True, timeout=120, env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
     assert p.returncode != 0
-    assert "BidirectionalPathTracer" in p.stderr and "not provided" in p.stderr
+    assert "getRenderer not found" in p.stderr and "PhotonMapper" in p.stderr
     assert not (tmp_path / "o.ppm").exists()
 
 
@@ -59,3 +59,24 @@ def test_cli_image_equals_library_render(tmp_path):
     got = np.frombuffer(data[len(header):], np.uint8).reshape(H, W, 3)
     assert np.array_equal(got, ref)
     assert ref.max() > 0
+
+
+@pytest.mark.gpu
+def test_cli_bidirectional_equals_library_render(tmp_path):
+    import master_thesis_b200 as swr
+    W, H = 48, 32
+    s, exe, _ = _setup(tmp_path)
+    rpath = tmp_path / "BDPT.renderer"
+    rpath.write_text("BidirectionalPathTracer\n\tvisionJumpCount(5)\n\tlightJumpCount(4)\n\tmaxDepth(5)\n"
+                     "\traysPerPixel(6)\n")
+    out = tmp_path / "bd.ppm"
+    p = subprocess.run([exe, str(rpath), s["scene"], str(W), str(H), "4", s["camera"], str(out)],
+                       capture_output=True, text=True, timeout=300, env=dict(os.environ, SWR_SEED="9"))
+    assert p.returncode == 0, p.stdout + p.stderr
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    cam = swr.load_camera(s["camera"], W, H)
+    img = swr.Scene(sd).render_bdpt(cam, W, H, 6, 5, 4, 5, seed=9)
+    header = b"P6\n%d\n%d\n255\n" % (W, H)
+    got = np.frombuffer(out.read_bytes()[len(header):], np.uint8).reshape(H, W, 3)
+    ref = swr.quantize_rgb8(img.cpu().numpy())
+    assert np.array_equal(got, ref) and ref.max() > 0

@@ -123,6 +123,27 @@ def test_renderer_file(tmp_path):
     assert e.value.code == 7
 
 
+def test_renderer_params_both_renderers(tmp_path):
+    p = tmp_path / "PT.renderer"
+    p.write_text("PathTracer\n\tvisionJumpCount(5)\n\traysPerPixel(2500)\n")
+    assert swr.load_renderer_params(str(p)) == dict(kind="PathTracer", vision_jumps=5, light_jumps=0, max_depth=0,
+                                                    spp=2500)
+    b = tmp_path / "BD.renderer"  # res/renderer/SoftwareRendererBidirectionalPathTracer.renderer
+    b.write_text("BidirectionalPathTracer\n\tvisionJumpCount(5)\n\tlightJumpCount(3)\n\tmaxDepth(4)\n"
+                 "\traysPerPixel(100)\n")
+    assert swr.load_renderer_params(str(b)) == dict(kind="BidirectionalPathTracer", vision_jumps=5, light_jumps=3,
+                                                    max_depth=4, spp=100)
+    m = tmp_path / "M.renderer"  # a key the bidirectional tracer requires is missing
+    m.write_text("BidirectionalPathTracer\n\tvisionJumpCount(5)\n\traysPerPixel(1)\n")
+    with pytest.raises(swr.SwrError):
+        swr.load_renderer_params(str(m))
+    u = tmp_path / "U.renderer"
+    u.write_text("PhotonMapper\n\traysPerPixel(1)\n")
+    with pytest.raises(swr.SwrError) as e:
+        swr.load_renderer_params(str(u))
+    assert "getRenderer not found" in str(e.value)
+
+
 def test_missing_files_report_io_errors(tmp_path):
     with pytest.raises(swr.SwrError) as e:
         swr.load_scene(str(tmp_path / "nope.scene"), str(tmp_path) + "/")
