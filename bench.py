@@ -35,6 +35,9 @@ CONFIGS = {
     "c2": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=64,
                depth=8, seed=2024, microbench_rays=1 << 24),
     "c1": dict(kind="cornell", W=256, H=256, spp=16, depth=5, seed=1),
+    # the Cornell scene through the bidirectional tracer with the reference's own BDPT renderer
+    # settings (res/renderer/SoftwareRendererBidirectionalPathTracer.renderer: 5/5/5)
+    "c1b": dict(kind="cornell", renderer="bdpt", W=256, H=256, spp=16, depth=5, light_jumps=5, max_depth=5, seed=1),
     # the terrain scene at a reduced image size, for profiler captures of single kernel launches
     "c2s": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=16,
                 depth=8, seed=2024),
@@ -136,9 +139,12 @@ def profile_traffic():
 
 
 def cpu_reference(cfg, files, threads, budget_s, impl_bin):
-    """Times the reference's own PathTracer (unmodified sources) on a bounded pixel sample."""
+    """Times the reference's own PathTracer or BidirectionalPathTracer (unmodified sources) on a
+    bounded pixel sample."""
     W, H, spp, depth = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
     fast = ["fast"] if cfg["kind"] == "terrain" else []
+    if cfg.get("renderer") == "bdpt":
+        fast += ["bdpt", str(cfg["light_jumps"]), str(cfg["max_depth"])]
 
     def run(pixels):
         out = subprocess.run([impl_bin, files["basepath"], files["scene"], files["camera"], str(W), str(H), str(spp),
@@ -251,6 +257,64 @@ def run_batch(args, cfg):
                    (len(jobs), tris, samples, cfg["depth"]), "tuned": tuned},
         "per_scene_launches": {"value": samples / (s_ms / 1e3) / 1e6, "ms_per_step": s_ms},
         "speedup_vs_per_scene": s_ms / b_ms, "max_rel_image_diff_vs_per_scene": diff, "setup_s": setup_s}))
+
+
+def run_bdpt(args, cfg, files, workload):
+    """Bidirectional tracer: K timed images (L2 flushed before each) and the same through a host
+    output buffer; the reference's own BidirectionalPathTracer timed on the host cores beside it."""
+    import torch
+    import master_thesis_b200 as swr
+    W, H, spp, vj, lj, md = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"], cfg["light_jumps"], cfg["max_depth"]
+    sd = swr.load_scene(files["scene"], files["basepath"])
+    sc = swr.Scene(sd)
+    cam = swr.load_camera(files["camera"], W, H)
+    out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    render = lambda o, seed: sc.render_bdpt(cam, W, H, spp, vj, lj, md, seed=seed, out=o, stream=stream)
+    for k in range(max(args.warmup, 3)):
+        render(out, k)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ms = []
+    for k in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        render(out, 100 + k)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
+    e2e = []
+    for k in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        render(host, 200 + k)
+        e1.record(stream)
+        e1.synchronize()
+        e2e.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    samples = W * H * spp
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import refdump
+        if os.path.exists(refdump.REF_BENCH):
+            r = cpu_reference(cfg, files, os.cpu_count() or 1, args.cpu_budget, refdump.REF_BENCH)
+            cpu = {"value": r["msamples_per_s"], "unit": "Msamples/s", "cores": os.cpu_count() or 1,
+                   "kind": "reference", "sample": "%d of %d pixels (every k-th), %d spp" % (r["pixels"], W * H, spp)}
+    t = sum(ms) / len(ms)
+    print(json.dumps({
+        "metric": "Msamples/s (bidirectional path tracer)", "value": samples / (t / 1e3) / 1e6, "unit": "Msamples/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
+        "config": {"workload": workload, "vision_jumps": vj, "light_jumps": lj, "max_depth": md,
+                   "l2": "flushed between steps (256 MB write)"},
+        "e2e": {"value": samples / (sum(e2e) / len(e2e) / 1e3) / 1e6, "unit": "Msamples/s", "h2d_bytes_per_step": 96,
+                "d2h_bytes_per_step": W * H * 12},
+        "clocks": clk, "cpu_baseline": cpu}))
 
 
 def run_diff(args, cfg):
@@ -447,6 +511,11 @@ def main():
                                                   cfg["spheres"], cfg["subdiv"], cfg["lights"], W, H, spp, depth)
                 if cfg["kind"] == "terrain" else
                 "cornell 36 tris, %dx%d, %d spp, depth %d, reference semantics" % (W, H, spp, depth))
+    bdpt = cfg.get("renderer") == "bdpt"
+    metric = "Msamples/s (bidirectional path tracer)" if bdpt else METRIC
+    if bdpt:
+        workload = "cornell 36 tris, %dx%d, %d spp, bidirectional: vision %d, light %d, maxDepth %d" % (
+            W, H, spp, depth, cfg["light_jumps"], cfg["max_depth"])
     tmp = args.scene_dir or tempfile.mkdtemp(prefix="swr_bench_")
     files_path = os.path.join(tmp, "files.json")
     if os.path.exists(files_path):
@@ -467,7 +536,7 @@ def main():
         v = res["msamples_per_s"]
         sample = "%d of %d pixels (every k-th), %d spp, depth %d, %d threads" % (res["pixels"], W * H, spp, depth, nproc)
         print(json.dumps({
-            "impl": "reference", "metric": METRIC, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
+            "impl": "reference", "metric": metric, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": W * H * spp / (v * 1e6) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene files)", "config": {"workload": workload},
@@ -478,6 +547,9 @@ def main():
 
     import torch
     torch.cuda.set_device(local_rank)
+    if bdpt:
+        run_bdpt(args, cfg, files, workload)
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist_mod
@@ -494,6 +566,11 @@ def main():
     torch.cuda.synchronize()
     t2 = time.time()
     stats = scene.stats()
+    # the same scene through the device builder (timed for the setup report, then released)
+    t3 = time.time()
+    swr.Scene(sd, builder="device").close()
+    torch.cuda.synchronize()
+    t4 = time.time()
     cam = swr.load_camera(files["camera"], W, H)
     seed = 1000 + rank
     out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
@@ -620,7 +697,7 @@ def main():
             "gpu_launches": int(launches_total),
             "clocks": clk,
             "cpu_baseline": cpu,
-            "setup_s": {"load": t1 - t0, "build_upload": t2 - t1},
+            "setup_s": {"load": t1 - t0, "build_upload": t2 - t1, "build_upload_device_builder": t4 - t3},
         }
         print(json.dumps(line))
     if dist is not None:

@@ -7,6 +7,10 @@
 // so it spans the whole frame.
 //
 //   ref_bench <basepath> <scene> <camera> <W> <H> <spp> <depth> <threads> <max_pixels> [fast]
+//             [bdpt <lightJumpCount> <maxDepth>]
+//
+// With "bdpt" the timed renderer is the reference's BidirectionalPathTracer (visionJumpCount =
+// depth) instead of its PathTracer.
 //
 // With "fast", scene loading replaces the two BVH::init calls (mesh topology, scene topology) by an
 // exact re-implementation of the same agglomerative build (tree-identical, checked by the tests)
@@ -38,6 +42,7 @@
 #define private public
 #include "camera.h"
 #include "graphic/graphics_engine.h"
+#include "graphic/bidirectional_path_tracer.h"
 #include "graphic/graphics_object.h"
 #include "graphic/path_tracer.h"
 #include "graphic/scene.h"
@@ -147,7 +152,7 @@ std::vector<GraphicsObject*> load_fast(const std::string& basepath, const std::s
 int main(int argc, char** argv) {
   if (argc < 10) {
     std::fprintf(stderr,
-                 "usage: ref_bench basepath scene camera W H spp depth threads max_pixels [fast]\n");
+                 "usage: ref_bench basepath scene camera W H spp depth threads max_pixels [fast] [bdpt light maxdepth]\n");
     return 2;
   }
   std::string basepath = argv[1], scenePath = argv[2], cameraPath = argv[3];
@@ -155,14 +160,37 @@ int main(int argc, char** argv) {
   unsigned spp = (unsigned)std::atoi(argv[6]), depth = (unsigned)std::atoi(argv[7]);
   unsigned threads = (unsigned)std::atoi(argv[8]);
   uint64_t maxPixels = std::strtoull(argv[9], nullptr, 10);
-  bool fast = argc > 10 && std::string(argv[10]) == "fast";
+  bool fast = false;
+  bool bdpt = false;
+  unsigned light_jumps = 0, max_depth = 0;
+  for (int a = 10; a < argc; ++a) {
+    const std::string k = argv[a];
+    if (k == "fast") fast = true;
+    if (k == "bdpt" && a + 2 < argc) {
+      bdpt = true;
+      light_jumps = (unsigned)std::atoi(argv[a + 1]);
+      max_depth = (unsigned)std::atoi(argv[a + 2]);
+      a += 2;
+    }
+  }
 
   auto t0 = std::chrono::steady_clock::now();
   GraphicsEngine engine;
   engine.imageSize = Vector2u({W, H});
-  PathTracer* pt = new PathTracer();
-  pt->visionJumpCount = depth;
-  pt->raysPerPixel = spp;
+  Renderer* pt;
+  if (bdpt) {
+    BidirectionalPathTracer* b = new BidirectionalPathTracer();
+    b->visionJumpCount = depth;
+    b->lightJumpCount = light_jumps;
+    b->maxDepth = max_depth;
+    b->raysPerPixel = spp;
+    pt = b;
+  } else {
+    PathTracer* p = new PathTracer();
+    p->visionJumpCount = depth;
+    p->raysPerPixel = spp;
+    pt = p;
+  }
   MeshManager* mm = nullptr;
   if (fast) {
     std::vector<GraphicsObject*> lights;
