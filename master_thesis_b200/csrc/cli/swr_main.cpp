@@ -8,7 +8,8 @@
 // thread_count sets the host threads of the BVH build (the render itself runs on the GPU).
 // The environment variable SWR_SEED (unsigned integer, default 0) selects the random-number
 // stream; the reference draws from a shared host generator instead, so its images agree with
-// these in distribution, not pixel by pixel. SWR_DEVICE selects the CUDA device (default 0).
+// these in distribution, not pixel by pixel. SWR_DEVICE selects the CUDA device (default 0);
+// SWR_BUILDER=device builds the BVH on the GPU (same image).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -75,6 +76,8 @@ int main(int argc, char* argv[]) {
   }
   swr_build_opts bo = {};
   bo.threads = threads;
+  const char* builder_env = std::getenv("SWR_BUILDER");
+  if (builder_env && std::string(builder_env) == "device") bo.builder = SWR_BUILD_DEVICE;
   swr_scene* scene = nullptr;
   if (swr_scene_create(&desc, &bo, &scene)) return fail("scene build");
   swr_host_scene_free(hs);
