@@ -40,7 +40,7 @@ CONFIGS = {
     "c1b": dict(kind="cornell", renderer="bdpt", W=256, H=256, spp=16, depth=5, light_jumps=5, max_depth=5, seed=1),
     # the terrain scene at a reduced image size, for profiler captures of single kernel launches
     "c2s": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=16,
-                depth=8, seed=2024),
+                depth=8, seed=2024, microbench_rays=1 << 22),
     # batched: 256 scenes, 1k-500k triangles (log-uniform), image sides {64..1024}, spp {4,16,64}, depth 6
     "c3": dict(kind="batch", scenes=256, depth=6, seed=7, sides=[64, 128, 256, 512, 1024], spps=[4, 16, 64],
                tris=[1e3, 5e5]),
