@@ -32,8 +32,10 @@ sys.path.insert(0, ROOT)
 
 CONFIGS = {
     # name: scene parameters, image, spp, depth
+    # wave_size: paths in flight, 2^25 measured best for this image (2^23..2^27 swept; the
+    # library's default of 2^23 bounds a scene's queue memory at 1.2 GB)
     "c2": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=64,
-               depth=8, seed=2024, microbench_rays=1 << 24),
+               depth=8, seed=2024, microbench_rays=1 << 24, wave_size=1 << 25),
     "c1": dict(kind="cornell", W=256, H=256, spp=16, depth=5, seed=1),
     # the Cornell scene through the bidirectional tracer with the reference's own BDPT renderer
     # settings (res/renderer/SoftwareRendererBidirectionalPathTracer.renderer: 5/5/5)
@@ -578,7 +580,8 @@ def main():
     stream = torch.cuda.current_stream()
 
     def render(o, **kw):
-        return scene.render(cam, W, H, spp, depth, seed=seed, out=o, stream=stream, return_profile=True, **kw)
+        return scene.render(cam, W, H, spp, depth, seed=seed, out=o, stream=stream, return_profile=True,
+                            wave_size=cfg.get("wave_size", 0), **kw)
 
     for _ in range(max(args.warmup, 3)):
         render(out)
@@ -677,6 +680,7 @@ def main():
             "config": {"workload": workload, "triangles": int(sd.num_triangles), "objects": int(sd.num_objects),
                        "pixels": W * H, "spp": spp, "depth": depth, "l2": "flushed between steps (256 MB write)",
                        "parallelism": "independent images per GPU" if world > 1 else "single GPU",
+                       "wave_size": cfg.get("wave_size", 0) or (1 << 23),
                        "bvh_nodes": stats["nodes"], "bvh_depth": stats["depth"]},
             "e2e": {"value": e2e_value, "unit": "Msamples/s",
                     "h2d_bytes_per_step": int(e2e_prof[-1]["h2d_bytes"]),

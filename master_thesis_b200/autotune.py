@@ -18,8 +18,9 @@ import torch
 
 CACHE = os.environ.get("SWR_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "swr_b200", "tune.json"))
 
-RENDER_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23], refill=[4, 8, 16], block_size=[256], trace_blocks=[0])
-BATCH_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23], refill=[4, 8, 16])
+RENDER_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16], block_size=[256],
+                   trace_blocks=[0])
+BATCH_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16])
 
 
 def _load():
