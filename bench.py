@@ -48,6 +48,13 @@ CONFIGS = {
                tris=[1e3, 5e5]),
     # the same batch restricted to small jobs (64x64..128x128, 4-16 spp, 1k-50k triangles): launch-bound per scene
     "c3s": dict(kind="batch", scenes=256, depth=6, seed=7, sides=[64, 128], spps=[4, 16], tris=[1e3, 5e4]),
+    # the RayTrace program's PathTracer (Vulkan shaders restated in CUDA) with its own renderer file
+    # settings (res/renderer/path_tracer.renderer: visionJumpCount 5, visionRayPerPixelCount 13) on
+    # the Cornell scene at 1920x1080, and on the terrain scene (no CPU baseline: the oracle's closest
+    # hit tests every triangle)
+    "c6": dict(kind="cornell", renderer="rt", W=1920, H=1080, spp=13, depth=5, seed=1),
+    "c6t": dict(kind="terrain", renderer="rt", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080,
+                spp=13, depth=5, seed=2024),
     # differentiable: tessellated Cornell (~49k triangles), 512x512, 32 spp primal + 32 spp adjoint, depth 6
     "c4": dict(kind="diff", W=512, H=512, spp=32, depth=6, seed=11),
     # batched inverse rendering: 64 scenes (5k-200k triangles, 128^2-512^2), 16 spp primal/adjoint, depth 5,
@@ -319,6 +326,89 @@ def run_bdpt(args, cfg, files, workload):
         "clocks": clk, "cpu_baseline": cpu}))
 
 
+def rt_cpu_port(cfg, files, threads, budget_s):
+    """The oracle's CPU restatement of the RayTrace PathTracer timed on a bounded run of whole
+    image rows through the image centre (all host threads)."""
+    import master_thesis_b200 as swr
+    from oracle import oracle as O
+    W, H, spp, vj = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
+    sd = swr.load_scene(files["scene"], files["basepath"])
+    cam = swr.load_camera(files["camera"], W, H)
+    vi, pi, org = swr.camera_arrays(cam)
+    osc, ocam = O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org)
+    mid = (H // 2) * W
+    t0 = time.time()
+    O.rt_render(osc, ocam, W, H, spp, vj, mid, mid + W, threads=threads)
+    rate = W / max(time.time() - t0, 1e-6)
+    rows = int(max(1, min(H, budget_s * rate / W)))
+    p0 = max(0, (H - rows) // 2) * W
+    t0 = time.time()
+    O.rt_render(osc, ocam, W, H, spp, vj, p0, p0 + rows * W, threads=threads)
+    dt = time.time() - t0
+    return {"msamples_per_s": rows * W * spp / dt / 1e6, "pixels": rows * W, "rows": rows, "seconds": dt}
+
+
+def run_rt(args, cfg, files, workload):
+    """RayTrace PathTracer frames (the LCG is seeded by the pixel, so every frame is the same
+    image): K timed frames with L2 flushed before each, the same through a pinned host output
+    buffer (swr_rt_render_frame, device->host copy inside), and the two denoisers on the frame."""
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import rt
+    W, H, spp, vj = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
+    t0 = time.time()
+    sd = swr.load_scene(files["scene"], files["basepath"])
+    t1 = time.time()
+    sc = swr.Scene(sd)
+    torch.cuda.synchronize()
+    t2 = time.time()
+    cam = swr.load_camera(files["camera"], W, H)
+    rgba = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    params = dict(vision_jumps=vj, spp=spp, denoisers=[])
+    frame = lambda out: rt.render_frame(sc, cam, W, H, params, out=out, stream=stream)
+    for _ in range(max(args.warmup, 3)):
+        frame(rgba)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ms = _events_ms(lambda: frame(rgba), args.steps, flush)
+    host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True).numpy()
+    e2e = _events_ms(lambda: frame(host), args.steps, flush)
+    den = torch.empty_like(rgba)
+    g_ms = _events_ms(lambda: rt.denoise_gauss(rgba, 5, 1.0, out=den, stream=stream), args.steps, flush)
+    m_ms = _events_ms(lambda: rt.denoise_median(rgba, out=den, stream=stream), args.steps, flush)
+    clk = clocks.stop()
+    samples = W * H * spp
+    cpu = None
+    if not args.no_cpu_baseline and cfg["kind"] == "cornell":
+        nproc = os.cpu_count() or 1
+        r = rt_cpu_port(cfg, files, nproc, args.cpu_budget)
+        cpu = {"value": r["msamples_per_s"], "unit": "Msamples/s", "cores": nproc, "kind": "port",
+               "sample": "%d image rows through the centre (%d of %d pixels), %d spp, the oracle's C restatement "
+                         "on %d threads" % (r["rows"], r["pixels"], W * H, spp, nproc)}
+    peak, peak_kind = measured_peaks()
+    img_bytes = W * H * 8  # one rgba8 image read and one written
+    print(json.dumps({
+        "metric": "Msamples/s (RayTrace PathTracer frame)", "value": samples / (ms / 1e3) / 1e6,
+        "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene files)",
+        "config": {"workload": workload, "triangles": int(sd.num_triangles), "l2": "flushed between steps (256 MB write)"},
+        "e2e": {"value": samples / (e2e / 1e3) / 1e6, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": W * H * 4},
+        "gpu_launches": 1 * args.steps,
+        "roofline": None,
+        "roofline_note": "k_rt_path: the scene's nodes and triangles stay in L1/L2 (no HBM bound); see the "
+                         "denoisers for the memory-bound kernels",
+        "denoisers": {"gauss_5_ms": g_ms, "median_ms": m_ms,
+                      "gauss_5_frac_of_hbm": img_bytes / (g_ms / 1e3) / 1e9 / peak,
+                      "median_frac_of_hbm": img_bytes / (m_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+        "clocks": clk, "cpu_baseline": cpu,
+        "setup_s": {"load": t1 - t0, "build_upload": t2 - t1}}))
+
+
 def run_diff(args, cfg):
     """C4: physical-mode primal render vs the path-replay adjoint of an L2 image loss."""
     import torch
@@ -514,10 +604,15 @@ def main():
                 if cfg["kind"] == "terrain" else
                 "cornell 36 tris, %dx%d, %d spp, depth %d, reference semantics" % (W, H, spp, depth))
     bdpt = cfg.get("renderer") == "bdpt"
+    rtp = cfg.get("renderer") == "rt"
     metric = "Msamples/s (bidirectional path tracer)" if bdpt else METRIC
     if bdpt:
         workload = "cornell 36 tris, %dx%d, %d spp, bidirectional: vision %d, light %d, maxDepth %d" % (
             W, H, spp, depth, cfg["light_jumps"], cfg["max_depth"])
+    if rtp:
+        metric = "Msamples/s (RayTrace PathTracer frame)"
+        workload = "%s, %dx%d, RayTrace PathTracer: visionJumpCount %d, visionRayPerPixelCount %d" % (
+            "cornell 36 tris" if cfg["kind"] == "cornell" else "terrain (as c2)", W, H, depth, spp)
     tmp = args.scene_dir or tempfile.mkdtemp(prefix="swr_bench_")
     files_path = os.path.join(tmp, "files.json")
     if os.path.exists(files_path):
@@ -527,6 +622,27 @@ def main():
         json.dump(files, open(files_path, "w"))
     nproc = os.cpu_count() or 1
 
+    if args.impl == "reference" and rtp:
+        # the RayTrace program's shaders need a Vulkan ray tracing pipeline, which this machine
+        # cannot bring up: its CPU restatement (the oracle) stands in as the reference arm
+        if rank != 0:
+            return
+        if cfg["kind"] != "cornell":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's shaders need a Vulkan ray "
+                                                                  "tracing pipeline (unavailable on this box); the "
+                                                                  "CPU restatement tests every triangle"}))
+            return
+        r = rt_cpu_port(cfg, files, nproc, args.cpu_budget * max(1, args.steps // 5))
+        v = r["msamples_per_s"]
+        sample = "%d image rows (%d of %d pixels), %d spp, %d threads" % (r["rows"], r["pixels"], W * H, spp, nproc)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": W * H * spp / (v * 1e6) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene files)", "config": {"workload": workload},
+            "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": nproc, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
     if args.impl == "reference":
         if rank != 0:
             return
@@ -551,6 +667,9 @@ def main():
     torch.cuda.set_device(local_rank)
     if bdpt:
         run_bdpt(args, cfg, files, workload)
+        return
+    if rtp:
+        run_rt(args, cfg, files, workload)
         return
     dist = None
     if world > 1:

@@ -326,6 +326,84 @@ int swr_render_adjoint_batch(swr_batch* batch, const swr_adjoint_job* jobs, uint
 int swr_render_noalloc(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                        float* rgb_out, float* samples_out, void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * The Vulkan application's PathTracer and denoisers (the RayTrace program: src/main.cpp:58-76,
+ * src/graphic/renderer/path_tracer.cpp, src/graphic/denoiser/gauss_denoiser.cpp and
+ * median_denoiser.cpp, and their shaders
+ * res/shader/path_tracer_vision_raygen.rgen, path_tracer.glsl, v1.glsl, helper.glsl,
+ * v1_closesthit.rchit, v1_miss.rmiss, denoise_gauss_comp.comp, denoise_median_comp.comp),
+ * restated as CUDA kernels over a built scene. No graphics API is involved. Where GLSL leaves
+ * precision to the implementation (division, sqrt, sin, cos, acos, normalize, multiply-add
+ * fusion) one IEEE choice is fixed; the same choice is made by the CPU restatement the tests use.
+ */
+
+/* traceRay's closest hit (v1.glsl:148-161; the pipeline's opaque triangle query): the smallest
+ * ray parameter t in [0.001, 10000], ties to the lower triangle id, with this library's
+ * Moller-Trumbore arithmetic. Rays and hits as in swr_trace_closest; dist2 is not computed
+ * (+inf). */
+int swr_rt_trace_closest(swr_scene* scene, const float* ray_o, const float* ray_d, uint64_t n,
+                         swr_hit* out, void* stream);
+
+typedef struct swr_rt_opts {
+  uint32_t width, height;  /* launch size = image size */
+  uint32_t vision_jumps;   /* visionJumpCount (path_tracer.cpp:30-33), <= 65536 */
+  uint32_t spp;            /* visionRayPerPixelCount, 1..2^24 */
+  uint32_t refill;         /* idle lanes of a warp that take new pixels (1..32), 0 = 8 */
+  uint32_t reserved[3];
+} swr_rt_opts;
+
+/* One PathTracer frame (path_tracer_vision_raygen.rgen:8-60): per pixel the LCG random numbers
+ * of helper.glsl seeded by the launch id, the camera ray of getVisionRay, traceRay with up to four
+ * back-face retries, and visionRayPerPixelCount paths of up to visionJumpCount-1 jumps that count
+ * when they reach a light from its front; lights seen directly give color * lightStrength.
+ * rgb_out [height*width*3] receives finalColor (optional), rgba8_out [height*width*4] the rgba8
+ * texel the shader stores (optional; clamp, *255, round to nearest even; alpha 0). Device or host
+ * memory. The camera is a swr_camera (the RayTrace camera file has the same keys). */
+int swr_rt_render(swr_scene* scene, const swr_camera* cam, const swr_rt_opts* opts, float* rgb_out,
+                  uint8_t* rgba8_out, void* stream);
+
+/* GaussDenoiser weights (gauss_denoiser.cpp:31-46): w[i] = exp(-(i - (k-1))^2 / (2 sigma^2)),
+ * normalised by their sum; exp is the double exp rounded to float. kernel_size odd, 1..19 (the
+ * shader reads w[0..kernel_size-1] only for odd sizes; the weight array holds 20 floats);
+ * sigma > 0. out[kernel_size], host memory. */
+int swr_rt_gauss_weights(uint32_t kernel_size, float sigma, float* out);
+/* denoise_gauss_comp.comp: out = sum over in-image offsets (x outer, y inner, -k/2..k/2) of
+ * texel * w[x + k/2] * w[y + k/2], stored as rgba8. in and out are separate rgba8 images
+ * [height*width*4], device or host memory. */
+int swr_rt_denoise_gauss(const uint8_t* rgba8_in, uint8_t* rgba8_out, uint32_t width, uint32_t height,
+                         uint32_t kernel_size, float sigma, void* stream);
+/* denoise_median_comp.comp: per-channel median of the 3x3 neighbourhood. The shader leaves
+ * texels outside the image undefined; here they count as 0. */
+int swr_rt_denoise_median(const uint8_t* rgba8_in, uint8_t* rgba8_out, uint32_t width,
+                          uint32_t height, void* stream);
+
+/* Renderer file of the RayTrace program (src/main.cpp:153-168): the first entry names the
+ * renderer (PathTracer: visionJumpCount, visionRayPerPixelCount), every further entry a denoiser
+ * applied in file order (GaussDenoiser: kernelSize, sigma; MedianDenoiser). The program's other
+ * renderers are reported as SWR_ERR_UNSUPPORTED, unknown names as in getRenderer/getDenoiser. */
+enum { SWR_DENOISER_GAUSS = 1, SWR_DENOISER_MEDIAN = 2 };
+#define SWR_RT_MAX_DENOISERS 8
+typedef struct swr_rt_denoiser {
+  uint32_t kind;         /* SWR_DENOISER_* */
+  uint32_t kernel_size;  /* Gauss: kernelSize */
+  float sigma;           /* Gauss: sigma */
+  uint32_t reserved;
+} swr_rt_denoiser;
+typedef struct swr_rt_renderer_params {
+  uint32_t vision_jumps;
+  uint32_t spp;
+  uint32_t num_denoisers;
+  uint32_t reserved;
+  swr_rt_denoiser denoisers[SWR_RT_MAX_DENOISERS];
+} swr_rt_renderer_params;
+int swr_rt_renderer_load(const char* renderer_path, swr_rt_renderer_params* out);
+
+/* One frame of GraphicsEngine::render (src/graphic/graphics_engine.cpp:30-70): the PathTracer
+ * image, then each denoiser reading the previous image; rgba8_out receives the last image. */
+int swr_rt_render_frame(swr_scene* scene, const swr_camera* cam, const swr_rt_opts* opts,
+                        const swr_rt_denoiser* denoisers, uint32_t num_denoisers,
+                        uint8_t* rgba8_out, void* stream);
+
 /* Reference-style 8-bit quantisation (graphics_engine.cpp:90-95: clamp to [0,1], *255, truncate)
  * and P6 PPM writer (graphics_engine.cpp:32-40). Host memory. */
 int swr_quantize_rgb8(const float* rgb, uint32_t width, uint32_t height, uint8_t* out);

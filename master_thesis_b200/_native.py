@@ -115,6 +115,26 @@ class AdjointJob(ctypes.Structure):
 
 BATCH_NO_GRAPH = 1
 
+
+class RtOpts(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("vision_jumps", ctypes.c_uint32),
+                ("spp", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
+
+
+DENOISER_GAUSS = 1
+DENOISER_MEDIAN = 2
+RT_MAX_DENOISERS = 8
+
+
+class RtDenoiser(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("kernel_size", ctypes.c_uint32), ("sigma", ctypes.c_float),
+                ("reserved", ctypes.c_uint32)]
+
+
+class RtRendererParams(ctypes.Structure):
+    _fields_ = [("vision_jumps", ctypes.c_uint32), ("spp", ctypes.c_uint32), ("num_denoisers", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("denoisers", RtDenoiser * RT_MAX_DENOISERS)]
+
 P = ctypes.c_void_p
 U32 = ctypes.c_uint32
 U64 = ctypes.c_uint64
@@ -154,6 +174,14 @@ SIGNATURES = {
                                      ctypes.POINTER(ctypes.c_double)]),
     "swr_render_bdpt": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), ctypes.POINTER(BdptOpts), P, P, P]),
     "swr_renderer_load_params": (I, [ctypes.c_char_p, ctypes.POINTER(RendererParams)]),
+    "swr_rt_trace_closest": (I, [P, P, P, U64, P, P]),
+    "swr_rt_render": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RtOpts), P, P, P]),
+    "swr_rt_gauss_weights": (I, [U32, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+    "swr_rt_denoise_gauss": (I, [P, P, U32, U32, U32, ctypes.c_float, P]),
+    "swr_rt_denoise_median": (I, [P, P, U32, U32, P]),
+    "swr_rt_renderer_load": (I, [ctypes.c_char_p, ctypes.POINTER(RtRendererParams)]),
+    "swr_rt_render_frame": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RtOpts), ctypes.POINTER(RtDenoiser), U32,
+                                P, P]),
     "swr_quantize_rgb8": (I, [P, U32, U32, P]),
     "swr_write_ppm": (I, [ctypes.c_char_p, P, U32, U32]),
 }

@@ -1,5 +1,5 @@
-"""Builds the native library in-tree: master_thesis_b200/lib/libswr.so and the SoftwareRenderer
-command-line drop-in, both for sm_100a. Host C++ is compiled without floating-point contraction
+"""Builds the native library in-tree: master_thesis_b200/lib/libswr.so and the command-line
+drop-ins SoftwareRenderer and RayTrace (headless), for sm_100a. Host C++ is compiled without floating-point contraction
 because the world-space geometry and camera math must round exactly like the reference's build.
 
 Usage: python -m master_thesis_b200.build [--verbose]
@@ -26,8 +26,8 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp
 
 HOST_SRC = ["host/surface.cpp", "host/ref_bvh.cpp", "host/wide_bvh.cpp", "host/derive.cpp",
             "host/capi_host.cpp", "host/scene_pack.cpp"]
-CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu", "cuda/batch.cu", "cuda/build.cu"]
-CLI_SRC = "cli/swr_main.cpp"
+CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu", "cuda/batch.cu", "cuda/build.cu", "cuda/rt.cu"]
+CLI_SRC = {"SoftwareRenderer": "cli/swr_main.cpp", "RayTrace": "cli/rt_main.cpp"}
 
 
 def _run(cmd, verbose):
@@ -80,12 +80,13 @@ def build(verbose=False, ptxas_info=False):
     so = os.path.join(LIB, "libswr.so")
     if _stale(so, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", so] + objs + ["-lpthread"], verbose)
-    cli = os.path.join(LIB, "SoftwareRenderer")
-    cli_src = os.path.join(CSRC, CLI_SRC)
-    if os.path.exists(cli_src) and _stale(cli, [cli_src, so] + headers):
-        _run([CXX, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include", cli_src,
-              "-o", cli, "-L" + LIB, "-lswr", "-L/usr/local/cuda/lib64", "-lcudart",
-              "-Wl,-rpath,$ORIGIN:" + LIB + ":/usr/local/cuda/lib64"], verbose)
+    for name, rel in CLI_SRC.items():
+        cli = os.path.join(LIB, name)
+        cli_src = os.path.join(CSRC, rel)
+        if _stale(cli, [cli_src, so] + headers):
+            _run([CXX, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include",
+                  cli_src, "-o", cli, "-L" + LIB, "-lswr", "-L/usr/local/cuda/lib64", "-lcudart",
+                  "-Wl,-rpath,$ORIGIN:" + LIB + ":/usr/local/cuda/lib64"], verbose)
     return so, "\n".join(logs)
 
 

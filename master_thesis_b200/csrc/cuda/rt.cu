@@ -1,0 +1,478 @@
+// The Vulkan application's PathTracer and its two denoisers as CUDA kernels over the library's
+// scene (C ABI: swr_rt_render, swr_rt_render_frame, swr_rt_denoise_gauss, swr_rt_denoise_median).
+//
+// The reference runs these as ray tracing pipeline and compute shaders (RayTrace program,
+// src/main.cpp:58-76; res/shader/path_tracer_vision_raygen.rgen:8-60, denoise_gauss_comp.comp,
+// denoise_median_comp.comp). Here traceRay is the wide-BVH traversal with the ray-query hit rule
+// (swr_bvh.cuh, kRuleRayQuery) and the shader arithmetic is rt_shading.cuh.
+//
+//   k_rt_path    persistent: one lane per pixel runs the raygen shader for its pixel (the LCG
+//                state is per pixel and carried from sample to sample, so a pixel's samples are
+//                sequential). Every traceRay is the resumable Traversal, so a lane whose ray is
+//                finished shades it and issues the next ray while the other lanes of its warp go
+//                on traversing; a warp with `refill` idle lanes takes that many new pixels with
+//                one atomic.
+//   k_rt_gauss   one thread per pixel: the (2*off+1)^2 weighted taps in the shader's order.
+//   k_rt_median  one thread per pixel: per-channel median of the 3x3 neighbourhood.
+#include <algorithm>
+#include <cstring>
+
+#include "rt_shading.cuh"
+#include "swr_internal.cuh"
+
+namespace swr {
+int device_input(const float* p, size_t bytes, cudaStream_t stream, void** tmp, const float** dev);
+
+namespace {
+
+using swrx::f3;
+using swrx::mk;
+namespace rt = swrx::rt;
+
+constexpr int kBlock = 128;
+constexpr uint32_t kMiss = 0xFFFFFFFFu;
+constexpr uint32_t kMaxJumps = 1u << 16;
+constexpr uint32_t kMaxSpp = 1u << 24;
+constexpr uint32_t kMaxGauss = 19;  // GAUSS_ARRAY_MAX_SIZE 20 holds the odd sizes up to 19
+
+struct RtFrame {
+  float vi[16], pi[16];
+  uint32_t W, H, vj, spp;
+  uint32_t refill;
+  float scale;      // (2 * PI) / float(spp)
+  float* rgb;       // [W*H*3] finalColor, or null
+  uchar4* rgba;     // [W*H] the stored rgba8 pixel, or null
+};
+
+enum RtStage : uint32_t { kPrimary = 0, kSampleStart = 1, kJump = 2, kJumpResult = 3 };
+
+__device__ __forceinline__ void store_pixel(const RtFrame& F, uint32_t p, f3 c) {
+  if (F.rgb) {
+    F.rgb[3 * (size_t)p + 0] = c.x;
+    F.rgb[3 * (size_t)p + 1] = c.y;
+    F.rgb[3 * (size_t)p + 2] = c.z;
+  }
+  if (F.rgba) F.rgba[p] = make_uchar4(rt::unorm8(c.x), rt::unorm8(c.y), rt::unorm8(c.z), 0);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_rt_path(DevScene sc, RtFrame F, unsigned long long* __restrict__ cursor) {
+  __shared__ uint2 stack[swrx::kStackShared * kBlock];
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned long long total = (unsigned long long)F.W * F.H;
+  swrx::Traversal tr;
+  rt::Payload def, cur;
+  uint32_t pixel = 0, rng = 0, s = 0, i = 0, cull = 0, stage = kPrimary;
+  bool active = false, tracing = false, exhausted = false;
+  f3 o = mk(0, 0, 0), d = mk(0, 0, 0), sdir = mk(0, 0, 0), col = mk(0, 0, 0), fin = mk(0, 0, 0);
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(cursor, (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) exhausted = true;
+      if (!active) {
+        const unsigned long long g = base + __popc(idle & lt);
+        if (g < total) {
+          pixel = (uint32_t)g;
+          const uint32_t x = pixel % F.W, y = pixel / F.W;
+          rng = rt::lcg_init(x, y, 0u);
+          rt::vision_ray(F.vi, F.pi, x, y, F.W, F.H, o, d);
+          sdir = d;
+          cull = 0;
+          fin = mk(0.0f, 0.0f, 0.0f);
+          stage = kPrimary;
+          tr.init(o, d, stack + threadIdx.x, kBlock);
+          tracing = true;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+    if (tracing) {
+      if (!tr.step<false, false, swrx::kRuleRayQuery>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes,
+                                                       nullptr))
+        continue;
+      tracing = false;
+    }
+    const uint32_t hs = tr.hit.slot;
+    if (stage == kPrimary) {
+      // traceRay with back-face culling: up to four traces, each retry from the culled hit
+      if (hs == kMiss) {
+        store_pixel(F, pixel, mk(0.0f, 0.0f, 0.0f));
+        active = false;
+        continue;
+      }
+      const rt::Payload P = rt::hit_payload(sc.tris, sc.shade, sc.mats, hs, o, d);
+      if (swrx::vdot(P.n, d) > 0.0f && cull < 3) {
+        o = P.pos;
+        ++cull;
+        tr.init(o, d, stack + threadIdx.x, kBlock);
+        tracing = true;
+        continue;
+      }
+      if (P.light) {  // a light seen directly: its color * lightStrength, unscaled
+        store_pixel(F, pixel, P.color);
+        active = false;
+        continue;
+      }
+      def = P;
+      s = 0;
+      stage = kSampleStart;
+    } else {  // kJumpResult
+      if (hs == kMiss) {  // color = 0: the sample adds nothing
+        ++s;
+        stage = kSampleStart;
+      } else {
+        const rt::Payload P = rt::hit_payload(sc.tris, sc.shade, sc.mats, hs, o, d);
+        if (P.light && swrx::vdot(d, P.n) <= 0.0f) {
+          col = swrx::vmul(col, P.color);
+          fin = swrx::vadd(fin, col);
+          ++s;
+          stage = kSampleStart;
+        } else {
+          cur = P;
+          ++i;
+          stage = kJump;
+        }
+      }
+    }
+    // run the raygen loops until the next traceRay or the end of the pixel
+    while (!tracing) {
+      if (stage == kSampleStart) {
+        if (s >= F.spp) {
+          store_pixel(F, pixel, swrx::vscale(F.scale, fin));
+          active = false;
+          break;
+        }
+        cur = def;
+        d = sdir;
+        col = mk(1.0f, 1.0f, 1.0f);
+        i = 1;
+        stage = kJump;
+      }
+      if (i >= F.vj) {  // the jumps ran out before a light was hit
+        ++s;
+        stage = kSampleStart;
+        continue;
+      }
+      if (rt::handle_hit(cur, rng, o, d)) {
+        const float cs = swrx::vdot(d, cur.n);
+        col = swrx::vmul(col, mk(swrx::fmul(cur.color.x, cs), swrx::fmul(cur.color.y, cs),
+                                 swrx::fmul(cur.color.z, cs)));
+      }
+      tr.init(o, d, stack + threadIdx.x, kBlock);
+      tracing = true;
+      stage = kJumpResult;
+    }
+  }
+}
+
+struct GaussArgs {
+  float g[kMaxGauss + 1];
+  int off;
+  uint32_t W, H;
+};
+
+// imageLoad of an rgba8 texel: byte / 255 as an IEEE float quotient
+__device__ __forceinline__ float unorm_load(const float* lut, uint32_t b) { return lut[b]; }
+
+__global__ void __launch_bounds__(256) k_rt_gauss(const uchar4* __restrict__ in, uchar4* __restrict__ out,
+                                                  GaussArgs A) {
+  __shared__ float lut[256];
+  for (uint32_t k = threadIdx.y * blockDim.x + threadIdx.x; k < 256; k += blockDim.x * blockDim.y)
+    lut[k] = __fdiv_rn((float)k, 255.0f);
+  __syncthreads();
+  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (x >= (int)A.W || y >= (int)A.H) return;
+  float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (int dx = -A.off; dx <= A.off; ++dx) {
+    const int px = x + dx;
+    if (px < 0 || px >= (int)A.W) continue;
+    const float gx = A.g[dx + A.off];
+    for (int dy = -A.off; dy <= A.off; ++dy) {
+      const int py = y + dy;
+      if (py < 0 || py >= (int)A.H) continue;
+      const float gy = A.g[dy + A.off];
+      const uchar4 v = __ldg(in + (size_t)py * A.W + px);
+      c.x = __fadd_rn(c.x, __fmul_rn(__fmul_rn(unorm_load(lut, v.x), gx), gy));
+      c.y = __fadd_rn(c.y, __fmul_rn(__fmul_rn(unorm_load(lut, v.y), gx), gy));
+      c.z = __fadd_rn(c.z, __fmul_rn(__fmul_rn(unorm_load(lut, v.z), gx), gy));
+      c.w = __fadd_rn(c.w, __fmul_rn(__fmul_rn(unorm_load(lut, v.w), gx), gy));
+    }
+  }
+  out[(size_t)y * A.W + x] =
+      make_uchar4(rt::unorm8(c.x), rt::unorm8(c.y), rt::unorm8(c.z), rt::unorm8(c.w));
+}
+
+// Median of nine per byte lane: sort each row of three, then the median of (largest row
+// minimum, median of the row medians, smallest row maximum). Selecting among the loaded texels
+// and storing the selected one back is exact, so the work stays on the packed bytes.
+__device__ __forceinline__ void ex(uint32_t& a, uint32_t& b) {
+  const uint32_t lo = __vminu4(a, b);
+  b = __vmaxu4(a, b);
+  a = lo;
+}
+__device__ __forceinline__ uint32_t med3(uint32_t a, uint32_t b, uint32_t c) {
+  return __vmaxu4(__vminu4(a, b), __vminu4(__vmaxu4(a, b), c));
+}
+
+__global__ void __launch_bounds__(256) k_rt_median(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                   uint32_t W, uint32_t H) {
+  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (x >= (int)W || y >= (int)H) return;
+  uint32_t v[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int px = x + k - 1, py = y + r - 1;
+      // texels outside the image are undefined in the shader; they count as 0 here
+      v[3 * r + k] = (px >= 0 && px < (int)W && py >= 0 && py < (int)H) ? __ldg(in + (size_t)py * W + px) : 0u;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    ex(v[3 * r], v[3 * r + 1]);
+    ex(v[3 * r + 1], v[3 * r + 2]);
+    ex(v[3 * r], v[3 * r + 1]);
+  }
+  const uint32_t lo = __vmaxu4(__vmaxu4(v[0], v[3]), v[6]);
+  const uint32_t hi = __vminu4(__vminu4(v[2], v[5]), v[8]);
+  const uint32_t mid = med3(v[1], v[4], v[7]);
+  out[(size_t)y * W + x] = med3(lo, mid, hi);
+}
+
+int check_image(uint32_t W, uint32_t H) {
+  if (W == 0 || H == 0) return set_error(SWR_ERR_INVALID, "swr: image size must be positive");
+  if ((uint64_t)W * H > (1ull << 31)) return set_error(SWR_ERR_INVALID, "swr: image too large");
+  return SWR_OK;
+}
+
+// Device view of a caller buffer: the buffer itself, or a stream-ordered temporary when it is host
+// memory (copied in when `in`, copied back by finish()).
+struct Staged {
+  void* user = nullptr;
+  void* dev = nullptr;
+  size_t bytes = 0;
+  bool host = false;
+};
+
+int stage(void* user, size_t bytes, bool in, cudaStream_t stream, Staged& st) {
+  st.user = user;
+  st.bytes = bytes;
+  st.dev = user;
+  st.host = user && is_host_pointer(user);
+  if (!st.host) return SWR_OK;
+  SWR_CUDA(cudaMallocAsync(&st.dev, bytes, stream));
+  if (in) SWR_CUDA(cudaMemcpyAsync(st.dev, user, bytes, cudaMemcpyHostToDevice, stream));
+  return SWR_OK;
+}
+
+void release(Staged& st, cudaStream_t stream) {
+  if (st.host && st.dev) cudaFreeAsync(st.dev, stream);
+  st.dev = nullptr;
+}
+
+int copy_back(Staged& st, cudaStream_t stream) {
+  if (st.host) SWR_CUDA(cudaMemcpyAsync(st.user, st.dev, st.bytes, cudaMemcpyDeviceToHost, stream));
+  return SWR_OK;
+}
+
+int render_impl(swr_scene* s, const swr_camera* cam, const swr_rt_opts* opts, float* rgb, uchar4* rgba,
+                cudaStream_t stream) {
+  RtFrame F;
+  std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
+  std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
+  F.W = opts->width;
+  F.H = opts->height;
+  F.vj = opts->vision_jumps;
+  F.spp = opts->spp;
+  F.refill = opts->refill ? opts->refill : 8u;
+  F.scale = (2.0f * rt::kPi) / (float)opts->spp;
+  F.rgb = rgb;
+  F.rgba = rgba;
+  unsigned long long* cursor = (unsigned long long*)s->d_scratch;
+  SWR_CUDA(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), stream));
+  int per_sm = 0;
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rt_path, kBlock, 0));
+  per_sm = std::max(per_sm, 1);
+  const uint64_t npix = (uint64_t)F.W * F.H;
+  const uint64_t need = (npix + kBlock - 1) / kBlock;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)s->num_sms * per_sm, need));
+  k_rt_path<<<grid, kBlock, 0, stream>>>(s->dev, F, cursor);
+  SWR_CUDA(cudaGetLastError());
+  return SWR_OK;
+}
+
+int check_render_args(const swr_scene* s, const swr_camera* cam, const swr_rt_opts* opts) {
+  if (!s || !cam || !opts) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  int rc = check_image(opts->width, opts->height);
+  if (rc) return rc;
+  if (opts->spp == 0 || opts->spp > kMaxSpp)
+    return set_error(SWR_ERR_INVALID, "swr: visionRayPerPixelCount must be in 1..2^24");
+  if (opts->vision_jumps > kMaxJumps) return set_error(SWR_ERR_INVALID, "swr: visionJumpCount above 65536");
+  if (opts->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  return SWR_OK;
+}
+
+int gauss_args(uint32_t W, uint32_t H, uint32_t k, float sigma, GaussArgs& A) {
+  std::memset(&A, 0, sizeof(A));
+  int rc = swr_rt_gauss_weights(k, sigma, A.g);
+  if (rc) return rc;
+  A.off = (int)(k / 2);
+  A.W = W;
+  A.H = H;
+  return SWR_OK;
+}
+
+void launch_gauss(const uchar4* in, uchar4* out, const GaussArgs& A, cudaStream_t stream) {
+  const dim3 blk(32, 8), grd((A.W + 31) / 32, (A.H + 7) / 8);
+  k_rt_gauss<<<grd, blk, 0, stream>>>(in, out, A);
+}
+
+void launch_median(const uchar4* in, uchar4* out, uint32_t W, uint32_t H, cudaStream_t stream) {
+  const dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
+  k_rt_median<<<grd, blk, 0, stream>>>((const uint32_t*)in, (uint32_t*)out, W, H);
+}
+
+int check_denoiser(const swr_rt_denoiser& dn) {
+  if (dn.kind == SWR_DENOISER_MEDIAN) return SWR_OK;
+  if (dn.kind != SWR_DENOISER_GAUSS) return set_error(SWR_ERR_INVALID, "swr: unknown denoiser kind");
+  float g[kMaxGauss + 1];
+  return swr_rt_gauss_weights(dn.kernel_size, dn.sigma, g);
+}
+
+}  // namespace
+}  // namespace swr
+
+using swr::set_error;
+
+extern "C" {
+
+int swr_rt_render(swr_scene* s, const swr_camera* cam, const swr_rt_opts* opts, float* rgb_out,
+                  uint8_t* rgba8_out, void* stream_) {
+  int rc = swr::check_render_args(s, cam, opts);
+  if (rc) return rc;
+  if (!rgb_out && !rgba8_out) return set_error(SWR_ERR_INVALID, "swr: no output buffer");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  const size_t npix = (size_t)opts->width * opts->height;
+  swr::Staged a, b;
+  if ((rc = swr::stage(rgb_out, npix * 12, false, stream, a))) return rc;
+  if ((rc = swr::stage(rgba8_out, npix * 4, false, stream, b))) {
+    swr::release(a, stream);
+    return rc;
+  }
+  rc = swr::render_impl(s, cam, opts, (float*)a.dev, (uchar4*)b.dev, stream);
+  if (!rc) rc = swr::copy_back(a, stream);
+  if (!rc) rc = swr::copy_back(b, stream);
+  swr::release(a, stream);
+  swr::release(b, stream);
+  if (!rc && (a.host || b.host)) SWR_CUDA(cudaStreamSynchronize(stream));
+  return rc;
+}
+
+int swr_rt_denoise_gauss(const uint8_t* in, uint8_t* out, uint32_t W, uint32_t H, uint32_t kernel_size,
+                         float sigma, void* stream_) {
+  if (!in || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (in == out) return set_error(SWR_ERR_INVALID, "swr: the denoisers read and write separate images");
+  int rc = swr::check_image(W, H);
+  if (rc) return rc;
+  swr::GaussArgs A;
+  if ((rc = swr::gauss_args(W, H, kernel_size, sigma, A))) return rc;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  const size_t bytes = (size_t)W * H * 4;
+  swr::Staged si, so;
+  if ((rc = swr::stage((void*)in, bytes, true, stream, si))) return rc;
+  if ((rc = swr::stage(out, bytes, false, stream, so))) {
+    swr::release(si, stream);
+    return rc;
+  }
+  swr::launch_gauss((const uchar4*)si.dev, (uchar4*)so.dev, A, stream);
+  cudaError_t e = cudaGetLastError();
+  rc = e != cudaSuccess ? swr::cuda_fail(e, "k_rt_gauss") : swr::copy_back(so, stream);
+  swr::release(si, stream);
+  swr::release(so, stream);
+  if (!rc && (si.host || so.host)) SWR_CUDA(cudaStreamSynchronize(stream));
+  return rc;
+}
+
+int swr_rt_denoise_median(const uint8_t* in, uint8_t* out, uint32_t W, uint32_t H, void* stream_) {
+  if (!in || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (in == out) return set_error(SWR_ERR_INVALID, "swr: the denoisers read and write separate images");
+  int rc = swr::check_image(W, H);
+  if (rc) return rc;
+  if (((uintptr_t)in | (uintptr_t)out) & 3) return set_error(SWR_ERR_INVALID, "swr: images must be 4-byte aligned");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  const size_t bytes = (size_t)W * H * 4;
+  swr::Staged si, so;
+  if ((rc = swr::stage((void*)in, bytes, true, stream, si))) return rc;
+  if ((rc = swr::stage(out, bytes, false, stream, so))) {
+    swr::release(si, stream);
+    return rc;
+  }
+  swr::launch_median((const uchar4*)si.dev, (uchar4*)so.dev, W, H, stream);
+  cudaError_t e = cudaGetLastError();
+  rc = e != cudaSuccess ? swr::cuda_fail(e, "k_rt_median") : swr::copy_back(so, stream);
+  swr::release(si, stream);
+  swr::release(so, stream);
+  if (!rc && (si.host || so.host)) SWR_CUDA(cudaStreamSynchronize(stream));
+  return rc;
+}
+
+int swr_rt_render_frame(swr_scene* s, const swr_camera* cam, const swr_rt_opts* opts,
+                        const swr_rt_denoiser* denoisers, uint32_t num_denoisers, uint8_t* rgba8_out,
+                        void* stream_) {
+  int rc = swr::check_render_args(s, cam, opts);
+  if (rc) return rc;
+  if (!rgba8_out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (num_denoisers > SWR_RT_MAX_DENOISERS) return set_error(SWR_ERR_INVALID, "swr: too many denoisers");
+  if (num_denoisers && !denoisers) return set_error(SWR_ERR_INVALID, "swr: null denoiser list");
+  for (uint32_t k = 0; k < num_denoisers; ++k)
+    if ((rc = swr::check_denoiser(denoisers[k]))) return rc;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  SWR_CUDA(cudaSetDevice(s->device));
+  const uint32_t W = opts->width, H = opts->height;
+  const size_t bytes = (size_t)W * H * 4;
+  swr::Staged so;
+  if ((rc = swr::stage(rgba8_out, bytes, false, stream, so))) return rc;
+  // ping-pong images: the renderer writes the first denoiser's input, the last denoiser the output
+  void* tmp[2] = {nullptr, nullptr};
+  const int ntmp = num_denoisers == 0 ? 0 : (num_denoisers == 1 ? 1 : 2);
+  for (int k = 0; k < ntmp && !rc; ++k) {
+    cudaError_t e = cudaMallocAsync(&tmp[k], bytes, stream);
+    if (e != cudaSuccess) rc = swr::cuda_fail(e, "cudaMallocAsync");
+  }
+  uchar4* cur = num_denoisers ? (uchar4*)tmp[0] : (uchar4*)so.dev;
+  if (!rc) rc = swr::render_impl(s, cam, opts, nullptr, cur, stream);
+  for (uint32_t k = 0; k < num_denoisers && !rc; ++k) {
+    uchar4* dst = (k + 1 == num_denoisers) ? (uchar4*)so.dev : (uchar4*)tmp[(k + 1) & 1];
+    if (denoisers[k].kind == SWR_DENOISER_GAUSS) {
+      swr::GaussArgs A;
+      rc = swr::gauss_args(W, H, denoisers[k].kernel_size, denoisers[k].sigma, A);
+      if (!rc) swr::launch_gauss(cur, dst, A, stream);
+    } else {
+      swr::launch_median(cur, dst, W, H, stream);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (!rc && e != cudaSuccess) rc = swr::cuda_fail(e, "denoiser launch");
+    cur = dst;
+  }
+  if (!rc) rc = swr::copy_back(so, stream);
+  for (void* p : tmp)
+    if (p) cudaFreeAsync(p, stream);
+  swr::release(so, stream);
+  if (!rc && so.host) SWR_CUDA(cudaStreamSynchronize(stream));
+  return rc;
+}
+
+}  // extern "C"

@@ -147,7 +147,7 @@ int device_input(const float* p, size_t bytes, cudaStream_t stream, void** tmp, 
 // with one atomic on the cursor, so lanes stay busy while long rays are still walking the tree.
 constexpr unsigned kRefill = 8;
 
-template <bool kStats>
+template <bool kStats, int kRule = swrx::kRuleReference>
 __global__ void __launch_bounds__(kTraceBlock)
     k_trace_closest(DevScene sc, const float4* __restrict__ ro, const float4* __restrict__ rd,
                     uint64_t n, uint4* __restrict__ out, uint2* __restrict__ counts,
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kTraceBlock)
       if (exhausted) break;
       continue;
     }
-    if (active && tr.template step<kStats>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, &st)) {
+    if (active && tr.template step<kStats, false, kRule>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, &st)) {
       const swrx::Hit h = tr.result(sc.tris);
       out[ray] = make_uint4(h.id, h.obj, __float_as_uint(h.d2), __float_as_uint(h.t));
       if (kStats) counts[ray] = make_uint2(st.nodes, st.tris);
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kTraceBlock)
 }
 
 int trace_impl(swr_scene* s, const float* ray_o, const float* ray_d, uint64_t n, swr_hit* out,
-               uint32_t* counts, void* stream_) {
+               uint32_t* counts, void* stream_, int rule = swrx::kRuleReference) {
   if (!s || !ray_o || !ray_d || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
   if (n == 0) return SWR_OK;
   cudaStream_t stream = (cudaStream_t)stream_;
@@ -233,14 +233,21 @@ int trace_impl(swr_scene* s, const float* ray_o, const float* ray_d, uint64_t n,
   unsigned long long* cursor = (unsigned long long*)s->d_scratch;
   SWR_CUDA(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), stream));
   int per_sm = 0;
-  if (counts)
+  const bool rq = rule == swrx::kRuleRayQuery;
+  if (rq)
+    SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_trace_closest<false, swrx::kRuleRayQuery>, kTraceBlock, 0));
+  else if (counts)
     SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_closest<true>, kTraceBlock, 0));
   else
     SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_closest<false>, kTraceBlock, 0));
   per_sm = std::max(per_sm, 1);
   const uint64_t max_blocks = (n + kTraceBlock - 1) / kTraceBlock;
   const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)s->num_sms * per_sm, max_blocks);
-  if (counts)
+  if (rq)
+    k_trace_closest<false, swrx::kRuleRayQuery>
+        <<<grid, kTraceBlock, 0, stream>>>(s->dev, dro, drd, n, dout, nullptr, cursor);
+  else if (counts)
     k_trace_closest<true><<<grid, kTraceBlock, 0, stream>>>(s->dev, dro, drd, n, dout, dcnt, cursor);
   else
     k_trace_closest<false><<<grid, kTraceBlock, 0, stream>>>(s->dev, dro, drd, n, dout, nullptr, cursor);
@@ -386,6 +393,11 @@ int swr_scene_set_emission(swr_scene* s, const float* emission, void* stream_) {
 int swr_trace_closest(swr_scene* s, const float* ray_o, const float* ray_d, uint64_t n, swr_hit* out,
                       void* stream) {
   return swr::trace_impl(s, ray_o, ray_d, n, out, nullptr, stream);
+}
+
+int swr_rt_trace_closest(swr_scene* s, const float* ray_o, const float* ray_d, uint64_t n,
+                         swr_hit* out, void* stream) {
+  return swr::trace_impl(s, ray_o, ray_d, n, out, nullptr, stream, swrx::kRuleRayQuery);
 }
 
 int swr_trace_closest_stats(swr_scene* s, const float* ray_o, const float* ray_d, uint64_t n,

@@ -1,5 +1,6 @@
 // Host-side half of the C ABI: error reporting, the file surface, derived triangle data and
 // image output. No CUDA here.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -167,6 +168,52 @@ int swr_renderer_load_params(const char* renderer_path, swr_renderer_params* out
   } catch (const std::exception& e) {
     return set_error(SWR_ERR_PARSE, std::string("swr: ") + e.what());
   }
+}
+
+int swr_rt_renderer_load(const char* renderer_path, swr_rt_renderer_params* out) {
+  if (!renderer_path || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  try {
+    swr::RtRendererParams r = swr::load_rt_renderer_file(renderer_path);
+    if (r.denoisers.size() > SWR_RT_MAX_DENOISERS)
+      return set_error(SWR_ERR_UNSUPPORTED, "swr: more than 8 denoisers");
+    std::memset(out, 0, sizeof(*out));
+    out->vision_jumps = r.vision_jump_count;
+    out->spp = r.vision_rays_per_pixel;
+    out->num_denoisers = (uint32_t)r.denoisers.size();
+    for (size_t k = 0; k < r.denoisers.size(); ++k) {
+      const bool gauss = r.denoisers[k].name == "GaussDenoiser";
+      out->denoisers[k].kind = gauss ? SWR_DENOISER_GAUSS : SWR_DENOISER_MEDIAN;
+      out->denoisers[k].kernel_size = r.denoisers[k].kernel_size;
+      out->denoisers[k].sigma = r.denoisers[k].sigma;
+    }
+    return SWR_OK;
+  } catch (const swr::SurfaceError& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SWR_ERR_PARSE, std::string("swr: ") + e.what());
+  }
+}
+
+// GaussDenoiser::updateUniforms (gauss_denoiser.cpp:31-46), in float with the same order of
+// operations; exp is evaluated in double and rounded.
+int swr_rt_gauss_weights(uint32_t k, float sigma, float* out) {
+  if (!out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (k == 0 || k > 19 || (k & 1u) == 0)
+    return set_error(SWR_ERR_INVALID, "swr: GaussDenoiser kernelSize must be odd and in 1..19");
+  if (!(sigma > 0.0f) || !std::isfinite(sigma))
+    return set_error(SWR_ERR_INVALID, "swr: GaussDenoiser sigma must be positive");
+  float sum = 0.0f;
+  for (uint32_t i = 0; i < k; ++i) {
+    float a = (float)i - ((float)k - 1.0f);
+    a = a * a;
+    const float b = 2.0f * sigma * sigma;
+    const float r = (float)std::exp((double)(-a / b));
+    out[i] = r;
+    sum += r;
+  }
+  sum = 1.0f / sum;
+  for (uint32_t i = 0; i < k; ++i) out[i] *= sum;
+  return SWR_OK;
 }
 
 int swr_scene_derive(const swr_scene_desc* d, float* tri_e0, float* tri_e1, float* tri_den,

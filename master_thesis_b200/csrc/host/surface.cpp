@@ -23,6 +23,7 @@ namespace swr {
 static constexpr int kErrIO = 1;
 static constexpr int kErrParse = 2;
 static constexpr int kErrInvalid = 6;
+static constexpr int kErrUnsupported = 7;
 
 // ------------------------------------------------------------------------------------------
 // InputEntry
@@ -592,6 +593,39 @@ RendererParams load_renderer_file(const std::string& path, bool bdpt_keys) {
     r.light_jump_count = entries[0].get_uint("lightJumpCount");
     r.max_depth = entries[0].get_uint("maxDepth");
     r.rays_per_pixel = entries[0].get_uint("raysPerPixel");
+  }
+  return r;
+}
+
+RtRendererParams load_rt_renderer_file(const std::string& path) {
+  auto entries = parse_input_file(path);
+  if (entries.empty()) throw SurfaceError(kErrParse, "Renderer", "no entry in \"" + path + "\"");
+  RtRendererParams r;
+  r.name = entries[0].name;
+  // getRenderer (src/main.cpp:58-71)
+  static const char* kOthers[] = {"PhotonMapper", "BidirectionalPathTracer", "ShadowTracer",
+                                  "Majercik2019", "Majercik2022", "Majercik2022BidirectionalPathTracer",
+                                  "Bitterli2020", "Bitterli2020BidirectionalPathTracer", "MetaRenderer",
+                                  "PhongShader"};
+  if (r.name != "PathTracer") {
+    for (const char* n : kOthers)
+      if (r.name == n)
+        throw SurfaceError(kErrUnsupported, "getRenderer",
+                           r.name + " is a renderer of the RayTrace program that this library does not restate");
+    throw SurfaceError(kErrInvalid, "getRenderer not found", r.name);
+  }
+  r.vision_jump_count = entries[0].get_uint("visionJumpCount");
+  r.vision_rays_per_pixel = entries[0].get_uint("visionRayPerPixelCount");
+  for (size_t i = 1; i < entries.size(); ++i) {  // getDenoiser (src/main.cpp:73-77)
+    RtDenoiserParams d;
+    d.name = entries[i].name;
+    if (d.name == "GaussDenoiser") {
+      d.kernel_size = entries[i].get_uint("kernelSize");
+      d.sigma = entries[i].get_float("sigma");
+    } else if (d.name != "MedianDenoiser") {
+      throw SurfaceError(kErrInvalid, "getDenoiser not found", d.name);
+    }
+    r.denoisers.push_back(d);
   }
   return r;
 }

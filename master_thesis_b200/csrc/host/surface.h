@@ -178,4 +178,21 @@ struct RendererParams {
 // Renderer file; the bidirectional tracer's keys are read (and required) only with bdpt_keys.
 RendererParams load_renderer_file(const std::string& path, bool bdpt_keys = true);
 
+// Renderer file of the RayTrace program (src/main.cpp:153-168): the renderer entry, then the
+// denoiser entries in file order (gauss_denoiser.cpp:51-54; MedianDenoiser has no keys).
+struct RtDenoiserParams {
+  std::string name;
+  unsigned kernel_size = 0;
+  float sigma = 0.0f;
+};
+struct RtRendererParams {
+  std::string name;
+  unsigned vision_jump_count = 0;
+  unsigned vision_rays_per_pixel = 0;
+  std::vector<RtDenoiserParams> denoisers;
+};
+// Accepts the PathTracer (path_tracer.cpp:30-33); the program's other renderers raise
+// SWR_ERR_UNSUPPORTED, unknown renderer or denoiser names the getRenderer / getDenoiser errors.
+RtRendererParams load_rt_renderer_file(const std::string& path);
+
 }  // namespace swr

@@ -40,6 +40,18 @@ constexpr int kStackShared = 8;   // entries per thread kept in shared memory
 constexpr int kStackTotal = 64;   // maximum traversal stack depth (checked at build time)
 constexpr float kPruneSlack = 1.0f + 1.0f / 1024.0f;
 
+// Hit rules of Traversal::step.
+//   kRuleReference  the software renderer's: smallest (squared distance, visit rank), accepted only
+//                   when the reference's slab tests pass (see above).
+//   kRuleRayQuery   the closest hit that the Vulkan renderers ask the ray tracing pipeline for
+//                   (traceRay, v1.glsl:148-161: opaque geometry, tmin 0.001, tmax 10000): the
+//                   smallest t in [kRqTmin, kRqTmax], ties to the lower triangle id, with the same
+//                   Moller-Trumbore arithmetic; hit.rank then holds the triangle id and hit.d2 is
+//                   left unset.
+enum HitRule : int { kRuleReference = 0, kRuleRayQuery = 1 };
+constexpr float kRqTmin = 0.001f;
+constexpr float kRqTmax = 10000.0f;
+
 struct Hit {
   uint32_t slot;   // index into the triangle records, 0xFFFFFFFF on a miss
   uint32_t id;     // global triangle id
@@ -221,7 +233,7 @@ struct Traversal {
   // stack, so the warp runs one phase at a time. Without it a lane with pending triangles tests
   // one of them per step and a lane without expands a node. (The visit order never changes the
   // result: the closest hit is an arg-min over the same candidates.)
-  template <bool kStats, bool kPostpone = false>
+  template <bool kStats, bool kPostpone = false, int kRule = kRuleReference>
   SWR_HD bool step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
                    const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
                    TraceStats* stats) {
@@ -310,6 +322,16 @@ struct Traversal {
       const float4 a = ldg4(tp + 0), b = ldg4(tp + 1), c = ldg4(tp + 2);
       float t, d2;
       if (!ref_intersect(o, d, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y), mk(b.z, b.w, c.x), t, d2)) break;
+      if (kRule == kRuleRayQuery) {
+        if (!(t >= kRqTmin && t <= kRqTmax)) break;
+        const uint32_t id = f2bits(c.y);
+        if (!(t < hit.t || (t == hit.t && id < hit.rank))) break;
+        hit.slot = s;
+        hit.rank = id;
+        hit.t = t;
+        tprune = t * kPruneSlack;
+        break;
+      }
       const uint32_t rank = f2bits(c.z);
       if (!(d2 < hit.d2 || (d2 == hit.d2 && rank < hit.rank))) break;
       const uint32_t obj = f2bits(c.w);
@@ -340,14 +362,14 @@ struct Traversal {
 
 // Closest hit of ray (o, d), run to completion. obj_boxes/tri_boxes hold the reference's own
 // boxes (lo.xyz, hi.xyz) per object and per triangle record. Returns false on a miss.
-template <bool kStats, bool kPostpone = false>
+template <bool kStats, bool kPostpone = false, int kRule = kRuleReference>
 SWR_HD bool trace_closest(const float4* __restrict__ nodes, const float4* __restrict__ tris,
                           const float* __restrict__ tri_boxes, const float* __restrict__ obj_boxes,
                           f3 o, f3 d, uint2* stack_shared, int stack_stride, Hit& hit,
                           TraceStats* stats) {
   Traversal tr;
   tr.init(o, d, stack_shared, stack_stride);
-  while (!tr.template step<kStats, kPostpone>(nodes, tris, tri_boxes, obj_boxes, stats)) {
+  while (!tr.template step<kStats, kPostpone, kRule>(nodes, tris, tri_boxes, obj_boxes, stats)) {
   }
   hit = tr.result(tris);
   return hit.slot != 0xFFFFFFFFu;

@@ -137,6 +137,17 @@ SWR_HD bool ref_intersect(f3 o, f3 d, f3 v0, f3 e0, f3 e1, float& t_out, float& 
   return true;
 }
 
+// The barycentric weights (u of v1, v of v2) that ref_intersect computes for the same ray and
+// triangle, with the same operations.
+SWR_HD void ref_uv(f3 o, f3 d, f3 v0, f3 e0, f3 e1, float& u, float& v) {
+  f3 h = vcross(d, e1);
+  float f = frcp(vdot(e0, h));
+  f3 s = vsub(o, v0);
+  u = fmul(f, vdot(s, h));
+  f3 q = vcross(s, e0);
+  v = fmul(f, vdot(d, q));
+}
+
 // hit position as Triangle::rayIntersects computes it
 SWR_HD f3 hit_point(f3 o, f3 d, float t) { return vadd(o, vscale(t, d)); }
 

@@ -29,6 +29,12 @@ def _lib():
     lib.swo_render_bdpt.argtypes = [P, P] + [ctypes.c_uint32] * 6 + [ctypes.c_uint64] + [ctypes.c_uint32] * 2 + \
         [P, P, ctypes.c_int]
     lib.swo_render_bdpt.restype = ctypes.c_int
+    lib.swo_rt_render.argtypes = [P, P] + [ctypes.c_uint32] * 6 + [P, P, ctypes.c_int]
+    lib.swo_rt_trace.argtypes = [P, P, P, ctypes.c_uint64, P, P, ctypes.c_int]
+    lib.swo_rt_gauss_weights.argtypes = [ctypes.c_uint32, ctypes.c_float, P]
+    lib.swo_rt_gauss_weights.restype = ctypes.c_int
+    lib.swo_rt_denoise_gauss.argtypes = [P, P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, P]
+    lib.swo_rt_denoise_median.argtypes = [P, P, ctypes.c_uint32, ctypes.c_uint32]
     return lib
 
 
@@ -184,3 +190,51 @@ def adjoint_physical64(sc, cam, W, H, spp, depth, seed, dl_dimg, rr_depth=0, rr_
     lib().swo_adjoint_physical64(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, depth, seed, rr_depth,
                                  float(np.float32(rr_q)), _p(dl), _p(ga), _p(ge), threads or _threads())
     return ga, ge
+
+
+def rt_render(sc, cam, W, H, spp, vision_jumps, p0=0, p1=None, threads=None):
+    """The RayTrace program's PathTracer for pixels [p0, p1): finalColor [n, 3] and the stored
+    rgba8 texels [n, 4]."""
+    p1 = W * H if p1 is None else p1
+    n = p1 - p0
+    rgb = np.empty((n, 3), np.float32)
+    rgba = np.empty((n, 4), np.uint8)
+    lib().swo_rt_render(ctypes.byref(sc._s), ctypes.byref(cam), W, H, vision_jumps, spp, p0, p1, _p(rgb), _p(rgba),
+                        threads or _threads())
+    return rgb, rgba
+
+
+def rt_trace(sc, ro, rd, threads=None):
+    """traceRay's closest hit per ray: (triangle id or 0xFFFFFFFF, t)."""
+    ro = np.ascontiguousarray(ro, dtype=np.float32).reshape(-1, 4)
+    rd = np.ascontiguousarray(rd, dtype=np.float32).reshape(-1, 4)
+    n = ro.shape[0]
+    tri = np.empty(n, np.uint32)
+    t = np.empty(n, np.float32)
+    lib().swo_rt_trace(ctypes.byref(sc._s), _p(ro), _p(rd), n, _p(tri), _p(t), threads or _threads())
+    return tri, t
+
+
+def rt_gauss_weights(kernel_size, sigma):
+    out = np.zeros(20, np.float32)
+    if lib().swo_rt_gauss_weights(kernel_size, float(np.float32(sigma)), _p(out)) != 0:
+        raise ValueError("GaussDenoiser kernel size must be odd and in 1..19")
+    return out[:kernel_size]
+
+
+def rt_denoise_gauss(img, kernel_size, sigma):
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape[:2]
+    g = np.zeros(20, np.float32)
+    g[:kernel_size] = rt_gauss_weights(kernel_size, sigma)
+    out = np.empty_like(img)
+    lib().swo_rt_denoise_gauss(_p(img), _p(out), w, h, kernel_size, _p(g))
+    return out
+
+
+def rt_denoise_median(img):
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape[:2]
+    out = np.empty_like(img)
+    lib().swo_rt_denoise_median(_p(img), _p(out), w, h)
+    return out

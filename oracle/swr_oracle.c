@@ -871,3 +871,304 @@ void swo_adjoint_physical64(const swo_scene* s, const swo_camera* cam, uint32_t 
   }
   pthread_mutex_destroy(&mu);
 }
+
+/* =============================================================================================
+ * The Vulkan application's PathTracer and denoisers (RayTrace program), restated on the CPU as
+ * the checker of the library's CUDA restatement. Sources restated:
+ *   random numbers   res/shader/helper.glsl:11-41 (LCG a=6237 c=10697 m=21023, randomNormal)
+ *   customRefract    res/shader/helper.glsl:43-57, GLSL reflect/refract
+ *   camera ray       res/shader/v1.glsl:130-142 (getVisionRay)
+ *   traceRay         res/shader/v1.glsl:148-161 (tmin 0.001, tmax 10000, back-face retries)
+ *   handleHit        res/shader/v1.glsl:163-188
+ *   hit payload      res/shader/v1_closesthit.rchit:9-41, v1_miss.rmiss
+ *   raygen           res/shader/path_tracer_vision_raygen.rgen:8-60
+ *   denoisers        res/shader/denoise_gauss_comp.comp, denoise_median_comp.comp,
+ *                    src/graphic/denoiser/gauss_denoiser.cpp:31-46 (weights)
+ * GLSL leaves the precision of division, sqrt, sin/cos/acos and normalize to the implementation;
+ * the choice fixed here (and by the library) is: IEEE float division and sqrt, the double
+ * sin/cos/acos of the widened argument rounded to float, normalize(v) = v / sqrt(dot(v, v)),
+ * no fused multiply-adds. The closest hit uses the Moller-Trumbore arithmetic above with t in
+ * [0.001, 10000] and ties to the lower triangle id, found by testing every triangle. Parity with
+ * the shaders on a GPU ray tracing pipeline cannot be checked here (no graphics stack), so this
+ * restatement is pinned only by its own known-answer tests. */
+
+static const float RT_PI = 3.1415926538f;
+
+static uint32_t rt_closest(const swo_scene* s, v3f o, v3f d, float* t_out) {
+  float bt = INFINITY;
+  uint32_t bi = 0xFFFFFFFFu, k;
+  for (k = 0; k < s->ntri; ++k) {
+    float t, d2;
+    if (!ref_intersect(o, d, ld3(s->v0 + 3 * (size_t)k), ld3(s->e0 + 3 * (size_t)k),
+                       ld3(s->e1 + 3 * (size_t)k), &t, &d2))
+      continue;
+    if (!(t >= 0.001f && t <= 10000.0f)) continue;
+    if (t < bt) { /* increasing ids: a tie keeps the lower id */
+      bt = t;
+      bi = k;
+    }
+  }
+  *t_out = bt;
+  return bi;
+}
+
+static uint32_t rt_lcg_init(uint32_t x, uint32_t y) { return (625u + x * 7444u + y * 1045u) % 21023u; }
+static float rt_rand(uint32_t* st) {
+  *st = (6237u * *st + 10697u) % 21023u;
+  return (float)*st / 21023.0f;
+}
+static v3f rt_normalize(v3f v) {
+  float l = sqrtf(dot(v, v));
+  return mk(v.x / l, v.y / l, v.z / l);
+}
+static v3f rt_reflect(v3f I, v3f N) {
+  float s = 2.0f * dot(N, I);
+  return mk(I.x - s * N.x, I.y - s * N.y, I.z - s * N.z);
+}
+static v3f rt_refract(v3f I, v3f N, float eta) {
+  float ndi = dot(N, I);
+  float k = 1.0f - eta * eta * (1.0f - ndi * ndi);
+  float s;
+  if (k < 0.0f) return mk(0.0f, 0.0f, 0.0f);
+  s = eta * ndi + sqrtf(k);
+  return mk(eta * I.x - s * N.x, eta * I.y - s * N.y, eta * I.z - s * N.z);
+}
+static v3f rt_custom_refract(v3f d, v3f n, float eta) {
+  float ndotd = dot(n, d), angle;
+  if (ndotd > 0.0f) {
+    n = mk(-n.x, -n.y, -n.z);
+    ndotd = dot(n, d);
+  } else {
+    eta = 1.0f / eta;
+  }
+  angle = (float)sin((double)(float)acos((double)ndotd)) * eta;
+  if (-1.0f < angle && angle < 1.0f) return rt_refract(d, n, eta);
+  return rt_reflect(d, n);
+}
+static v3f rt_random_normal_dir(uint32_t* rng, v3f n) {
+  float theta = 2.0f * RT_PI * rt_rand(rng);
+  float u = 2.0f * rt_rand(rng) - 1.0f;
+  float suu = sqrtf(1.0f - u * u);
+  v3f v = mk(suu * (float)cos((double)theta), suu * (float)sin((double)theta), u);
+  if (dot(v, n) < 0.0f) v = mk(-v.x, -v.y, -v.z);
+  return v;
+}
+
+typedef struct {
+  v3f pos, n, color;
+  float dT, rT, tT, eta;
+  int light;
+} rt_payload;
+
+/* barycentric (u, v) of the Moller-Trumbore test, the same operations as ref_intersect */
+static rt_payload rt_hit(const swo_scene* s, uint32_t k, v3f o, v3f d) {
+  rt_payload P;
+  v3f v0 = ld3(s->v0 + 3 * (size_t)k), e0 = ld3(s->e0 + 3 * (size_t)k), e1 = ld3(s->e1 + 3 * (size_t)k);
+  v3f h = cross(d, e1), sv = sub(o, v0), q;
+  float f = 1.0f / dot(e0, h), u, v, b0;
+  const float* nr = s->nrm + 9 * (size_t)k;
+  const float* m = s->mats + 9 * (size_t)s->tri_obj[k];
+  u = f * dot(sv, h);
+  q = cross(sv, e0);
+  v = f * dot(d, q);
+  b0 = 1.0f - u - v;
+  P.pos = mk(v0.x + e0.x * u + e1.x * v, v0.y + e0.y * u + e1.y * v, v0.z + e0.z * u + e1.z * v);
+  P.n = rt_normalize(mk(nr[0] * b0 + nr[3] * u + nr[6] * v, nr[1] * b0 + nr[4] * u + nr[7] * v,
+                        nr[2] * b0 + nr[5] * u + nr[8] * v));
+  P.light = m[7] != 0.0f;
+  P.color = mk(m[0], m[1], m[2]);
+  if (P.light) P.color = mk(m[0] * m[8], m[1] * m[8], m[2] * m[8]);
+  P.dT = m[3];
+  P.rT = m[4];
+  P.tT = m[5];
+  P.eta = m[6];
+  return P;
+}
+
+/* handleHit: returns 1 for DIFFUSE_VALUE (also the value when no branch is taken) */
+static int rt_handle_hit(const rt_payload* P, uint32_t* rng, v3f* o, v3f* d) {
+  float r = rt_rand(rng);
+  int diffuse = 1;
+  if (r <= P->dT) {
+    *d = rt_random_normal_dir(rng, P->n);
+  } else if (r <= P->rT) {
+    *d = rt_reflect(*d, P->n);
+    diffuse = 0;
+  } else if (r <= P->tT) {
+    *d = rt_custom_refract(*d, P->n, P->eta);
+    diffuse = 0;
+  }
+  *o = mk(P->pos.x + d->x * 0.001f, P->pos.y + d->y * 0.001f, P->pos.z + d->z * 0.001f);
+  return diffuse;
+}
+
+static uint8_t rt_unorm8(float x) {
+  float c = x > 0.0f ? x : 0.0f; /* NaN -> 0 */
+  if (c > 1.0f) c = 1.0f;
+  return (uint8_t)nearbyintf(c * 255.0f);
+}
+
+static v3f rt_pixel(const swo_scene* s, const swo_camera* cam, uint32_t x, uint32_t y, uint32_t W, uint32_t H,
+                    uint32_t vj, uint32_t spp) {
+  const float* vi = cam->vi;
+  const float* pi = cam->pi;
+  uint32_t rng = rt_lcg_init(x, y), smp, i, c;
+  float ux = ((float)x + 0.5f) / (float)W, uy = ((float)y + 0.5f) / (float)H;
+  float dx = ux * 2.0f - 1.0f, dy = uy * 2.0f - 1.0f, t;
+  v3f o = mk(vi[12], vi[13], vi[14]), tg, w, d, sdir, fin = mk(0.0f, 0.0f, 0.0f);
+  rt_payload def;
+  uint32_t k;
+  tg = mk(pi[0] * dx + pi[4] * dy + pi[8] * 1.0f + pi[12] * 1.0f, pi[1] * dx + pi[5] * dy + pi[9] * 1.0f + pi[13] * 1.0f,
+          pi[2] * dx + pi[6] * dy + pi[10] * 1.0f + pi[14] * 1.0f);
+  tg = rt_normalize(tg);
+  w = mk(vi[0] * tg.x + vi[4] * tg.y + vi[8] * tg.z + vi[12] * 0.0f,
+         vi[1] * tg.x + vi[5] * tg.y + vi[9] * tg.z + vi[13] * 0.0f,
+         vi[2] * tg.x + vi[6] * tg.y + vi[10] * tg.z + vi[14] * 0.0f);
+  sdir = rt_normalize(w);
+  /* traceRay with back-face culling: up to four traces */
+  for (c = 0;; ++c) {
+    k = rt_closest(s, o, sdir, &t);
+    if (k == 0xFFFFFFFFu) return mk(0.0f, 0.0f, 0.0f);
+    def = rt_hit(s, k, o, sdir);
+    if (!(dot(def.n, sdir) > 0.0f) || c == 3) break;
+    o = def.pos;
+  }
+  if (def.light) return def.color;
+  for (smp = 0; smp < spp; ++smp) {
+    rt_payload cur = def;
+    v3f col = mk(1.0f, 1.0f, 1.0f);
+    int light_hit = 0;
+    d = sdir;
+    for (i = 1; i < vj; ++i) {
+      if (rt_handle_hit(&cur, &rng, &o, &d)) {
+        float cs = dot(d, cur.n);
+        col = mk(col.x * (cur.color.x * cs), col.y * (cur.color.y * cs), col.z * (cur.color.z * cs));
+      }
+      k = rt_closest(s, o, d, &t);
+      if (k == 0xFFFFFFFFu) break; /* color = 0 */
+      cur = rt_hit(s, k, o, d);
+      if (cur.light && dot(d, cur.n) <= 0.0f) {
+        col = mk(col.x * cur.color.x, col.y * cur.color.y, col.z * cur.color.z);
+        light_hit = 1;
+        break;
+      }
+    }
+    if (light_hit) fin = add(fin, col);
+  }
+  {
+    float sc = (2.0f * RT_PI) / (float)spp;
+    return mk(fin.x * sc, fin.y * sc, fin.z * sc);
+  }
+}
+
+typedef struct {
+  const swo_scene* s;
+  const swo_camera* cam;
+  uint32_t W, H, vj, spp, p0;
+  float* rgb;
+  uint8_t* rgba;
+} rt_ctx;
+
+static void rt_range(void* c_, uint64_t b, uint64_t e) {
+  rt_ctx* c = (rt_ctx*)c_;
+  uint64_t k;
+  for (k = b; k < e; ++k) {
+    uint32_t p = c->p0 + (uint32_t)k;
+    v3f v = rt_pixel(c->s, c->cam, p % c->W, p / c->W, c->W, c->H, c->vj, c->spp);
+    if (c->rgb) {
+      c->rgb[3 * k + 0] = v.x;
+      c->rgb[3 * k + 1] = v.y;
+      c->rgb[3 * k + 2] = v.z;
+    }
+    if (c->rgba) {
+      c->rgba[4 * k + 0] = rt_unorm8(v.x);
+      c->rgba[4 * k + 1] = rt_unorm8(v.y);
+      c->rgba[4 * k + 2] = rt_unorm8(v.z);
+      c->rgba[4 * k + 3] = 0;
+    }
+  }
+}
+
+void swo_rt_render(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H, uint32_t vj, uint32_t spp,
+                   uint32_t p0, uint32_t p1, float* rgb, uint8_t* rgba, int threads) {
+  rt_ctx c = {s, cam, W, H, vj, spp, p0, rgb, rgba};
+  parallel_for(p1 - p0, 4, threads, rt_range, &c);
+}
+
+typedef struct {
+  const swo_scene* s;
+  const float *ro, *rd;
+  uint32_t* tri;
+  float* t;
+} rt_trace_ctx;
+
+static void rt_trace_range(void* c_, uint64_t b, uint64_t e) {
+  rt_trace_ctx* c = (rt_trace_ctx*)c_;
+  uint64_t i;
+  for (i = b; i < e; ++i) c->tri[i] = rt_closest(c->s, ld3(c->ro + 4 * i), ld3(c->rd + 4 * i), &c->t[i]);
+}
+
+void swo_rt_trace(const swo_scene* s, const float* ro, const float* rd, uint64_t n, uint32_t* hit_tri,
+                  float* hit_t, int threads) {
+  rt_trace_ctx c = {s, ro, rd, hit_tri, hit_t};
+  parallel_for(n, 64, threads, rt_trace_range, &c);
+}
+
+int swo_rt_gauss_weights(uint32_t k, float sigma, float* out) {
+  float sum = 0.0f;
+  uint32_t i;
+  if (k == 0 || k > 19 || (k & 1u) == 0) return -1;
+  for (i = 0; i < k; ++i) {
+    float a = (float)i - ((float)k - 1.0f), b, r;
+    a = a * a;
+    b = 2.0f * sigma * sigma;
+    r = (float)exp((double)(-a / b));
+    out[i] = r;
+    sum += r;
+  }
+  sum = 1.0f / sum;
+  for (i = 0; i < k; ++i) out[i] *= sum;
+  return 0;
+}
+
+void swo_rt_denoise_gauss(const uint8_t* in, uint8_t* out, uint32_t W, uint32_t H, uint32_t k,
+                          const float* g) {
+  int off = (int)(k / 2), x, y, dx, dy, ch;
+  for (y = 0; y < (int)H; ++y)
+    for (x = 0; x < (int)W; ++x) {
+      float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      for (dx = -off; dx <= off; ++dx)
+        for (dy = -off; dy <= off; ++dy) {
+          int px = x + dx, py = y + dy;
+          if (0 <= px && px < (int)W && 0 <= py && py < (int)H)
+            for (ch = 0; ch < 4; ++ch)
+              c[ch] += (float)in[4 * ((size_t)py * W + px) + ch] / 255.0f * g[dx + off] * g[dy + off];
+        }
+      for (ch = 0; ch < 4; ++ch) out[4 * ((size_t)y * W + x) + ch] = rt_unorm8(c[ch]);
+    }
+}
+
+static int cmp_float(const void* a, const void* b) {
+  float x = *(const float*)a, y = *(const float*)b;
+  return (x > y) - (x < y);
+}
+
+void swo_rt_denoise_median(const uint8_t* in, uint8_t* out, uint32_t W, uint32_t H) {
+  int x, y, dx, dy, ch;
+  for (y = 0; y < (int)H; ++y)
+    for (x = 0; x < (int)W; ++x)
+      for (ch = 0; ch < 4; ++ch) {
+        float v[9];
+        int n = 0;
+        for (dx = -1; dx <= 1; ++dx)
+          for (dy = -1; dy <= 1; ++dy) {
+            int px = x + dx, py = y + dy;
+            /* texels outside the image: undefined in the shader, 0 here */
+            v[n++] = (0 <= px && px < (int)W && 0 <= py && py < (int)H)
+                         ? (float)in[4 * ((size_t)py * W + px) + ch] / 255.0f
+                         : 0.0f;
+          }
+        qsort(v, 9, sizeof(float), cmp_float);
+        out[4 * ((size_t)y * W + x) + ch] = rt_unorm8(v[4]);
+      }
+}

@@ -61,6 +61,19 @@ int swo_render_bdpt(const swo_scene* s, const swo_camera* cam, uint32_t W, uint3
                     uint32_t vision_jumps, uint32_t light_jumps, uint32_t max_depth, uint64_t seed,
                     uint32_t p0, uint32_t p1, float* per_sample, float* per_pixel, int threads);
 
+/* The Vulkan application's PathTracer (RayTrace program) for pixels [p0, p1): finalColor [n*3]
+ * and the stored rgba8 texel [n*4] (either may be NULL). */
+void swo_rt_render(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H, uint32_t vision_jumps,
+                   uint32_t spp, uint32_t p0, uint32_t p1, float* rgb, uint8_t* rgba, int threads);
+/* traceRay's closest hit: triangle id (0xFFFFFFFF on a miss) and t */
+void swo_rt_trace(const swo_scene* s, const float* ro, const float* rd, uint64_t n, uint32_t* hit_tri,
+                  float* hit_t, int threads);
+/* GaussDenoiser weights; -1 for a kernel size that is not odd in 1..19 */
+int swo_rt_gauss_weights(uint32_t kernel_size, float sigma, float* out);
+void swo_rt_denoise_gauss(const uint8_t* in, uint8_t* out, uint32_t W, uint32_t H, uint32_t kernel_size,
+                          const float* weights);
+void swo_rt_denoise_median(const uint8_t* in, uint8_t* out, uint32_t W, uint32_t H);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,8 @@ class Twin:
             L.twin_render.argtypes = [P, P] + [ctypes.c_uint32] * 4 + [ctypes.c_uint64, ctypes.c_uint32,
                                                                         ctypes.c_uint32, ctypes.c_float,
                                                                         ctypes.c_uint32, ctypes.c_uint32, P]
+            L.twin_rt_trace.argtypes = [P, P, P, ctypes.c_uint64, P, P]
+            L.twin_rt_render.argtypes = [P, P] + [ctypes.c_uint32] * 6 + [P]
             Twin._lib = L
         from master_thesis_b200 import _native as N
         self._d = scene_data.desc()
@@ -90,6 +92,20 @@ class Twin:
         out = np.empty((p1 - p0, spp, 4), np.float32)
         Twin._lib.twin_render(self._h, ctypes.byref(cam), W, H, spp, depth, seed, mode, rr_depth, rr_q,
                               p0, p1, out.ctypes.data)
+        return out
+
+
+    def rt_trace(self, ro, rd):
+        n = ro.shape[0]
+        tri = np.empty(n, np.uint32)
+        t = np.empty(n, np.float32)
+        Twin._lib.twin_rt_trace(self._h, ro.ctypes.data, rd.ctypes.data, n, tri.ctypes.data, t.ctypes.data)
+        return tri, t
+
+    def rt_render(self, cam, W, H, spp, vision_jumps, p0=0, p1=None):
+        p1 = W * H if p1 is None else p1
+        out = np.empty((p1 - p0, 3), np.float32)
+        Twin._lib.twin_rt_render(self._h, ctypes.byref(cam), W, H, vision_jumps, spp, p0, p1, out.ctypes.data)
         return out
 
 

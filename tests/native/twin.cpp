@@ -6,7 +6,7 @@
 #include <cstring>
 #include <vector>
 
-#include "../../master_thesis_b200/csrc/cuda/shading.cuh"
+#include "../../master_thesis_b200/csrc/cuda/rt_shading.cuh"
 #include "../../master_thesis_b200/csrc/host/ref_bvh.h"
 #include "../../master_thesis_b200/csrc/host/scene_pack.h"
 
@@ -185,6 +185,76 @@ void twin_render(void* tw, const swr_camera* cam, uint32_t W, uint32_t H, uint32
         t = h.t;
       }
     }
+  }
+}
+
+// traceRay's closest hit (the ray-query rule) with the kernels' traversal code
+void twin_rt_trace(void* tw, const float* ro, const float* rd, uint64_t n, uint32_t* tri, float* t) {
+  const swr::PackedScene& p = ((Twin*)tw)->pk;
+  uint2 stack[swrx::kStackShared];
+  for (uint64_t i = 0; i < n; ++i) {
+    swrx::Hit h;
+    swrx::trace_closest<false, false, swrx::kRuleRayQuery>(
+        (const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(), p.obj_boxes.data(),
+        swrx::mk(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), swrx::mk(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]), stack, 1,
+        h, nullptr);
+    tri[i] = h.id;
+    t[i] = h.t;
+  }
+}
+
+// The RayTrace PathTracer's raygen for pixels [p0, p1) with the kernels' shading code
+// (rt_shading.cuh) and traversal; the control flow restates k_rt_path per pixel.
+void twin_rt_render(void* tw, const swr_camera* cam, uint32_t W, uint32_t H, uint32_t vj, uint32_t spp,
+                    uint32_t p0, uint32_t p1, float* rgb) {
+  namespace rt = swrx::rt;
+  const swr::PackedScene& p = ((Twin*)tw)->pk;
+  const float4* nodes = (const float4*)p.nodes.data();
+  uint2 stack[swrx::kStackShared];
+  auto trace = [&](swrx::f3 o, swrx::f3 d, swrx::Hit& h) {
+    return swrx::trace_closest<false, false, swrx::kRuleRayQuery>(nodes, p.tris.data(), p.tri_boxes.data(),
+                                                                  p.obj_boxes.data(), o, d, stack, 1, h, nullptr);
+  };
+  for (uint32_t pix = p0; pix < p1; ++pix) {
+    float* out = rgb + 3 * (size_t)(pix - p0);
+    uint32_t rng = rt::lcg_init(pix % W, pix / W, 0u);
+    swrx::f3 o, sdir;
+    rt::vision_ray(cam->view_inv, cam->proj_inv, pix % W, pix / W, W, H, o, sdir);
+    swrx::Hit h;
+    rt::Payload def;
+    bool hit = false;
+    for (uint32_t c = 0; c < 4; ++c) {
+      hit = trace(o, sdir, h);
+      if (!hit) break;
+      def = rt::hit_payload(p.tris.data(), p.shade.data(), p.mats.data(), h.slot, o, sdir);
+      if (!(swrx::vdot(def.n, sdir) > 0.0f)) break;
+      o = def.pos;
+    }
+    swrx::f3 fin = swrx::mk(0.0f, 0.0f, 0.0f);
+    if (hit && def.light) {
+      fin = def.color;
+    } else if (hit) {
+      for (uint32_t s = 0; s < spp; ++s) {
+        rt::Payload cur = def;
+        swrx::f3 d = sdir, col = swrx::mk(1.0f, 1.0f, 1.0f);
+        for (uint32_t i = 1; i < vj; ++i) {
+          if (rt::handle_hit(cur, rng, o, d)) {
+            const float cs = swrx::vdot(d, cur.n);
+            col = swrx::vmul(col, swrx::vscale(cs, cur.color));
+          }
+          if (!trace(o, d, h)) break;
+          cur = rt::hit_payload(p.tris.data(), p.shade.data(), p.mats.data(), h.slot, o, d);
+          if (cur.light && swrx::vdot(d, cur.n) <= 0.0f) {
+            fin = swrx::vadd(fin, swrx::vmul(col, cur.color));
+            break;
+          }
+        }
+      }
+      fin = swrx::vscale((2.0f * rt::kPi) / (float)spp, fin);
+    }
+    out[0] = fin.x;
+    out[1] = fin.y;
+    out[2] = fin.z;
   }
 }
 
