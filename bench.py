@@ -52,9 +52,13 @@ CONFIGS = {
     # settings (res/renderer/path_tracer.renderer: visionJumpCount 5, visionRayPerPixelCount 13) on
     # the Cornell scene at 1920x1080, and on the terrain scene (no CPU baseline: the oracle's closest
     # hit tests every triangle)
-    "c6": dict(kind="cornell", renderer="rt", W=1920, H=1080, spp=13, depth=5, seed=1),
+    # (launch shape: refill / shading batch / blocks per SM measured best per scene)
+    "c6": dict(kind="cornell", renderer="rt", W=1920, H=1080, spp=13, depth=5, seed=1, refill=4, shade_batch=16,
+               blocks_per_sm=6),
+    # the same at 480x270, for profiler captures of single kernel launches
+    "c6s": dict(kind="cornell", renderer="rt", W=480, H=270, spp=13, depth=5, seed=1),
     "c6t": dict(kind="terrain", renderer="rt", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080,
-                spp=13, depth=5, seed=2024),
+                spp=13, depth=5, seed=2024, refill=2, shade_batch=8, blocks_per_sm=0),
     # differentiable: tessellated Cornell (~49k triangles), 512x512, 32 spp primal + 32 spp adjoint, depth 6
     "c4": dict(kind="diff", W=512, H=512, spp=32, depth=6, seed=11),
     # batched inverse rendering: 64 scenes (5k-200k triangles, 128^2-512^2), 16 spp primal/adjoint, depth 5,
@@ -367,7 +371,9 @@ def run_rt(args, cfg, files, workload):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
     params = dict(vision_jumps=vj, spp=spp, denoisers=[])
-    frame = lambda out: rt.render_frame(sc, cam, W, H, params, out=out, stream=stream)
+    shape = dict(refill=cfg.get("refill", 0), shade_batch=cfg.get("shade_batch", 0),
+                 blocks_per_sm=cfg.get("blocks_per_sm", 0))
+    frame = lambda out: rt.render_frame(sc, cam, W, H, params, out=out, stream=stream, **shape)
     for _ in range(max(args.warmup, 3)):
         frame(rgba)
     torch.cuda.synchronize()
@@ -375,8 +381,13 @@ def run_rt(args, cfg, files, workload):
     clocks.start()
     ms = _events_ms(lambda: frame(rgba), args.steps, flush)
     host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True).numpy()
+    for _ in range(max(args.warmup, 3)):
+        frame(host)
     e2e = _events_ms(lambda: frame(host), args.steps, flush)
     den = torch.empty_like(rgba)
+    for _ in range(max(args.warmup, 3)):
+        rt.denoise_gauss(rgba, 5, 1.0, out=den, stream=stream)
+        rt.denoise_median(rgba, out=den, stream=stream)
     g_ms = _events_ms(lambda: rt.denoise_gauss(rgba, 5, 1.0, out=den, stream=stream), args.steps, flush)
     m_ms = _events_ms(lambda: rt.denoise_median(rgba, out=den, stream=stream), args.steps, flush)
     clk = clocks.stop()
@@ -395,7 +406,8 @@ def run_rt(args, cfg, files, workload):
         "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scene files)",
-        "config": {"workload": workload, "triangles": int(sd.num_triangles), "l2": "flushed between steps (256 MB write)"},
+        "config": {"workload": workload, "triangles": int(sd.num_triangles), "l2": "flushed between steps (256 MB write)",
+                   "launch": shape},
         "e2e": {"value": samples / (e2e / 1e3) / 1e6, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": W * H * 4},
         "gpu_launches": 1 * args.steps,

@@ -348,8 +348,12 @@ typedef struct swr_rt_opts {
   uint32_t width, height;  /* launch size = image size */
   uint32_t vision_jumps;   /* visionJumpCount (path_tracer.cpp:30-33), <= 65536 */
   uint32_t spp;            /* visionRayPerPixelCount, 1..2^24 */
-  uint32_t refill;         /* idle lanes of a warp that take new pixels (1..32), 0 = 8 */
-  uint32_t reserved[3];
+  uint32_t refill;         /* idle lanes of a warp that take new pixels (1..32), 0 = 4 */
+  uint32_t shade_batch;    /* lanes of a warp with a finished ray that shade together (1..32; fewer
+                              when no ray of the warp is in flight), 0 = 12 */
+  uint32_t blocks_per_sm;  /* resident blocks per SM targeted by the register budget: 0 (compiler's
+                              choice), 5 or 6 */
+  uint32_t reserved;
 } swr_rt_opts;
 
 /* One PathTracer frame (path_tracer_vision_raygen.rgen:8-60): per pixel the LCG random numbers

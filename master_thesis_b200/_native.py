@@ -118,7 +118,8 @@ BATCH_NO_GRAPH = 1
 
 class RtOpts(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("vision_jumps", ctypes.c_uint32),
-                ("spp", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
+                ("spp", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("shade_batch", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 DENOISER_GAUSS = 1

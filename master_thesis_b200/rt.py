@@ -37,14 +37,14 @@ def trace(scene, ray_o, ray_d, out=None, stream=None):
 
 
 def render(scene, cam, width, height, spp, vision_jumps, rgb=None, rgba=None, want_rgb=True, want_rgba=True,
-           refill=0, stream=None):
+           refill=0, shade_batch=0, blocks_per_sm=0, stream=None):
     """One PathTracer frame: (finalColor (height, width, 3) float32, rgba8 (height, width, 4)
     uint8); either output may be switched off (None is returned for it)."""
     if want_rgb and rgb is None:
         rgb = _empty((height, width, 3), np.float32, rgba)
     if want_rgba and rgba is None:
         rgba = _empty((height, width, 4), np.uint8, rgb)
-    o = N.RtOpts(width, height, vision_jumps, spp, refill)
+    o = N.RtOpts(width, height, vision_jumps, spp, refill, shade_batch, blocks_per_sm)
     check(N.lib.swr_rt_render(scene.handle, ctypes.byref(cam), ctypes.byref(o), ptr(rgb) if want_rgb else None,
                               ptr(rgba) if want_rgba else None, _stream_handle(stream)))
     return (rgb if want_rgb else None), (rgba if want_rgba else None)
@@ -103,12 +103,13 @@ def _denoiser_array(denoisers):
     return arr
 
 
-def render_frame(scene, cam, width, height, params, out=None, refill=0, stream=None):
+def render_frame(scene, cam, width, height, params, out=None, refill=0, shade_batch=0, blocks_per_sm=0,
+                 stream=None):
     """GraphicsEngine::render for the PathTracer: the frame, then the denoisers of `params`
     (a load_renderer() dict) in order. Returns the final rgba8 image (height, width, 4)."""
     if out is None:
         out = _empty((height, width, 4), np.uint8)
-    o = N.RtOpts(width, height, params["vision_jumps"], params["spp"], refill)
+    o = N.RtOpts(width, height, params["vision_jumps"], params["spp"], refill, shade_batch, blocks_per_sm)
     dn = params.get("denoisers", [])
     check(N.lib.swr_rt_render_frame(scene.handle, ctypes.byref(cam), ctypes.byref(o), _denoiser_array(dn), len(dn),
                                     ptr(out), _stream_handle(stream)))

@@ -64,9 +64,10 @@ def test_gpu_rt_render_matches_oracle(name):
     assert np.any(want_rgb > 0)
 
 
-@pytest.mark.parametrize("refill", [1, 8, 32])
-def test_gpu_rt_render_larger_image_and_refill(tmp_path, refill):
-    """Many pixels per lane (persistent refill), host output buffers, one output only."""
+@pytest.mark.parametrize("refill,shade_batch", [(1, 1), (8, 1), (32, 1), (4, 8), (2, 32)])
+def test_gpu_rt_render_larger_image_and_refill(tmp_path, refill, shade_batch):
+    """Many pixels per lane (persistent refill, batched shading), host output buffers, one output
+    only."""
     s = scenes.cornell(8, str(tmp_path))
     sd = swr.load_scene(s["scene"], s["basepath"])
     sc = swr.Scene(sd)
@@ -75,11 +76,11 @@ def test_gpu_rt_render_larger_image_and_refill(tmp_path, refill):
     vi, pi, org = swr.camera_arrays(cam)
     want_rgb, want_rgba = O.rt_render(O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org), W, H, spp, vj)
     rgba = np.zeros((H, W, 4), np.uint8)
-    _, out = rt.render(sc, cam, W, H, spp, vj, rgba=rgba, want_rgb=False, refill=refill)
+    _, out = rt.render(sc, cam, W, H, spp, vj, rgba=rgba, want_rgb=False, refill=refill, shade_batch=shade_batch)
     assert out is rgba
     assert np.mean(np.all(rgba.reshape(-1, 4) == want_rgba, axis=1)) > 0.99
     rgb = np.zeros((H, W, 3), np.float32)
-    rt.render(sc, cam, W, H, spp, vj, rgb=rgb, want_rgba=False, refill=refill)
+    rt.render(sc, cam, W, H, spp, vj, rgb=rgb, want_rgba=False, refill=refill, shade_batch=shade_batch)
     assert _close(rgb.reshape(-1, 3), want_rgb)
 
 
