@@ -97,6 +97,11 @@ class ClockSampler:
                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         self.t = threading.Thread(target=self._read, daemon=True)
         self.t.start()
+        # nvidia-smi's start-up (driver and NVML initialisation) stalls this process's CUDA calls
+        # for up to ~0.1 s: wait for its first sample so the start-up falls before the timed region
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:

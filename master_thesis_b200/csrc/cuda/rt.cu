@@ -16,8 +16,10 @@
 //                shading code for one or two lanes at a time (7.2 of 32 lanes per instruction);
 //                batching 12-16 lanes made the Cornell frame 1.9x and the terrain frame 1.2x
 //                faster.
-//   k_rt_gauss   one thread per pixel: the (2*off+1)^2 weighted taps in the shader's order.
-//   k_rt_median  one thread per pixel: per-channel median of the 3x3 neighbourhood.
+//   k_rt_gauss   one thread per pixel: the (2*off+1)^2 weighted taps in the shader's order, from
+//                a shared-memory tile of converted texels.
+//   k_rt_median  one thread per pixel: per-channel median of the 3x3 neighbourhood, from a
+//                shared-memory tile.
 #include <algorithm>
 #include <cstring>
 
@@ -217,36 +219,53 @@ struct GaussArgs {
   uint32_t W, H;
 };
 
-// imageLoad of an rgba8 texel: byte / 255 as an IEEE float quotient
-__device__ __forceinline__ float unorm_load(const float* lut, uint32_t b) { return lut[b]; }
+// Denoiser blocks: 32 x 8 threads, one output texel each. A block first stages the texels its
+// outputs read (the halo of the largest kernel, 19 taps, included) in shared memory, converted
+// once per block; texels outside the image are stored as zeros, which add +0 to a tap sum that
+// never holds -0, so the sum is the shader's sum over the in-image taps alone.
+constexpr int kDx = 32, kDy = 8;
+constexpr int kGaussTile = (kDx + 2 * (kMaxGauss / 2)) * (kDy + 2 * (kMaxGauss / 2));
 
-__global__ void __launch_bounds__(256) k_rt_gauss(const uchar4* __restrict__ in, uchar4* __restrict__ out,
-                                                  GaussArgs A) {
+__global__ void __launch_bounds__(kDx * kDy) k_rt_gauss(const uchar4* __restrict__ in, uchar4* __restrict__ out,
+                                                        GaussArgs A) {
   __shared__ float lut[256];
-  for (uint32_t k = threadIdx.y * blockDim.x + threadIdx.x; k < 256; k += blockDim.x * blockDim.y)
-    lut[k] = __fdiv_rn((float)k, 255.0f);
+  __shared__ float g[kMaxGauss + 1];
+  __shared__ float4 tile[kGaussTile];
+  const int tid = (int)(threadIdx.y * kDx + threadIdx.x);
+  // imageLoad of an rgba8 texel: byte / 255 as an IEEE float quotient
+  lut[tid] = __fdiv_rn((float)tid, 255.0f);
+  if (tid <= kMaxGauss) g[tid] = A.g[tid];
   __syncthreads();
-  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
-  if (x >= (int)A.W || y >= (int)A.H) return;
+  const int W = (int)A.W, H = (int)A.H, off = A.off;
+  const int tw = kDx + 2 * off, th = kDy + 2 * off;
+  const int x0 = (int)blockIdx.x * kDx - off, y0 = (int)blockIdx.y * kDy - off;
+  for (int k = tid; k < tw * th; k += kDx * kDy) {
+    const int ty = k / tw, tx = k - ty * tw;
+    const int px = x0 + tx, py = y0 + ty;
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (px >= 0 && px < W && py >= 0 && py < H) {
+      const uchar4 b = __ldg(in + (size_t)py * W + px);
+      v = make_float4(lut[b.x], lut[b.y], lut[b.z], lut[b.w]);
+    }
+    tile[k] = v;
+  }
+  __syncthreads();
+  const int x = (int)(blockIdx.x * kDx + threadIdx.x), y = (int)(blockIdx.y * kDy + threadIdx.y);
+  if (x >= W || y >= H) return;
   float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  for (int dx = -A.off; dx <= A.off; ++dx) {
-    const int px = x + dx;
-    if (px < 0 || px >= (int)A.W) continue;
-    const float gx = A.g[dx + A.off];
-    for (int dy = -A.off; dy <= A.off; ++dy) {
-      const int py = y + dy;
-      if (py < 0 || py >= (int)A.H) continue;
-      const float gy = A.g[dy + A.off];
-      const uchar4 v = __ldg(in + (size_t)py * A.W + px);
-      c.x = __fadd_rn(c.x, __fmul_rn(__fmul_rn(unorm_load(lut, v.x), gx), gy));
-      c.y = __fadd_rn(c.y, __fmul_rn(__fmul_rn(unorm_load(lut, v.y), gx), gy));
-      c.z = __fadd_rn(c.z, __fmul_rn(__fmul_rn(unorm_load(lut, v.z), gx), gy));
-      c.w = __fadd_rn(c.w, __fmul_rn(__fmul_rn(unorm_load(lut, v.w), gx), gy));
+  for (int dx = 0; dx <= 2 * off; ++dx) {  // x offset outer, y offset inner, as the shader loops
+    const float gx = g[dx];
+    const float4* col = tile + (int)threadIdx.y * tw + (int)threadIdx.x + dx;
+    for (int dy = 0; dy <= 2 * off; ++dy) {
+      const float gy = g[dy];
+      const float4 v = col[dy * tw];
+      c.x = __fadd_rn(c.x, __fmul_rn(__fmul_rn(v.x, gx), gy));
+      c.y = __fadd_rn(c.y, __fmul_rn(__fmul_rn(v.y, gx), gy));
+      c.z = __fadd_rn(c.z, __fmul_rn(__fmul_rn(v.z, gx), gy));
+      c.w = __fadd_rn(c.w, __fmul_rn(__fmul_rn(v.w, gx), gy));
     }
   }
-  out[(size_t)y * A.W + x] =
-      make_uchar4(rt::unorm8(c.x), rt::unorm8(c.y), rt::unorm8(c.z), rt::unorm8(c.w));
+  out[(size_t)y * W + x] = make_uchar4(rt::unorm8(c.x), rt::unorm8(c.y), rt::unorm8(c.z), rt::unorm8(c.w));
 }
 
 // Median of nine per byte lane: sort each row of three, then the median of (largest row
@@ -261,21 +280,26 @@ __device__ __forceinline__ uint32_t med3(uint32_t a, uint32_t b, uint32_t c) {
   return __vmaxu4(__vminu4(a, b), __vminu4(__vmaxu4(a, b), c));
 }
 
-__global__ void __launch_bounds__(256) k_rt_median(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                   uint32_t W, uint32_t H) {
-  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+__global__ void __launch_bounds__(kDx * kDy) k_rt_median(const uint32_t* __restrict__ in,
+                                                         uint32_t* __restrict__ out, uint32_t W, uint32_t H) {
+  constexpr int tw = kDx + 2, th = kDy + 2;
+  __shared__ uint32_t tile[tw * th];
+  const int tid = (int)(threadIdx.y * kDx + threadIdx.x);
+  const int x0 = (int)blockIdx.x * kDx - 1, y0 = (int)blockIdx.y * kDy - 1;
+  for (int k = tid; k < tw * th; k += kDx * kDy) {
+    const int ty = k / tw, tx = k - ty * tw;
+    const int px = x0 + tx, py = y0 + ty;
+    // texels outside the image are undefined in the shader; they count as 0 here
+    tile[k] = (px >= 0 && px < (int)W && py >= 0 && py < (int)H) ? __ldg(in + (size_t)py * W + px) : 0u;
+  }
+  __syncthreads();
+  const int x = (int)(blockIdx.x * kDx + threadIdx.x), y = (int)(blockIdx.y * kDy + threadIdx.y);
   if (x >= (int)W || y >= (int)H) return;
   uint32_t v[9];
 #pragma unroll
-  for (int r = 0; r < 3; ++r) {
+  for (int r = 0; r < 3; ++r)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int px = x + k - 1, py = y + r - 1;
-      // texels outside the image are undefined in the shader; they count as 0 here
-      v[3 * r + k] = (px >= 0 && px < (int)W && py >= 0 && py < (int)H) ? __ldg(in + (size_t)py * W + px) : 0u;
-    }
-  }
+    for (int k = 0; k < 3; ++k) v[3 * r + k] = tile[((int)threadIdx.y + r) * tw + (int)threadIdx.x + k];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     ex(v[3 * r], v[3 * r + 1]);
@@ -379,12 +403,12 @@ int gauss_args(uint32_t W, uint32_t H, uint32_t k, float sigma, GaussArgs& A) {
 }
 
 void launch_gauss(const uchar4* in, uchar4* out, const GaussArgs& A, cudaStream_t stream) {
-  const dim3 blk(32, 8), grd((A.W + 31) / 32, (A.H + 7) / 8);
+  const dim3 blk(kDx, kDy), grd((A.W + kDx - 1) / kDx, (A.H + kDy - 1) / kDy);
   k_rt_gauss<<<grd, blk, 0, stream>>>(in, out, A);
 }
 
 void launch_median(const uchar4* in, uchar4* out, uint32_t W, uint32_t H, cudaStream_t stream) {
-  const dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
+  const dim3 blk(kDx, kDy), grd((W + kDx - 1) / kDx, (H + kDy - 1) / kDy);
   k_rt_median<<<grd, blk, 0, stream>>>((const uint32_t*)in, (uint32_t*)out, W, H);
 }
 

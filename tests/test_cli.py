@@ -80,3 +80,30 @@ def test_cli_bidirectional_equals_library_render(tmp_path):
     got = np.frombuffer(out.read_bytes()[len(header):], np.uint8).reshape(H, W, 3)
     ref = swr.quantize_rgb8(img.cpu().numpy())
     assert np.array_equal(got, ref) and ref.max() > 0
+
+
+RT_CLI = os.path.join(os.path.dirname(CLI), "RayTrace")
+
+
+def test_raytrace_cli_argument_handling(tmp_path):
+    """The headless RayTrace drop-in (src/main.cpp:100-133 of the Vulkan program): argument count
+    check, the windowed form without a camera file refused, renderer names checked before any
+    device work."""
+    p = subprocess.run([RT_CLI, "a", "b"], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 255
+    assert "wrong paramter count" in p.stdout and "Usage: RayTrace renderer scene" in p.stdout
+    s = scenes.cornell(3, str(tmp_path))
+    exe = os.path.join(s["basepath"], "RayTrace")
+    shutil.copy(RT_CLI, exe)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    p = subprocess.run([exe, "r.renderer", s["scene"], "8", "8"], capture_output=True, text=True, timeout=60, env=env)
+    assert p.returncode == 255 and "needs one" in p.stdout
+    for text, msg in [("Majercik2022\n", "does not restate"), ("Raymarcher\n", "getRenderer not found"),
+                      ("PathTracer\n\tvisionJumpCount(5)\n\tvisionRayPerPixelCount(2)\nBlur\n", "getDenoiser not found")]:
+        r = tmp_path / "x.renderer"
+        r.write_text(text)
+        out = tmp_path / "o.ppm"
+        p = subprocess.run([exe, str(r), s["scene"], "8", "8", s["camera"], str(out), "1"], capture_output=True,
+                           text=True, timeout=120, env=env)
+        assert p.returncode != 0 and msg in p.stderr, p.stderr
+        assert not out.exists()
