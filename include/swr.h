@@ -112,7 +112,9 @@ typedef struct swr_render_opts {
   uint32_t refill;         /* bounce traversal: idle lanes (1..32) that trigger a refill, 0 = 8 */
   uint32_t trace_blocks;   /* bounce traversal: resident blocks per SM targeted by the register
                               budget, one of 0 (compiler's choice), 9, 10 */
-  uint32_t reserved;
+  uint32_t shade_batch;    /* adjoint: lanes of a warp with a pending hit that shade together
+                              (1..32; fewer when no trace of the warp is in flight), 0 = the
+                              library's choice; the wavefront renders ignore it */
 } swr_render_opts;
 
 #define SWR_RENDER_SAMPLES_OUT 1u   /* write per-sample radiance to the samples buffer */
@@ -243,7 +245,9 @@ int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_rende
 typedef struct swr_bdpt_opts {
   uint32_t light_jumps;
   uint32_t max_depth;
-  uint32_t reserved[2];
+  uint32_t shade_batch;  /* lanes of a warp with a finished trace that advance together (1..32), 0 =
+                            the library's choice */
+  uint32_t reserved;
 } swr_bdpt_opts;
 int swr_render_bdpt(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                     const swr_bdpt_opts* bdpt, float* rgb_out, float* samples_out, void* stream);
@@ -263,7 +267,7 @@ typedef struct swr_batch_opts {
   uint32_t wave_size;     /* paths in flight, 0 = 2^23 */
   uint32_t refill;        /* as in swr_render_opts, 0 = 8 */
   uint32_t flags;         /* SWR_BATCH_* */
-  uint32_t reserved;
+  uint32_t shade_batch;   /* batched adjoint: as swr_render_opts.shade_batch */
 } swr_batch_opts;
 #define SWR_BATCH_NO_GRAPH 1u /* launch the shade/trace rounds directly instead of from a CUDA graph */
 

@@ -73,7 +73,7 @@ class RenderOpts(ctypes.Structure):
                 ("rr_depth", ctypes.c_uint32), ("rr_survive", ctypes.c_float),
                 ("wave_size", ctypes.c_uint32), ("block_size", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("trace_blocks", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("shade_batch", ctypes.c_uint32)]
 
 
 class RenderProfile(ctypes.Structure):
@@ -92,11 +92,12 @@ class BatchJob(ctypes.Structure):
 
 class BatchOpts(ctypes.Structure):
     _fields_ = [("wave_size", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("flags", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("shade_batch", ctypes.c_uint32)]
 
 
 class BdptOpts(ctypes.Structure):
-    _fields_ = [("light_jumps", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2)]
+    _fields_ = [("light_jumps", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("shade_batch", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class RendererParams(ctypes.Structure):

@@ -220,14 +220,15 @@ def _scene_set_emission(self, emission, stream=None):
 
 
 def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=0, rr_depth=0, rr_survive=1.0,
-                          refill=0, stream=None, return_ms=False):
+                          refill=0, stream=None, return_ms=False, shade_batch=0):
     """Gradients (albedo [num_triangles,3], emission [num_objects,3]) of sum(dl_dimage * image) for
     the physical-mode image rendered with the same arguments (path replay). Device tensors."""
     import torch
     dl = dl_dimage.contiguous()
     ga = torch.empty((self.data.num_triangles, 3), dtype=torch.float32, device=dl.device)
     ge = torch.empty((self.data.num_objects, 3), dtype=torch.float32, device=dl.device)
-    o = N.RenderOpts(width, height, spp, depth, seed, N.MODE_PHYSICAL, rr_depth, rr_survive, 0, 0, 0, refill, 0, 0)
+    o = N.RenderOpts(width, height, spp, depth, seed, N.MODE_PHYSICAL, rr_depth, rr_survive, 0, 0, 0, refill, 0,
+                     shade_batch)
     ms = ctypes.c_double(0.0)
     check(N.lib.swr_render_adjoint_timed(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(dl), ptr(ga), ptr(ge),
                                          _stream_handle(stream), ctypes.byref(ms) if return_ms else None))
@@ -235,12 +236,12 @@ def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=
 
 
 def _scene_render_bdpt(self, cam, width, height, spp, vision_jumps, light_jumps, max_depth, seed=0, out=None,
-                       samples=None, refill=0, stream=None):
+                       samples=None, refill=0, shade_batch=0, stream=None):
     """BidirectionalPathTracer image (height, width, 3) into `out` (torch cuda tensor or numpy
     array); `samples` (optional, (height*width, spp, 4)) receives the per-sample contributions."""
     flags = N.RENDER_SAMPLES_OUT if samples is not None else 0
     o = N.RenderOpts(width, height, spp, vision_jumps, seed, N.MODE_REFERENCE, 0, 1.0, 0, 0, flags, refill, 0, 0)
-    b = N.BdptOpts(light_jumps, max_depth)
+    b = N.BdptOpts(light_jumps, max_depth, shade_batch)
     if out is None:
         import torch
         out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
@@ -294,7 +295,7 @@ class Batch:
         check(N.lib.swr_render_batch(self._h, arr, len(jobs), ctypes.byref(o), _stream_handle(stream)))
         return outs
 
-    def render_adjoint(self, jobs, refill=0, stream=None):
+    def render_adjoint(self, jobs, refill=0, stream=None, shade_batch=0):
         """Path-replay adjoint of many physical-mode jobs in one launch. jobs: dicts as for render
         plus dl_dimage (cuda tensor [h, w, 3]) and optionally grad_albedo / grad_emission (cuda
         tensors [num_triangles, 3] / [num_objects, 3]; jobs of one scene may share them and then
@@ -320,7 +321,7 @@ class Batch:
             arr[k].dl_dimage = dl.data_ptr()
             arr[k].dl_dalbedo = ga.data_ptr()
             arr[k].dl_demission = ge.data_ptr()
-        o = N.BatchOpts(0, refill, 0, 0)
+        o = N.BatchOpts(0, refill, 0, shade_batch)
         check(N.lib.swr_render_adjoint_batch(self._h, arr, len(jobs), ctypes.byref(o), _stream_handle(stream)))
         return grads
 

@@ -69,6 +69,7 @@ struct BArgs {
   uint32_t njobs;
   uint64_t npix;  // total pixels
   uint32_t capacity, refill;
+  uint32_t batch;               // adjoint: lanes with a finished trace that shade together
   float4* cam;                  // [npix*2]
   unsigned long long* accum;    // [npix*3] fixed point
 };
@@ -329,17 +330,20 @@ __global__ void __launch_bounds__(kTB) k_badjoint(BArgs A, BCtrl* __restrict__ c
       if (exhausted) break;
       continue;
     }
-    if (!active) continue;
-    if (tracing) {
-      if (!tr.step<false, false>(sc->nodes, sc->tris, sc->tri_boxes, sc->obj_boxes, nullptr)) continue;
+    if (active && tracing && tr.step<false, false>(sc->nodes, sc->tris, sc->tri_boxes, sc->obj_boxes, nullptr)) {
       tracing = false;
       if (tr.hit.slot == 0xFFFFFFFFu) {  // the path left the scene: no emitter, no gradient
         active = false;
-        continue;
+      } else {
+        pend_slot = tr.hit.slot;
+        pend_t = tr.hit.t;
       }
-      pend_slot = tr.hit.slot;
-      pend_t = tr.hit.t;
     }
+    // lanes with a pending hit wait until A.batch of them (or every active lane) shade together
+    const unsigned waiting = __ballot_sync(0xffffffffu, active && !tracing);
+    const unsigned inflight = __ballot_sync(0xffffffffu, active && tracing);
+    if (waiting == 0u || ((unsigned)__popc(waiting) < A.batch && inflight != 0u)) continue;
+    if (!active || tracing) continue;
     swrx::ShadeParams P;
     P.seed = J->seed;
     P.pixel = pixel;
@@ -643,6 +647,8 @@ int swr_render_adjoint_batch(swr_batch* b, const swr_adjoint_job* jobs, uint32_t
   }
   const uint32_t refill = (bo && bo->refill) ? bo->refill : 8;
   if (refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
+  const uint32_t batch = (bo && bo->shade_batch) ? bo->shade_batch : swrx::kAdjointBatch;
+  if (batch > 32) return set_error(SWR_ERR_INVALID, "swr: shade_batch must be 0..32");
   if ((rc = ensure_bytes(&b->cam, b->cambytes, pixels * 2 * sizeof(float4)))) return rc;
   if ((rc = ensure_bytes(&b->jobs, b->jobbytes, n * sizeof(BJob)))) return rc;
   if ((rc = ensure_bytes(&b->scenes, b->scenebytes, hs.size() * sizeof(DevScene)))) return rc;
@@ -657,6 +663,7 @@ int swr_render_adjoint_batch(swr_batch* b, const swr_adjoint_job* jobs, uint32_t
   A.njobs = n;
   A.npix = pixels;
   A.refill = refill;
+  A.batch = batch;
   A.cam = (float4*)b->cam;
   BCtrl init;
   std::memset(&init, 0, sizeof(init));

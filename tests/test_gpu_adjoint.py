@@ -38,11 +38,13 @@ def _render(scene, cam, albedo, emission):
     return img
 
 
-def test_adjoint_matches_fp64_reference_gradient(setup):
+@pytest.mark.parametrize("shade_batch", [0, 1, 16, 32])
+def test_adjoint_matches_fp64_reference_gradient(setup, shade_batch):
     sd, scene, albedo, emission, cam, target = setup
     img = _render(scene, cam, albedo, emission)
     dl = (2.0 * (img - target)).contiguous()
-    ga, ge = scene.render_adjoint(cam, W, H, SPP, DEPTH, dl, seed=SEED, rr_depth=RR, rr_survive=Q)
+    ga, ge = scene.render_adjoint(cam, W, H, SPP, DEPTH, dl, seed=SEED, rr_depth=RR, rr_survive=Q,
+                                  shade_batch=shade_batch)
     torch.cuda.synchronize()
     ga, ge = ga.cpu().numpy().astype(np.float64), ge.cpu().numpy().astype(np.float64)
     vi, pi, org = swr.camera_arrays(cam)

@@ -30,14 +30,15 @@ def _close(a, b, tol=1e-4):
     return float((a - b).norm()) <= tol * max(float(b.norm()), 1e-30)
 
 
-def test_batch_adjoint_matches_single_jobs():
+@pytest.mark.parametrize("shade_batch", [0, 1, 24])
+def test_batch_adjoint_matches_single_jobs(shade_batch):
     jobs = _jobs()
     rng = np.random.default_rng(1)
     for j in jobs:
         j["dl_dimage"] = torch.from_numpy(rng.normal(size=(j["height"], j["width"], 3)).astype(np.float32)).cuda()
     batch = swr.Batch()
     for rep in range(2):  # the second call reuses the batch buffers and re-zeroes the gradients
-        grads = batch.render_adjoint(jobs)
+        grads = batch.render_adjoint(jobs, shade_batch=shade_batch)
         torch.cuda.synchronize()
         for j, (ga, ge) in zip(jobs, grads):
             ra, re = j["scene"].render_adjoint(j["cam"], j["width"], j["height"], j["spp"], j["depth"],

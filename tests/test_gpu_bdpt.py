@@ -18,9 +18,10 @@ def _close(a, b):
     return np.all(np.abs(a - b) <= RTOL * np.maximum(np.abs(b), 1e-6) + 1e-7)
 
 
-def _render(sc, cam, W, H, spp, vj, lj, md, seed, refill=0):
+def _render(sc, cam, W, H, spp, vj, lj, md, seed, refill=0, shade_batch=0):
     samples = torch.empty((W * H, spp, 4), dtype=torch.float32, device="cuda")
-    img = sc.render_bdpt(cam, W, H, spp, vj, lj, md, seed=seed, samples=samples, refill=refill)
+    img = sc.render_bdpt(cam, W, H, spp, vj, lj, md, seed=seed, samples=samples, refill=refill,
+                         shade_batch=shade_batch)
     torch.cuda.synchronize()
     return img.cpu().numpy().reshape(-1, 3), samples.cpu().numpy()
 
@@ -39,13 +40,13 @@ def test_gpu_bdpt_matches_reference_golden(name):
     assert (np.abs(ref).sum(-1) > 0).mean() > 0.05
 
 
-@pytest.mark.parametrize("refill", [0, 1, 32])
-def test_gpu_bdpt_matches_oracle_on_terrain(tmp_path, refill):
+@pytest.mark.parametrize("refill,shade_batch", [(0, 0), (1, 1), (32, 1), (4, 16), (2, 32)])
+def test_gpu_bdpt_matches_oracle_on_terrain(tmp_path, refill, shade_batch):
     s = scenes.terrain(3, str(tmp_path), cells=64, tile=16, spheres=6, sphere_subdiv=2, lights=3)
     sd = swr.load_scene(s["scene"], s["basepath"])
     W, H, spp, vj, lj, md, seed = 40, 28, 3, 6, 4, 7, 5
     cam = swr.load_camera(s["camera"], W, H)
-    img, ps = _render(swr.Scene(sd), cam, W, H, spp, vj, lj, md, seed, refill)
+    img, ps = _render(swr.Scene(sd), cam, W, H, spp, vj, lj, md, seed, refill, shade_batch)
     vi, pi, org = swr.camera_arrays(cam)
     ops, opp = O.render_bdpt(O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org), W, H, spp, vj, lj, md, seed)
     assert _close(ps[..., :3], ops[..., :3])
