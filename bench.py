@@ -59,6 +59,10 @@ CONFIGS = {
     "c6s": dict(kind="cornell", renderer="rt", W=480, H=270, spp=13, depth=5, seed=1),
     "c6t": dict(kind="terrain", renderer="rt", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080,
                 spp=13, depth=5, seed=2024, refill=2, shade_batch=8, blocks_per_sm=0),
+    # moving objects: the terrain scene with its 64 spheres on a seeded random walk, one refit
+    # (swr_scene_set_transforms) and one 1920x1080 x 16 spp render per frame
+    "c7": dict(kind="animate", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=16,
+               depth=8, seed=2024, step=0.01),
     # differentiable: tessellated Cornell (~49k triangles), 512x512, 32 spp primal + 32 spp adjoint, depth 6
     "c4": dict(kind="diff", W=512, H=512, spp=32, depth=6, seed=11),
     # batched inverse rendering: 64 scenes (5k-200k triangles, 128^2-512^2), 16 spp primal/adjoint, depth 5,
@@ -429,6 +433,93 @@ def run_rt(args, cfg, files, workload):
         "setup_s": {"load": t1 - t0, "build_upload": t2 - t1}}))
 
 
+def run_animate(args, cfg):
+    """Moving objects: per frame, new placements for the spheres (a seeded random walk), the GPU
+    transform + BVH refit, and a render; against the same frames with the BVH rebuilt on the
+    device from the moved scene's data each frame."""
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import scenes
+    tmp = args.scene_dir or tempfile.mkdtemp(prefix="swr_bench_c7_")
+    s = scenes.terrain(cfg["seed"], tmp, cells=cfg["cells"], tile=cfg["tile"], spheres=cfg["spheres"],
+                       sphere_subdiv=cfg["subdiv"], lights=cfg["lights"])
+    t0 = time.time()
+    sc = swr.Scene.from_file(s["scene"], s["basepath"], builder="device")
+    torch.cuda.synchronize()
+    t1 = time.time()
+    W, H, spp, depth = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
+    cam = swr.load_camera(s["camera"], W, H)
+    xf0 = sc.transforms()
+    tiles = (cfg["cells"] // cfg["tile"]) ** 2
+    movers = np.arange(tiles, tiles + cfg["spheres"])
+    rng = np.random.default_rng(cfg["seed"])
+    out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    frames = []
+    xf = xf0.copy()
+    for _ in range(max(args.warmup, 3) + args.steps):
+        xf[movers, :3] += rng.normal(scale=cfg["step"], size=(len(movers), 3)).astype(np.float32)
+        frames.append(xf.copy())
+    for f in frames[:max(args.warmup, 3)]:
+        sc.set_transforms(f, stream=stream)
+        sc.render(cam, W, H, spp, depth, seed=1, out=out, stream=stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    refit_ms, render_ms = [], []
+    for f in frames[max(args.warmup, 3):]:
+        flush.fill_(1.0)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        sc.set_transforms(f, stream=stream)
+        e1.record(stream)
+        sc.render(cam, W, H, spp, depth, seed=1, out=out, stream=stream)
+        e2.record(stream)
+        e2.synchronize()
+        refit_ms.append(e0.elapsed_time(e1))
+        render_ms.append(e1.elapsed_time(e2))
+    clk = clocks.stop()
+    # the last frame's placements with a BVH built from scratch (device builder), for the tree
+    # quality after the moves and the rebuild time a refit replaces
+    sd = sc.data
+    moved = sc.transforms()
+    path = os.path.join(tmp, "moved.scene")
+    text = open(s["scene"]).read().split("\n")
+    k, lines = -1, []
+    for line in text:
+        if line and not line.startswith("\t"):
+            k += 1
+        if line.startswith("\tposition("):
+            line = "\tposition(%s, %s, %s)" % tuple(scenes._fmt(x) for x in moved[k, :3])
+        lines.append(line)
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines))
+    sdm = swr.load_scene(path, s["basepath"])
+    torch.cuda.synchronize()
+    t2 = time.time()
+    fresh = swr.Scene(sdm, builder="device")
+    torch.cuda.synchronize()
+    t3 = time.time()
+    fresh_ms = _events_ms(lambda: fresh.render(cam, W, H, spp, depth, seed=1, out=out, stream=stream), args.steps,
+                          flush)
+    samples = W * H * spp
+    step_ms = (sum(refit_ms) + sum(render_ms)) / args.steps
+    print(json.dumps({
+        "metric": "Msamples/s (moving objects: refit + render per frame)", "value": samples / (step_ms / 1e3) / 1e6,
+        "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene files)",
+        "config": {"workload": "terrain %d^2 cells + %d icospheres moving (random walk, sigma %.3g per frame) + %d "
+                               "lights, %dx%d, %d spp, depth %d" % (cfg["cells"], cfg["spheres"], cfg["step"],
+                                                                     cfg["lights"], W, H, spp, depth),
+                   "triangles": int(sd.num_triangles), "objects": int(sd.num_objects),
+                   "l2": "flushed between frames (256 MB write)"},
+        "refit_ms": sum(refit_ms) / args.steps, "render_ms": sum(render_ms) / args.steps,
+        "render_ms_fresh_tree": fresh_ms, "device_rebuild_s": t3 - t2, "setup_s": t1 - t0,
+        "clocks": clk}))
+
+
 def run_diff(args, cfg):
     """C4: physical-mode primal render vs the path-replay adjoint of an L2 image loss."""
     import torch
@@ -605,14 +696,14 @@ def main():
     ap.add_argument("--tune", action="store_true", help="autotune the launch shape (cached) before timing")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
-    if cfg["kind"] in ("batch", "diff", "inverse"):
+    if cfg["kind"] in ("batch", "diff", "inverse", "animate"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or differentiable "
-                                                                  "renderer"}))
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's software renderer has no batched, "
+                                                                  "differentiable or moving-object rendering"}))
             return
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        {"batch": run_batch, "diff": run_diff, "inverse": run_inverse}[cfg["kind"]](args, cfg)
+        {"batch": run_batch, "diff": run_diff, "inverse": run_inverse, "animate": run_animate}[cfg["kind"]](args, cfg)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -331,6 +331,35 @@ int swr_render_noalloc(swr_scene* scene, const swr_camera* cam, const swr_render
                        float* rgb_out, float* samples_out, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Moving objects: the object transform of GraphicsObject::init (graphics_object.cpp:12-27,54-62)
+ * and the BVH refit of BVH::rebuild (bounding_volume_hierachy.cpp:77-79,130-139) on the GPU. */
+
+/* An object's placement: position, scale and the rotation quaternion (s, x, y, z) that a scene
+ * file's rotation(axis_x, axis_y, axis_z, angle) gives (swr_rotation_from_axis_angle). */
+typedef struct swr_object_transform {
+  float position[3];
+  float scale[3];
+  float rotation[4];
+} swr_object_transform;
+/* InputEntry::getRotation (input_parser.cpp:20-26): s = cos(angle/2), (x,y,z) = sin(angle/2) *
+ * axis/|axis|, each in double and rounded to float. */
+int swr_rotation_from_axis_angle(const float axis[3], float angle, float out[4]);
+/* The placements of a loaded host scene's objects, in object order ([num_objects]). */
+int swr_host_scene_transforms(const swr_host_scene* hs, swr_object_transform* out);
+/* A scene built from a loaded host scene (as swr_scene_create on its descriptor) that also keeps
+ * the object-space meshes on the device, so that swr_scene_set_transforms can move its objects. */
+int swr_scene_create_from_host(const swr_host_scene* hs, const swr_build_opts* opts, swr_scene** out);
+/* New placements for every object of a scene made by swr_scene_create_from_host: each object's
+ * world vertices and normals are recomputed on the GPU from its object-space mesh (M = S*R*T,
+ * row vectors, the reference's float order of operations), then the triangle records, the
+ * reference's triangle and object boxes, the light tables and the tie ranks (the scene-level
+ * order of the moved objects' boxes) are rederived and the BVH is refit in place (topology kept,
+ * boxes recomputed bottom-up and requantised). Hits and renders afterwards equal those of a scene
+ * loaded from a file with the same placements. xf: [num_objects], host memory. */
+int swr_scene_set_transforms(swr_scene* scene, const swr_object_transform* xf, uint32_t num_objects,
+                             void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * The Vulkan application's PathTracer and denoisers (the RayTrace program: src/main.cpp:58-76,
  * src/graphic/renderer/path_tracer.cpp, src/graphic/denoiser/gauss_denoiser.cpp and
  * median_denoiser.cpp, and their shaders

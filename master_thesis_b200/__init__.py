@@ -12,7 +12,7 @@ _EXPORTS = {
     "MODE_PHYSICAL": "._native", "MODE_REFERENCE": "._native", "SwrError": "._native",
     "Scene": ".api", "SceneData": ".api", "Batch": ".api", "MAT_DTYPE": ".api", "camera_arrays": ".api",
     "load_camera": ".api", "make_camera": ".api", "load_renderer": ".api", "load_renderer_params": ".api",
-    "load_scene": ".api", "quantize_rgb8": ".api",
+    "load_scene": ".api", "quantize_rgb8": ".api", "rotation_from_axis_angle": ".api",
     "write_ppm": ".api",
 }
 

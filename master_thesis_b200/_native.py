@@ -117,6 +117,10 @@ class AdjointJob(ctypes.Structure):
 BATCH_NO_GRAPH = 1
 
 
+class ObjectTransform(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float * 3), ("scale", ctypes.c_float * 3), ("rotation", ctypes.c_float * 4)]
+
+
 class RtOpts(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("vision_jumps", ctypes.c_uint32),
                 ("spp", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("shade_batch", ctypes.c_uint32),
@@ -176,6 +180,11 @@ SIGNATURES = {
                                      ctypes.POINTER(ctypes.c_double)]),
     "swr_render_bdpt": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RenderOpts), ctypes.POINTER(BdptOpts), P, P, P]),
     "swr_renderer_load_params": (I, [ctypes.c_char_p, ctypes.POINTER(RendererParams)]),
+    "swr_rotation_from_axis_angle": (I, [ctypes.POINTER(ctypes.c_float), ctypes.c_float,
+                                         ctypes.POINTER(ctypes.c_float)]),
+    "swr_host_scene_transforms": (I, [P, P]),
+    "swr_scene_create_from_host": (I, [P, ctypes.POINTER(BuildOpts), ctypes.POINTER(P)]),
+    "swr_scene_set_transforms": (I, [P, P, U32, P]),
     "swr_rt_trace_closest": (I, [P, P, P, U64, P, P]),
     "swr_rt_render": (I, [P, ctypes.POINTER(Camera), ctypes.POINTER(RtOpts), P, P, P]),
     "swr_rt_gauss_weights": (I, [U32, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),

@@ -71,24 +71,37 @@ def load_scene(scene_path, basepath):
     h = ctypes.c_void_p()
     check(N.lib.swr_host_scene_load(os.fsencode(scene_path), os.fsencode(basepath), ctypes.byref(h)))
     try:
-        d = N.SceneDesc()
-        check(N.lib.swr_host_scene_desc(h, ctypes.byref(d)))
-        nv, nt, no = d.num_vertices, d.num_triangles, d.num_objects
-
-        def arr(p, n, dt):
-            return np.ctypeslib.as_array((dt * n).from_address(p)).copy()
-
-        vpos = arr(d.vertex_pos, nv * 3, ctypes.c_float)
-        vnrm = arr(d.vertex_normal, nv * 3, ctypes.c_float)
-        tri = arr(d.tri_vertices, nt * 3, ctypes.c_uint32)
-        tobj = arr(d.tri_object, nt, ctypes.c_uint32)
-        rank = arr(d.tri_rank, nt, ctypes.c_uint32)
-        ofv = arr(d.object_first_vertex, no + 1, ctypes.c_uint32)
-        mats = np.frombuffer(ctypes.string_at(d.materials, no * MAT_DTYPE.itemsize), dtype=MAT_DTYPE).copy()
-        exact = bool(N.lib.swr_host_scene_ranks_exact(h))
+        return _scene_data(h)
     finally:
         N.lib.swr_host_scene_free(h)
+
+
+def _scene_data(h):
+    """SceneData copied out of a loaded host scene."""
+    d = N.SceneDesc()
+    check(N.lib.swr_host_scene_desc(h, ctypes.byref(d)))
+    nv, nt, no = d.num_vertices, d.num_triangles, d.num_objects
+
+    def arr(p, n, dt):
+        return np.ctypeslib.as_array((dt * n).from_address(p)).copy()
+
+    vpos = arr(d.vertex_pos, nv * 3, ctypes.c_float)
+    vnrm = arr(d.vertex_normal, nv * 3, ctypes.c_float)
+    tri = arr(d.tri_vertices, nt * 3, ctypes.c_uint32)
+    tobj = arr(d.tri_object, nt, ctypes.c_uint32)
+    rank = arr(d.tri_rank, nt, ctypes.c_uint32)
+    ofv = arr(d.object_first_vertex, no + 1, ctypes.c_uint32)
+    mats = np.frombuffer(ctypes.string_at(d.materials, no * MAT_DTYPE.itemsize), dtype=MAT_DTYPE).copy()
+    exact = bool(N.lib.swr_host_scene_ranks_exact(h))
     return SceneData(vpos, vnrm, tri, tobj, ofv, mats, tri_rank=rank, ranks_exact=exact)
+
+
+def rotation_from_axis_angle(axis, angle):
+    """The quaternion (s, x, y, z) a scene file's rotation(x, y, z, angle) gives."""
+    a = (ctypes.c_float * 3)(*[float(x) for x in axis])
+    out = (ctypes.c_float * 4)()
+    check(N.lib.swr_rotation_from_axis_angle(a, float(angle), out))
+    return np.array(out[:], np.float32)
 
 
 def load_camera(camera_path, width, height, use_fov_key=False):
@@ -150,6 +163,39 @@ class Scene:
         o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius)
         self._h = ctypes.c_void_p()
         check(N.lib.swr_scene_create(ctypes.byref(d), ctypes.byref(o), ctypes.byref(self._h)))
+
+    @classmethod
+    def from_file(cls, scene_path, basepath, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0, builder="host",
+                  radius=0):
+        """Scene loaded from a scene file, keeping the object-space meshes on the device so that
+        set_transforms() can move its objects."""
+        h = ctypes.c_void_p()
+        check(N.lib.swr_host_scene_load(os.fsencode(scene_path), os.fsencode(basepath), ctypes.byref(h)))
+        self = cls.__new__(cls)
+        try:
+            self.data = _scene_data(h)
+            no = self.data.num_objects
+            xf = np.zeros((no, 10), np.float32)
+            check(N.lib.swr_host_scene_transforms(h, ptr(xf)))
+            b = {"host": N.BUILD_HOST, "device": N.BUILD_DEVICE}[builder]
+            o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius)
+            self._h = ctypes.c_void_p()
+            check(N.lib.swr_scene_create_from_host(h, ctypes.byref(o), ctypes.byref(self._h)))
+            self._xf = xf
+        finally:
+            N.lib.swr_host_scene_free(h)
+        return self
+
+    def transforms(self):
+        """Current object placements [num_objects, 10]: position xyz, scale xyz, rotation quaternion
+        (s, x, y, z); a scene made from SceneData has none."""
+        return None if getattr(self, "_xf", None) is None else self._xf.copy()
+
+    def set_transforms(self, xf, stream=None):
+        """Moves the objects of a scene made by from_file: xf [num_objects, 10] as transforms()."""
+        xf = np.ascontiguousarray(xf, dtype=np.float32).reshape(-1, 10)
+        check(N.lib.swr_scene_set_transforms(self._h, ptr(xf), xf.shape[0], _stream_handle(stream)))
+        self._xf = xf.copy()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -26,7 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp
 
 HOST_SRC = ["host/surface.cpp", "host/ref_bvh.cpp", "host/wide_bvh.cpp", "host/derive.cpp",
             "host/capi_host.cpp", "host/scene_pack.cpp"]
-CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu", "cuda/batch.cu", "cuda/build.cu", "cuda/rt.cu"]
+CUDA_SRC = ["cuda/scene.cu", "cuda/render.cu", "cuda/batch.cu", "cuda/build.cu", "cuda/rt.cu", "cuda/instance.cu"]
 CLI_SRC = {"SoftwareRenderer": "cli/swr_main.cpp", "RayTrace": "cli/rt_main.cpp"}
 
 

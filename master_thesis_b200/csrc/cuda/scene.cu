@@ -341,6 +341,7 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
 void swr_scene_destroy(swr_scene* s) {
   if (!s) return;
   swr::free_workspace(s);
+  swr::free_instance(s);
   for (void* p : {s->d_nodes, s->d_tris, s->d_shade, s->d_tri_boxes, s->d_obj_boxes, s->d_mats,
                   s->d_albedo, s->d_slot_of, s->d_scratch, s->d_lights, s->d_light_tris})
     if (p) cudaFree(p);

@@ -52,6 +52,7 @@ struct swr_scene {
   int num_sms = 0;
   std::vector<uint32_t> slot_to_id;  // host copy
   void* workspace = nullptr;          // render workspace (render.cu), grown on demand
+  void* instance = nullptr;           // object-space data for moving objects (instance.cu)
 };
 
 namespace swr {
@@ -70,5 +71,7 @@ bool is_host_pointer(const void* p);
 
 // releases the render workspace of a scene (render.cu)
 void free_workspace(swr_scene* s);
+// releases the object-space data of a scene made from a host scene (instance.cu)
+void free_instance(swr_scene* s);
 
 }  // namespace swr

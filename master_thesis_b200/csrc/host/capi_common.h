@@ -48,4 +48,23 @@ void parallel_for(size_t n, F f, unsigned threads = 0) {
 int validate_desc(const swr_scene_desc* d);
 void derive(const swr_scene_desc& d, Derived& out);
 
+// What a scene needs on the device to move its objects (swr_scene_set_transforms): the
+// object-space meshes, where each world vertex comes from, and each triangle's position in its
+// mesh's reference leaf order.
+struct InstanceSource {
+  std::vector<float> mesh_pos, mesh_nrm;       // [3 * mesh vertices] of all distinct meshes
+  std::vector<uint32_t> vert_src, vert_obj;    // per world vertex: mesh vertex, object
+  std::vector<uint32_t> obj_first_vertex;      // [objects + 1]
+  std::vector<uint32_t> obj_first_tri;         // [objects + 1]
+  std::vector<uint32_t> local_rank;            // per triangle id
+  std::vector<swr_object_transform> xf;        // placements as loaded
+  bool scene_order_exact = true;               // objects few enough for the reference's order
+};
+void instance_source(const swr_host_scene* hs, InstanceSource& out);
+// M = I * S * R * T of a placement (graphics_object.cpp:54-62), row-major m[i*4 + j].
+void object_matrix(const swr_object_transform& xf, float m[16]);
+// The reference's scene-level leaf order of objects from their boxes (lo.xyz hi.xyz each), or
+// the identity order when `exact` is false (too many objects for the reference's builder).
+std::vector<uint32_t> object_order(const float* boxes, uint32_t n, bool exact);
+
 }  // namespace swr

@@ -9,6 +9,7 @@
 
 #include "../../../include/swr.h"
 #include "capi_common.h"
+#include "ref_bvh.h"
 #include "surface.h"
 
 namespace swr {
@@ -83,6 +84,109 @@ int swr_host_scene_desc(const swr_host_scene* hs, swr_scene_desc* d) {
 int swr_host_scene_ranks_exact(const swr_host_scene* hs) { return hs && hs->s.ranks_exact ? 1 : 0; }
 
 void swr_host_scene_free(swr_host_scene* hs) { delete hs; }
+
+}  // extern "C"
+
+namespace swr {
+
+static swr_object_transform transform_of(const Object& o) {
+  swr_object_transform x;
+  for (int k = 0; k < 3; ++k) {
+    x.position[k] = o.position[k];
+    x.scale[k] = o.scl[k];
+  }
+  x.rotation[0] = o.rotation.s;
+  for (int k = 0; k < 3; ++k) x.rotation[1 + k] = o.rotation.v[k];
+  return x;
+}
+
+void instance_source(const swr_host_scene* hs, InstanceSource& out) {
+  const HostScene& s = hs->s;
+  const size_t no = s.objects.size();
+  std::vector<uint32_t> mesh_base(s.meshes.size(), 0);
+  uint32_t nmv = 0;
+  for (size_t m = 0; m < s.meshes.size(); ++m) {
+    mesh_base[m] = nmv;
+    nmv += (uint32_t)s.meshes[m].pos.size();
+  }
+  out.mesh_pos.resize((size_t)nmv * 3);
+  out.mesh_nrm.resize((size_t)nmv * 3);
+  for (size_t m = 0; m < s.meshes.size(); ++m)
+    for (size_t i = 0; i < s.meshes[m].pos.size(); ++i)
+      for (int k = 0; k < 3; ++k) {
+        out.mesh_pos[3 * (mesh_base[m] + i) + k] = s.meshes[m].pos[i][k];
+        out.mesh_nrm[3 * (mesh_base[m] + i) + k] = s.meshes[m].nrm[i][k];
+      }
+  out.vert_src.resize(s.vpos.size());
+  out.vert_obj.resize(s.vpos.size());
+  out.obj_first_vertex.assign(no + 1, 0);
+  out.obj_first_tri.assign(no + 1, 0);
+  out.local_rank.assign(s.num_tris(), 0);
+  out.xf.resize(no);
+  for (size_t o = 0; o < no; ++o) {
+    const Object& ob = s.objects[o];
+    const Mesh& m = s.meshes[ob.mesh_id];
+    for (uint32_t i = 0; i < ob.num_vertices; ++i) {
+      out.vert_src[ob.first_vertex + i] = mesh_base[ob.mesh_id] + i;
+      out.vert_obj[ob.first_vertex + i] = (uint32_t)o;
+    }
+    out.obj_first_vertex[o] = ob.first_vertex;
+    out.obj_first_tri[o] = ob.first_tri;
+    // rank = base of the object in the scene order + position in the mesh's leaf order
+    // (SceneBuilder::finish)
+    for (uint32_t k = 0; k < ob.num_tris; ++k) out.local_rank[ob.first_tri + (m.dfs.empty() ? k : m.dfs[k])] = k;
+    out.xf[o] = transform_of(ob);
+  }
+  out.obj_first_vertex[no] = (uint32_t)s.vpos.size();
+  out.obj_first_tri[no] = (uint32_t)s.num_tris();
+  out.scene_order_exact = no <= LoadOptions().max_exact_order;
+}
+
+void object_matrix(const swr_object_transform& xf, float out[16]) {
+  Rot r;
+  r.s = xf.rotation[0];
+  r.v = v3(xf.rotation[1], xf.rotation[2], xf.rotation[3]);
+  // M = I * S * R * T, each step a full matrix product (graphics_object.cpp:54-62)
+  M4 m = M4::identity();
+  m = matmul(m, scale_matrix(v3(xf.scale[0], xf.scale[1], xf.scale[2])));
+  m = matmul(m, r.matrix());
+  m = matmul(m, translation_matrix(v3(xf.position[0], xf.position[1], xf.position[2])));
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) out[4 * i + j] = m.m[i][j];
+}
+
+std::vector<uint32_t> object_order(const float* boxes, uint32_t n, bool exact) {
+  std::vector<uint32_t> order(n);
+  if (!exact) {
+    for (uint32_t o = 0; o < n; ++o) order[o] = o;
+    return order;
+  }
+  std::vector<Box> b(n);
+  for (uint32_t o = 0; o < n; ++o) {
+    b[o].empty = false;
+    b[o].lo = v3(boxes[6 * o], boxes[6 * o + 1], boxes[6 * o + 2]);
+    b[o].hi = v3(boxes[6 * o + 3], boxes[6 * o + 4], boxes[6 * o + 5]);
+  }
+  return ref_bvh_leaf_order(b);
+}
+
+}  // namespace swr
+
+extern "C" {
+
+int swr_rotation_from_axis_angle(const float axis[3], float angle, float out[4]) {
+  if (!axis || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  const swr::Rot r = swr::Rot::from_axis_angle(swr::v3(axis[0], axis[1], axis[2]), angle);
+  out[0] = r.s;
+  for (int k = 0; k < 3; ++k) out[1 + k] = r.v[k];
+  return SWR_OK;
+}
+
+int swr_host_scene_transforms(const swr_host_scene* hs, swr_object_transform* out) {
+  if (!hs || !out) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  for (size_t o = 0; o < hs->s.objects.size(); ++o) out[o] = swr::transform_of(hs->s.objects[o]);
+  return SWR_OK;
+}
 
 int swr_camera_load(const char* camera_path, uint32_t width, uint32_t height, uint32_t use_fov_key,
                     swr_camera* out) {
