@@ -445,6 +445,9 @@ int swr_rt_render_frame(swr_scene* scene, const swr_camera* cam, const swr_rt_op
  * and P6 PPM writer (graphics_engine.cpp:32-40). Host memory. */
 int swr_quantize_rgb8(const float* rgb, uint32_t width, uint32_t height, uint8_t* out);
 int swr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height);
+/* The same 8-bit RGB image as PNG (8-bit RGB, uncompressed deflate blocks); the thesis tooling
+ * converts the reference's PPM outputs to PNG for its comparisons. Host memory. */
+int swr_write_png(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height);
 
 #ifdef __cplusplus
 }

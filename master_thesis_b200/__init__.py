@@ -13,7 +13,7 @@ _EXPORTS = {
     "Scene": ".api", "SceneData": ".api", "Batch": ".api", "MAT_DTYPE": ".api", "camera_arrays": ".api",
     "load_camera": ".api", "make_camera": ".api", "load_renderer": ".api", "load_renderer_params": ".api",
     "load_scene": ".api", "quantize_rgb8": ".api", "rotation_from_axis_angle": ".api",
-    "write_ppm": ".api",
+    "write_ppm": ".api", "write_png": ".api",
 }
 
 __all__ = sorted(_EXPORTS)

@@ -195,6 +195,7 @@ SIGNATURES = {
                                 P, P]),
     "swr_quantize_rgb8": (I, [P, U32, U32, P]),
     "swr_write_ppm": (I, [ctypes.c_char_p, P, U32, U32]),
+    "swr_write_png": (I, [ctypes.c_char_p, P, U32, U32]),
 }
 
 

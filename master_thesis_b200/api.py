@@ -384,3 +384,9 @@ def write_ppm(path, rgb8):
     rgb8 = np.ascontiguousarray(rgb8, dtype=np.uint8)
     h, w = rgb8.shape[:2]
     check(N.lib.swr_write_ppm(os.fsencode(path), ptr(rgb8), w, h))
+
+
+def write_png(path, rgb8):
+    rgb8 = np.ascontiguousarray(rgb8, dtype=np.uint8)
+    h, w = rgb8.shape[:2]
+    check(N.lib.swr_write_png(os.fsencode(path), ptr(rgb8), w, h))

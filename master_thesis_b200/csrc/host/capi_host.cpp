@@ -1,11 +1,13 @@
 // Host-side half of the C ABI: error reporting, the file surface, derived triangle data and
 // image output. No CUDA here.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../../include/swr.h"
 #include "capi_common.h"
@@ -366,6 +368,90 @@ int swr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t width, uint32_
   if (!f) return set_error(SWR_ERR_IO, std::string("swr: cannot write \"") + path + "\"");
   f << "P6\n" << width << "\n" << height << "\n" << 255u << "\n";
   f.write((const char*)rgb8, (std::streamsize)width * height * 3);
+  return f ? SWR_OK : set_error(SWR_ERR_IO, std::string("swr: write failed \"") + path + "\"");
+}
+
+}  // extern "C"
+
+namespace {
+
+// CRC-32 (ISO 3309 / ITU-T V.42 polynomial 0xEDB88320, reflected), as PNG chunks use it
+uint32_t crc32_png(const uint8_t* p, size_t n, uint32_t c = 0xFFFFFFFFu) {
+  static uint32_t table[256];
+  static bool init = false;
+  if (!init) {
+    for (uint32_t i = 0; i < 256; ++i) {
+      uint32_t x = i;
+      for (int k = 0; k < 8; ++k) x = (x & 1u) ? (0xEDB88320u ^ (x >> 1)) : (x >> 1);
+      table[i] = x;
+    }
+    init = true;
+  }
+  for (size_t i = 0; i < n; ++i) c = table[(c ^ p[i]) & 0xFFu] ^ (c >> 8);
+  return c;
+}
+
+void put32(std::vector<uint8_t>& v, uint32_t x) {
+  v.push_back((uint8_t)(x >> 24));
+  v.push_back((uint8_t)(x >> 16));
+  v.push_back((uint8_t)(x >> 8));
+  v.push_back((uint8_t)x);
+}
+
+void chunk(std::vector<uint8_t>& out, const char* type, const std::vector<uint8_t>& data) {
+  put32(out, (uint32_t)data.size());
+  const size_t start = out.size();
+  out.insert(out.end(), type, type + 4);
+  out.insert(out.end(), data.begin(), data.end());
+  put32(out, crc32_png(out.data() + start, out.size() - start) ^ 0xFFFFFFFFu);
+}
+
+}  // namespace
+
+extern "C" {
+
+// PNG (RFC 2083): 8-bit RGB, filter 0 on every row, the image data as a zlib stream (RFC 1950)
+// of stored deflate blocks (RFC 1951 BTYPE 00) with its Adler-32; no compression library needed.
+int swr_write_png(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height) {
+  if (!path || !rgb8) return set_error(SWR_ERR_INVALID, "swr: null argument");
+  if (width == 0 || height == 0 || width > (1u << 24) || height > (1u << 24))
+    return set_error(SWR_ERR_INVALID, "swr: bad PNG image size");
+  std::vector<uint8_t> raw;
+  raw.reserve((size_t)height * (1 + (size_t)width * 3));
+  for (uint32_t y = 0; y < height; ++y) {
+    raw.push_back(0);  // filter type None
+    raw.insert(raw.end(), rgb8 + (size_t)y * width * 3, rgb8 + (size_t)(y + 1) * width * 3);
+  }
+  std::vector<uint8_t> z{0x78, 0x01};
+  for (size_t off = 0; off < raw.size() || off == 0;) {
+    const size_t n = std::min<size_t>(65535, raw.size() - off);
+    const bool last = off + n >= raw.size();
+    z.push_back(last ? 1 : 0);
+    z.push_back((uint8_t)n);
+    z.push_back((uint8_t)(n >> 8));
+    z.push_back((uint8_t)~n);
+    z.push_back((uint8_t)(~n >> 8));
+    z.insert(z.end(), raw.begin() + off, raw.begin() + off + n);
+    off += n;
+    if (last) break;
+  }
+  uint32_t a = 1, b = 0;  // Adler-32
+  for (uint8_t c : raw) {
+    a = (a + c) % 65521u;
+    b = (b + a) % 65521u;
+  }
+  put32(z, (b << 16) | a);
+  std::vector<uint8_t> png{0x89, 'P', 'N', 'G', 0x0D, 0x0A, 0x1A, 0x0A};
+  std::vector<uint8_t> ihdr;
+  put32(ihdr, width);
+  put32(ihdr, height);
+  ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});  // 8 bits, RGB, deflate, adaptive filters, no interlace
+  chunk(png, "IHDR", ihdr);
+  chunk(png, "IDAT", z);
+  chunk(png, "IEND", {});
+  std::ofstream f(path, std::ios::out | std::ios::binary);
+  if (!f) return set_error(SWR_ERR_IO, std::string("swr: cannot write \"") + path + "\"");
+  f.write((const char*)png.data(), (std::streamsize)png.size());
   return f ? SWR_OK : set_error(SWR_ERR_IO, std::string("swr: write failed \"") + path + "\"");
 }
 

@@ -237,3 +237,30 @@ def test_quantize_and_ppm(tmp_path):
     p = tmp_path / "o.ppm"
     swr.write_ppm(str(p), q)
     assert p.read_bytes() == b"P6\n2\n1\n255\n" + q.tobytes()
+
+
+@pytest.mark.parametrize("W,H", [(1, 1), (7, 3), (300, 257)])
+def test_png_writer_round_trip(tmp_path, W, H):
+    """PNG output (RFC 2083): chunk CRCs, the zlib stream and every pixel read back with the
+    standard zlib and PIL decoders."""
+    import struct
+    import zlib
+    rgb = np.random.default_rng(W * H).integers(0, 256, (H, W, 3), dtype=np.uint8)
+    p = tmp_path / "img.png"
+    swr.write_png(str(p), rgb)
+    data = p.read_bytes()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    off, chunks = 8, []
+    while off < len(data):
+        n, = struct.unpack(">I", data[off:off + 4])
+        typ, body = data[off + 4:off + 8], data[off + 8:off + 8 + n]
+        crc, = struct.unpack(">I", data[off + 8 + n:off + 12 + n])
+        assert zlib.crc32(typ + body) == crc
+        chunks.append((typ, body))
+        off += 12 + n
+    assert [c[0] for c in chunks] == [b"IHDR", b"IDAT", b"IEND"]
+    assert struct.unpack(">IIBBBBB", chunks[0][1]) == (W, H, 8, 2, 0, 0, 0)
+    raw = np.frombuffer(zlib.decompress(chunks[1][1]), np.uint8).reshape(H, 1 + W * 3)
+    assert np.all(raw[:, 0] == 0) and np.array_equal(raw[:, 1:].reshape(H, W, 3), rgb)
+    from PIL import Image
+    assert np.array_equal(np.asarray(Image.open(p).convert("RGB")), rgb)
