@@ -50,8 +50,7 @@ CONFIGS = {
     "c3s": dict(kind="batch", scenes=256, depth=6, seed=7, sides=[64, 128], spps=[4, 16], tris=[1e3, 5e4]),
     # the RayTrace program's PathTracer (Vulkan shaders restated in CUDA) with its own renderer file
     # settings (res/renderer/path_tracer.renderer: visionJumpCount 5, visionRayPerPixelCount 13) on
-    # the Cornell scene at 1920x1080, and on the terrain scene (no CPU baseline: the oracle's closest
-    # hit tests every triangle)
+    # the Cornell scene at 1920x1080, and on the terrain scene
     # (launch shape: refill / shading batch / blocks per SM measured best per scene)
     "c6": dict(kind="cornell", renderer="rt", W=1920, H=1080, spp=13, depth=5, seed=1, refill=4, shade_batch=16,
                blocks_per_sm=6),
@@ -405,7 +404,7 @@ def run_rt(args, cfg, files, workload):
     clk = clocks.stop()
     samples = W * H * spp
     cpu = None
-    if not args.no_cpu_baseline and cfg["kind"] == "cornell":
+    if not args.no_cpu_baseline:
         nproc = os.cpu_count() or 1
         r = rt_cpu_port(cfg, files, nproc, args.cpu_budget)
         cpu = {"value": r["msamples_per_s"], "unit": "Msamples/s", "cores": nproc, "kind": "port",
@@ -737,11 +736,6 @@ def main():
         # the RayTrace program's shaders need a Vulkan ray tracing pipeline, which this machine
         # cannot bring up: its CPU restatement (the oracle) stands in as the reference arm
         if rank != 0:
-            return
-        if cfg["kind"] != "cornell":
-            print(json.dumps({"impl": "reference", "unavailable": "the reference's shaders need a Vulkan ray "
-                                                                  "tracing pipeline (unavailable on this box); the "
-                                                                  "CPU restatement tests every triangle"}))
             return
         r = rt_cpu_port(cfg, files, nproc, args.cpu_budget * max(1, args.steps // 5))
         v = r["msamples_per_s"]

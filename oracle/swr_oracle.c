@@ -888,24 +888,56 @@ void swo_adjoint_physical64(const swo_scene* s, const swo_camera* cam, uint32_t 
  * the choice fixed here (and by the library) is: IEEE float division and sqrt, the double
  * sin/cos/acos of the widened argument rounded to float, normalize(v) = v / sqrt(dot(v, v)),
  * no fused multiply-adds. The closest hit uses the Moller-Trumbore arithmetic above with t in
- * [0.001, 10000] and ties to the lower triangle id, found by testing every triangle. Parity with
+ * [0.001, 10000] and ties to the lower triangle id, found by testing every triangle of every
+ * object whose widened box the ray meets. Parity with
  * the shaders on a GPU ray tracing pipeline cannot be checked here (no graphics stack), so this
  * restatement is pinned only by its own known-answer tests. */
 
 static const float RT_PI = 3.1415926538f;
 
+/* Culling only: does the ray (t >= 0) pass through the object box widened by a margin far above
+ * any float rounding of the intersection test? Evaluated in double; a miss here means no
+ * triangle of the object can be accepted. */
+static int rt_box_maybe(const float* box, v3f o, v3f d) {
+  const double ov[3] = {o.x, o.y, o.z}, dv[3] = {d.x, d.y, d.z};
+  double tmin = 0.0, tmax = INFINITY, m = 1.0;
+  int i;
+  for (i = 0; i < 6; ++i) m = fmax(m, fabs((double)box[i]));
+  m *= 1e-3;
+  for (i = 0; i < 3; ++i) {
+    const double lo = (double)box[i] - m, hi = (double)box[3 + i] + m;
+    if (dv[i] == 0.0) {
+      if (ov[i] < lo || ov[i] > hi) return 0;
+    } else {
+      double t1 = (lo - ov[i]) / dv[i], t2 = (hi - ov[i]) / dv[i];
+      if (t1 > t2) {
+        const double x = t1;
+        t1 = t2;
+        t2 = x;
+      }
+      tmin = fmax(tmin, t1);
+      tmax = fmin(tmax, t2);
+    }
+  }
+  return tmin <= tmax;
+}
+
 static uint32_t rt_closest(const swo_scene* s, v3f o, v3f d, float* t_out) {
   float bt = INFINITY;
-  uint32_t bi = 0xFFFFFFFFu, k;
-  for (k = 0; k < s->ntri; ++k) {
-    float t, d2;
-    if (!ref_intersect(o, d, ld3(s->v0 + 3 * (size_t)k), ld3(s->e0 + 3 * (size_t)k),
-                       ld3(s->e1 + 3 * (size_t)k), &t, &d2))
-      continue;
-    if (!(t >= 0.001f && t <= 10000.0f)) continue;
-    if (t < bt) { /* increasing ids: a tie keeps the lower id */
-      bt = t;
-      bi = k;
+  uint32_t bi = 0xFFFFFFFFu, k, obj;
+  for (obj = 0; obj < s->nobj; ++obj) {
+    if (!rt_box_maybe(s->obj_box + 6 * (size_t)obj, o, d)) continue;
+    /* objects in order and triangles in id order: a tie keeps the lower id */
+    for (k = s->obj_first[obj]; k < s->obj_first[obj + 1]; ++k) {
+      float t, d2;
+      if (!ref_intersect(o, d, ld3(s->v0 + 3 * (size_t)k), ld3(s->e0 + 3 * (size_t)k),
+                         ld3(s->e1 + 3 * (size_t)k), &t, &d2))
+        continue;
+      if (!(t >= 0.001f && t <= 10000.0f)) continue;
+      if (t < bt) {
+        bt = t;
+        bi = k;
+      }
     }
   }
   *t_out = bt;

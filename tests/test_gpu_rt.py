@@ -175,3 +175,26 @@ def test_gpu_raytrace_cli(tmp_path):
     _, img = O.rt_render(O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org), W, H, 6, 5)
     want = O.rt_denoise_median(img.reshape(H, W, 4))[..., :3]
     assert np.mean(np.all(got == want, axis=2)) > 0.97
+
+
+def test_gpu_rt_on_a_terrain_matches_oracle(tmp_path):
+    """A deep tree (a 256^2-cell terrain in 256 tiles, spheres, lights): ray-query hits on random
+    rays and a small frame against the oracle."""
+    s = scenes.terrain(6, str(tmp_path), cells=256, tile=16, spheres=16, sphere_subdiv=3, lights=3)
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    sc = swr.Scene(sd)
+    osc = O.OracleScene.from_scene_data(sd)
+    ro, rd = rays_uniform(20000, sd.vpos.min(0) - 0.05, sd.vpos.max(0) + 0.05, seed=8)
+    hits = rt.trace(sc, torch.from_numpy(ro).cuda(), torch.from_numpy(rd).cuda()).cpu().numpy().view(np.uint32)
+    otri, ot = O.rt_trace(osc, ro, rd)
+    assert np.array_equal(hits[:, 0], otri)
+    m = otri != 0xFFFFFFFF
+    assert np.array_equal(hits[m, 3], ot[m].view(np.uint32)) and m.mean() > 0.2
+    W, H, spp, vj = 48, 27, 4, 5
+    cam = swr.load_camera(s["camera"], W, H)
+    vi, pi, org = swr.camera_arrays(cam)
+    rgb, rgba = rt.render(sc, cam, W, H, spp, vj)
+    torch.cuda.synchronize()
+    want_rgb, want_rgba = O.rt_render(osc, O.camera(vi, pi, org), W, H, spp, vj)
+    assert _close(rgb.cpu().numpy().reshape(-1, 3), want_rgb)
+    assert np.mean(np.all(rgba.cpu().numpy().reshape(-1, 4) == want_rgba, axis=1)) > 0.99
