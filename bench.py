@@ -889,7 +889,7 @@ def main():
     launches_total = sum(p["launches"] for p in plain)
 
     if rank == 0:
-        cpu = None
+        cpu = cpu_shim = None
         if not args.no_cpu_baseline:
             from oracle import refdump
             if os.path.exists(refdump.REF_BENCH):
@@ -901,6 +901,17 @@ def main():
                 except Exception as ex:  # the baseline is reported, never required
                     cpu = {"value": None, "unit": "Msamples/s", "cores": nproc, "kind": "reference",
                            "sample": "failed: %s" % str(ex)[:200]}
+            if os.path.exists(refdump.REF_BENCH_SHIM):
+                # second row: the reference's path with the lock-free Philox shim instead of its
+                # mutex-guarded generator
+                try:
+                    r = cpu_reference(cfg, files, nproc, args.cpu_budget / 2, refdump.REF_BENCH_SHIM)
+                    cpu_shim = {"value": r["msamples_per_s"], "unit": "Msamples/s", "cores": nproc,
+                                "kind": "reference (lock-free Philox RNG shim)",
+                                "sample": "%d of %d pixels (every k-th), %d spp, depth %d"
+                                          % (r["pixels"], W * H, spp, depth)}
+                except Exception as ex:
+                    cpu_shim = {"value": None, "sample": "failed: %s" % str(ex)[:200]}
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -929,6 +940,7 @@ def main():
             "gpu_launches": int(launches_total),
             "clocks": clk,
             "cpu_baseline": cpu,
+            "cpu_baseline_rng_shim": cpu_shim,
             "setup_s": {"load": t1 - t0, "build_upload": t2 - t1, "build_upload_device_builder": t4 - t3},
         }
         print(json.dumps(line))

@@ -9,6 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 HARNESS = os.path.join(REF_DIR, "ref_harness")
 REF_BENCH = os.path.join(REF_DIR, "ref_bench")
+REF_BENCH_SHIM = os.path.join(REF_DIR, "ref_bench_shim")
 REF_CLI = os.path.join(REF_DIR, "SoftwareRenderer")
 
 _KINDS = {"f": np.float32, "u": np.uint32}
