@@ -1,6 +1,12 @@
 /* swr.h - C ABI of the B200 path tracer (drop-in for vikkre/master_thesis's SoftwareRenderer
  * PathTracer path).
  *
+ * Parts: the file surface (scene, mesh, camera and renderer files), scene creation with a host or
+ * device BVH build, closest-hit queries, the PathTracer render (reference and physical modes),
+ * the BidirectionalPathTracer, batched and differentiable (adjoint) rendering, moving objects
+ * (GPU transforms and BVH refit), the Vulkan program's PathTracer and denoisers restated in
+ * CUDA, and PPM/PNG output.
+ *
  * Conventions
  *  - Every call returns an int status: SWR_OK (0) or one of the SWR_ERR_* codes. No C++ exception
  *    crosses this boundary. swr_last_error() returns a thread-local "system: message" string for
@@ -247,7 +253,8 @@ typedef struct swr_bdpt_opts {
   uint32_t max_depth;
   uint32_t shade_batch;  /* lanes of a warp with a finished trace that advance together (1..32), 0 =
                             the library's choice */
-  uint32_t reserved;
+  uint32_t blocks_per_sm;  /* resident blocks per SM targeted by the register budget: 0 (compiler's
+                              choice), 5, 6 or 8 */
 } swr_bdpt_opts;
 int swr_render_bdpt(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
                     const swr_bdpt_opts* bdpt, float* rgb_out, float* samples_out, void* stream);

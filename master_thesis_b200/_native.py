@@ -97,7 +97,7 @@ class BatchOpts(ctypes.Structure):
 
 class BdptOpts(ctypes.Structure):
     _fields_ = [("light_jumps", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("shade_batch", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("blocks_per_sm", ctypes.c_uint32)]
 
 
 class RendererParams(ctypes.Structure):

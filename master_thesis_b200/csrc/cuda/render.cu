@@ -448,7 +448,8 @@ struct BdptArgs {
 
 enum BdptPhase : uint32_t { kVision = 0, kVisionDone = 1, kLight = 2, kConnectNext = 3, kConnectResult = 4 };
 
-__global__ void __launch_bounds__(kTraceBlock)
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     k_bdpt(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, BdptArgs B) {
   __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
   const unsigned lane = lane_id();
@@ -1061,6 +1062,8 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   if ((uint64_t)o->width * o->height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
   if (b->shade_batch > 32) return set_error(SWR_ERR_INVALID, "swr: shade_batch must be 0..32");
+  if (b->blocks_per_sm != 0 && b->blocks_per_sm != 5 && b->blocks_per_sm != 6 && b->blocks_per_sm != 8)
+    return set_error(SWR_ERR_INVALID, "swr: blocks_per_sm must be 0, 5, 6 or 8");
   if (s->dev.num_lights == 0)
     return set_error(SWR_ERR_INVALID, "swr: the bidirectional tracer needs a light source in the scene");
   const bool want_samples = (o->flags & SWR_RENDER_SAMPLES_OUT) != 0;
@@ -1106,8 +1109,12 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   B.lj = b->light_jumps;
   B.md = b->max_depth;
   B.batch = b->shade_batch ? b->shade_batch : kBdptBatch;
+  auto kern = k_bdpt<0>;
+  if (b->blocks_per_sm == 5) kern = k_bdpt<5>;
+  else if (b->blocks_per_sm == 6) kern = k_bdpt<6>;
+  else if (b->blocks_per_sm == 8) kern = k_bdpt<8>;
   int per_sm = 0;
-  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bdpt, kTraceBlock, 0));
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceBlock, 0));
   const unsigned grid = (unsigned)(s->num_sms * std::max(per_sm, 1));
   for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
     const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
@@ -1120,7 +1127,7 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
     *ws->host_ctrl = init;
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
     k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
-    k_bdpt<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
+    kern<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
     k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
     SWR_CUDA(cudaGetLastError());
     if (want_samples)
