@@ -251,8 +251,9 @@ int swr_render_profiled(swr_scene* scene, const swr_camera* cam, const swr_rende
 typedef struct swr_bdpt_opts {
   uint32_t light_jumps;
   uint32_t max_depth;
-  uint32_t shade_batch;  /* lanes of a warp with a finished trace that advance together (1..32), 0 =
-                            the library's choice */
+  uint32_t shade_batch;  /* lanes of a warp with a finished trace that advance together, bits 0-7
+                            for the path stages and bits 8-15 for the connection queries (each
+                            1..32, 0 = the library's choice) */
   uint32_t blocks_per_sm;  /* resident blocks per SM targeted by the register budget: 0 (compiler's
                               choice), 5, 6 or 8 */
 } swr_bdpt_opts;

@@ -426,44 +426,65 @@ __global__ void __launch_bounds__(kTraceBlock)
 // ---------------------------------------------------------------------------------------------
 // Bidirectional path tracer (BidirectionalPathTracer, bidirectional_path_tracer.cpp:20-168).
 //
-// Each lane carries one camera sample through the reference's three stages: the vision path
-// (starting from the per-pixel camera record, which already holds the back-face-skipping prefix
-// and the first front hit), a light subpath from a sampled point on a light source, and the
-// connections of every vision vertex with every light vertex (vi + li <= maxDepth) through
-// occlusion queries (Scene::isOccluded, scene.cpp:58-83). Every trace, closest hit or occlusion,
-// is the resumable Traversal, so lanes in different stages share the traversal loop; a lane that
-// finishes a sample takes a new one. Random numbers: the sample's k-th draw of the reference
-// (one per scattering vertex, four for the light point) is Philox vertex k of the sample.
-// The vision slots of the skipped prefix hold the reference's zero-initialised hit points: their
-// connections add exactly zero, so their occlusion queries are not run.
+// Two persistent kernels per chunk of samples, each lane carrying one sample at a time:
+//   k_bdpt_paths    the reference's first two stages: the vision path (starting from the
+//                   per-pixel camera record, which already holds the back-face-skipping prefix and
+//                   the first front hit) and a light subpath from a sampled point on a light
+//                   source; every recorded vertex (point, normal, throughput) goes to a per-sample
+//                   slot table in device memory.
+//   k_bdpt_connect  the connections of every vision vertex with every light vertex
+//                   (vi + li <= maxDepth) through occlusion queries (Scene::isOccluded,
+//                   scene.cpp:58-83), summed in the reference's order.
+// Splitting the stages keeps each kernel's lanes on the same code (path tracing, or occlusion
+// queries) and the vertex tables out of registers and local memory. Every trace is the resumable
+// Traversal; lanes whose trace finished wait until B.batch of them can run their stage code
+// together. Random numbers: the sample's k-th draw of the reference (one per scattering vertex,
+// four for the light point) is Philox vertex k of the sample. The vision slots of the skipped
+// prefix hold the reference's zero-initialised hit points: their connections add exactly zero,
+// so their occlusion queries are not run.
 constexpr int kBdptMax = 16;
 // measured on the Cornell BDPT image (256x256x16, 5/5/5): batch 1 / 8 / 16 / 20 / 24 ->
 // 5.84 / 4.62 / 4.23 / 3.95 / 3.95 ms at refill 4 (identical images)
 constexpr uint32_t kBdptBatch = 20;
+constexpr uint32_t kConnectBatch = 16;
+constexpr uint64_t kBdptChunkSamples = 1ull << 20;
 
 struct BdptArgs {
   uint32_t vj, lj, md;
-  uint32_t batch;  // lanes of a warp whose trace finished that advance their samples together
+  uint32_t batch;     // lanes of a warp whose trace finished that advance their samples together
+  uint32_t cbatch;    // the same for the connection queries
+  uint32_t nsamp;     // samples of the chunk (pixels x spp)
+  float4* vtx;        // [3 * 2 * kBdptMax * nsamp]: point, normal, throughput of vertex slot k of
+                      // sample q at (3k + field) * nsamp + q; vision vertex i is slot i, light
+                      // vertex i slot kBdptMax + i
+  uint4* head;        // [nsamp] first vision slot, vision end, light count, 1 = already resolved
 };
 
-enum BdptPhase : uint32_t { kVision = 0, kVisionDone = 1, kLight = 2, kConnectNext = 3, kConnectResult = 4 };
+enum BdptPhase : uint32_t { kVision = 0, kVisionDone = 1, kLight = 2 };
+
+__device__ __forceinline__ void bd_put(const BdptArgs& B, uint32_t slot, uint32_t q, f3 p, f3 n, f3 c) {
+  B.vtx[(size_t)(3 * slot + 0) * B.nsamp + q] = make_float4(p.x, p.y, p.z, 0.0f);
+  B.vtx[(size_t)(3 * slot + 1) * B.nsamp + q] = make_float4(n.x, n.y, n.z, 0.0f);
+  B.vtx[(size_t)(3 * slot + 2) * B.nsamp + q] = make_float4(c.x, c.y, c.z, 0.0f);
+}
+__device__ __forceinline__ f3 bd_get(const BdptArgs& B, uint32_t slot, uint32_t field, uint32_t q) {
+  const float4 v = __ldg(B.vtx + (size_t)(3 * slot + field) * B.nsamp + q);
+  return mk(v.x, v.y, v.z);
+}
 
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
-    k_bdpt(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, BdptArgs B) {
+    k_bdpt_paths(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, BdptArgs B) {
   __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
   const unsigned lane = lane_id();
   const unsigned lt = (1u << lane) - 1u;
   const unsigned long long total = ctrl->total;
   swrx::Traversal tr;
-  f3 vpos[kBdptMax], vnrm[kBdptMax], vcol[kBdptMax];
-  f3 lpos[kBdptMax], lnrm[kBdptMax], lcol[kBdptMax];
-  uint32_t pixel = 0, sample = 0, phase = kVision, i = 0, draws = 0, vfirst = 0, dv = 0, dl = 0, vi = 0, li = 0;
+  uint32_t pixel = 0, sample = 0, phase = kVision, i = 0, draws = 0, vfirst = 0, dv = 0, dl = 0;
   bool active = false, tracing = false, exhausted = false, vlight = false;
-  f3 o = mk(0, 0, 0), d = mk(0, 0, 0), c = mk(1, 1, 1), acc = mk(0, 0, 0), dn = mk(0, 0, 0);
+  f3 o = mk(0, 0, 0), d = mk(0, 0, 0), c = mk(1, 1, 1);
   uint32_t hslot = 0;
   float ht = 0.0f;
-  const float inv_md = 1.0f / (float)B.md;
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
@@ -481,6 +502,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
           const uint32_t bits = __float_as_uint(r1.w);
           if (bits == kDeadSlot) {  // no front hit within visionJumpCount: the sample adds nothing
             F.contrib[(size_t)pixel * F.spp + sample] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            B.head[(size_t)pixel * F.spp + sample] = make_uint4(0u, 0u, 0u, 1u);
           } else {
             o = mk(r0.x, r0.y, r0.z);
             d = mk(r1.x, r1.y, r1.z);
@@ -515,15 +537,18 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     if (waiting == 0u || ((unsigned)__popc(waiting) < B.batch && inflight != 0u)) continue;
     if (!active || tracing) continue;
     const uint32_t gpix = F.pixel0 + pixel;
+    const uint32_t q = pixel * F.spp + sample;
     // advance the sample until it needs a trace or is finished
     while (active && !tracing) {
       if (phase == kVision || phase == kLight) {
         const bool vision = phase == kVision;
         if (hslot == 0xFFFFFFFFu) {
-          phase = vision ? (uint32_t)kVisionDone : (uint32_t)kConnectNext;
-          vi = vfirst;
-          li = 0;
-          acc = mk(0.0f, 0.0f, 0.0f);
+          if (vision) {
+            phase = kVisionDone;
+          } else {  // the light subpath left the scene: its vertices so far go to the connections
+            B.head[q] = make_uint4(vfirst, dv, dl, 0u);
+            active = false;
+          }
           continue;
         }
         const f3 p = swrx::hit_point(o, d, ht);
@@ -545,15 +570,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
           const float cs = swrx::vdot(n, vision ? nd : prev);
           c = swrx::vmul(c, mk(__fmul_rn(m.m0.x, cs), __fmul_rn(m.m0.y, cs), __fmul_rn(m.m0.z, cs)));
         }
-        if (vision) {
-          vpos[i] = p;
-          vnrm[i] = n;
-          vcol[i] = c;
-        } else {
-          lpos[i] = p;
-          lnrm[i] = n;
-          lcol[i] = c;
-        }
+        bd_put(B, (vision ? 0u : (uint32_t)kBdptMax) + i, q, p, n, c);
         const bool light_hit = __float_as_uint(m.m1.w) != 0u && swrx::vdot(n, prev) <= 0.0f;
         ++i;
         if (light_hit || i >= (vision ? B.vj : B.lj)) {
@@ -561,18 +578,17 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
             vlight = light_hit;
             phase = kVisionDone;
           } else {
-            phase = kConnectNext;
-            vi = vfirst;
-            li = 0;
-            acc = mk(0.0f, 0.0f, 0.0f);
+            B.head[q] = make_uint4(vfirst, dv, dl, 0u);
+            active = false;
           }
           continue;
         }
         tr.init(o, d, stack + threadIdx.x, kTraceBlock);
         tracing = true;
       } else if (phase == kVisionDone) {
-        if (vlight) {
-          F.contrib[(size_t)pixel * F.spp + sample] = make_float4(vcol[dv - 1].x, vcol[dv - 1].y, vcol[dv - 1].z, 1.0f);
+        if (vlight) {  // c is the throughput recorded at the last vision vertex
+          F.contrib[(size_t)pixel * F.spp + sample] = make_float4(c.x, c.y, c.z, 1.0f);
+          B.head[q] = make_uint4(0u, 0u, 0u, 1u);
           active = false;
           continue;
         }
@@ -589,8 +605,8 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
         uint32_t ti = __float2uint_rz(__fmul_rn(U.u[0], (float)L.y));
         ti = min(ti, L.y - 1u);
         const float b0 = __fsub_rn(1.0f, sr1), b1 = __fmul_rn(sr1, __fsub_rn(1.0f, r2)), b2 = __fmul_rn(sr1, r2);
-        const float4* q = sc.light_tris + 5 * (size_t)(L.x + ti);
-        const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        const float4* lq = sc.light_tris + 5 * (size_t)(L.x + ti);
+        const float4 q0 = __ldg(lq), q1 = __ldg(lq + 1), q2 = __ldg(lq + 2), q3 = __ldg(lq + 3), q4 = __ldg(lq + 4);
         const f3 v0 = mk(q0.x, q0.y, q0.z), v1 = mk(q0.w, q1.x, q1.y), v2 = mk(q1.z, q1.w, q2.x);
         const f3 n0 = mk(q2.y, q2.z, q2.w), n1 = mk(q3.x, q3.y, q3.z), n2 = mk(q3.w, q4.x, q4.y);
         const f3 lp = swrx::vadd(swrx::vadd(swrx::vscale(b0, v0), swrx::vscale(b1, v1)), swrx::vscale(b2, v2));
@@ -599,9 +615,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
         ln = swrx::vadd(ln, swrx::vscale(b2, n2));
         ln = swrx::vnormalize(ln);
         const float4 lc = __ldg(sc.mats + 3 * (size_t)L.z);
-        lpos[0] = lp;
-        lnrm[0] = ln;
-        lcol[0] = mk(lc.x, lc.y, lc.z);
+        bd_put(B, (uint32_t)kBdptMax, q, lp, ln, mk(lc.x, lc.y, lc.z));
         o = lp;
         d = swrx::hemisphere_dir(ln, U.u[1], U.u[2]);
         c = mk(1.0f, 1.0f, 1.0f);
@@ -611,45 +625,106 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
           tr.init(o, d, stack + threadIdx.x, kTraceBlock);
           tracing = true;
         } else {
-          phase = kConnectNext;
-          vi = vfirst;
-          li = 0;
-          acc = mk(0.0f, 0.0f, 0.0f);
-        }
-      } else if (phase == kConnectNext) {
-        if (vi >= dv) {
-          const f3 r = swrx::vscale(inv_md, acc);
-          F.contrib[(size_t)pixel * F.spp + sample] = make_float4(r.x, r.y, r.z, 1.0f);
+          B.head[q] = make_uint4(vfirst, dv, dl, 0u);
           active = false;
-          continue;
         }
-        if (li >= dl) {
-          ++vi;
-          li = 0;
-          continue;
-        }
-        if (vi + li > B.md) {
-          ++li;
-          continue;
-        }
-        const f3 a = swrx::vadd(vpos[vi], swrx::vscale(0.01f, vnrm[vi]));
-        const f3 b = swrx::vadd(lpos[li], swrx::vscale(0.01f, lnrm[li]));
-        const f3 dd = swrx::vsub(b, a);
-        const float dist2 = swrx::vdot(dd, dd);
-        dn = swrx::vnormalize(dd);
-        tr.init_occlusion(a, dn, dist2, stack + threadIdx.x, kTraceBlock);
-        tracing = true;
-        phase = kConnectResult;
-      } else {  // kConnectResult
-        if (hslot == 0xFFFFFFFFu) {  // not occluded
-          const float cs = swrx::vdot(dn, vnrm[vi]);
-          const f3 vc = vcol[vi], lc = lcol[li];
-          acc = swrx::vadd(acc, mk(__fmul_rn(__fmul_rn(vc.x, lc.x), cs), __fmul_rn(__fmul_rn(vc.y, lc.y), cs),
-                                   __fmul_rn(__fmul_rn(vc.z, lc.z), cs)));
-        }
-        ++li;
-        phase = kConnectNext;
       }
+    }
+  }
+}
+
+
+// Connections of one sample (bidirectional_path_tracer.cpp:70-96): for vi from the first vision
+// slot, for li from 0, every pair with vi + li <= maxDepth is joined by an occlusion query between
+// the two points lifted by 0.01 along their normals; an unoccluded pair adds
+// (vision throughput * light throughput) * cos at the vision vertex. The sum, in that order, is
+// divided by maxDepth.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
+    k_bdpt_connect(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, BdptArgs B) {
+  __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned long long total = B.nsamp;
+  swrx::Traversal tr;
+  uint32_t q = 0, vi = 0, li = 0, dv = 0, dl = 0;
+  bool active = false, tracing = false, exhausted = false, pending = false;
+  f3 acc = mk(0.0f, 0.0f, 0.0f), dn = mk(0.0f, 0.0f, 0.0f);
+  const float inv_md = 1.0f / (float)B.md;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
+      unsigned long long base = 0;
+      // inj_base[1] serves as the sample cursor of the connection launch
+      if (lane == 0) base = atomicAdd(&ctrl->inj_base[1], (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) exhausted = true;
+      if (!active) {
+        const unsigned long long g = base + __popc(idle & lt);
+        if (g < total) {
+          const uint4 h = B.head[g];
+          if (h.w == 0u) {
+            q = (uint32_t)g;
+            vi = h.x;
+            dv = h.y;
+            dl = h.z;
+            li = 0;
+            acc = mk(0.0f, 0.0f, 0.0f);
+            pending = false;
+            tracing = false;
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active && tracing && tr.step<false, false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, nullptr))
+      tracing = false;
+    const unsigned waiting = __ballot_sync(0xffffffffu, active && !tracing);
+    const unsigned inflight = __ballot_sync(0xffffffffu, active && tracing);
+    if (waiting == 0u || ((unsigned)__popc(waiting) < B.cbatch && inflight != 0u)) continue;
+    if (!active || tracing) continue;
+    if (pending) {  // the query of pair (vi, li) is answered
+      if (tr.hit.slot == 0xFFFFFFFFu) {  // not occluded
+        const float cs = swrx::vdot(dn, bd_get(B, vi, 1, q));
+        const f3 vc = bd_get(B, vi, 2, q), lc = bd_get(B, kBdptMax + li, 2, q);
+        acc = swrx::vadd(acc, mk(__fmul_rn(__fmul_rn(vc.x, lc.x), cs), __fmul_rn(__fmul_rn(vc.y, lc.y), cs),
+                                 __fmul_rn(__fmul_rn(vc.z, lc.z), cs)));
+      }
+      ++li;
+      pending = false;
+    }
+    for (;;) {
+      if (vi >= dv) {
+        const uint32_t pixel = q / F.spp, sample = q % F.spp;
+        const f3 r = swrx::vscale(inv_md, acc);
+        F.contrib[(size_t)pixel * F.spp + sample] = make_float4(r.x, r.y, r.z, 1.0f);
+        active = false;
+        break;
+      }
+      if (li >= dl) {
+        ++vi;
+        li = 0;
+        continue;
+      }
+      if (vi + li > B.md) {
+        ++li;
+        continue;
+      }
+      const f3 vp = bd_get(B, vi, 0, q), vn = bd_get(B, vi, 1, q);
+      const f3 lp = bd_get(B, kBdptMax + li, 0, q), ln = bd_get(B, kBdptMax + li, 1, q);
+      const f3 a = swrx::vadd(vp, swrx::vscale(0.01f, vn));
+      const f3 b = swrx::vadd(lp, swrx::vscale(0.01f, ln));
+      const f3 dd = swrx::vsub(b, a);
+      const float dist2 = swrx::vdot(dd, dd);
+      dn = swrx::vnormalize(dd);
+      tr.init_occlusion(a, dn, dist2, stack + threadIdx.x, kTraceBlock);
+      tracing = true;
+      pending = true;
+      break;
     }
   }
 }
@@ -677,11 +752,13 @@ __global__ void k_resolve(Frame F, float* __restrict__ img) {
 }
 
 struct Workspace {
-  size_t qbytes = 0, cam_px = 0, contrib_n = 0, stage_n = 0;
+  size_t qbytes = 0, cam_px = 0, contrib_n = 0, stage_n = 0, bd_vtx_n = 0, bd_head_n = 0;
   void* qbuf = nullptr;
   void* cam = nullptr;
   void* contrib = nullptr;
   void* stage = nullptr;  // device image for callers that pass a host output buffer
+  void* bd_vtx = nullptr;   // bidirectional tracer: per-sample vertex tables
+  void* bd_head = nullptr;  // bidirectional tracer: per-sample vertex counts
   Ctrl* ctrl = nullptr;
   Ctrl* host_ctrl = nullptr;
 };
@@ -963,6 +1040,8 @@ void free_workspace(swr_scene* s) {
   if (ws->cam) cudaFree(ws->cam);
   if (ws->contrib) cudaFree(ws->contrib);
   if (ws->stage) cudaFree(ws->stage);
+  if (ws->bd_vtx) cudaFree(ws->bd_vtx);
+  if (ws->bd_head) cudaFree(ws->bd_head);
   if (ws->ctrl) cudaFree(ws->ctrl);
   if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
   delete ws;
@@ -1061,7 +1140,8 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   if (b->max_depth == 0) return set_error(SWR_ERR_INVALID, "swr: bidirectional maxDepth must be positive");
   if ((uint64_t)o->width * o->height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
-  if (b->shade_batch > 32) return set_error(SWR_ERR_INVALID, "swr: shade_batch must be 0..32");
+  if ((b->shade_batch & 0xFFu) > 32 || ((b->shade_batch >> 8) & 0xFFu) > 32 || (b->shade_batch >> 16))
+    return set_error(SWR_ERR_INVALID, "swr: shade_batch fields must be 0..32");
   if (b->blocks_per_sm != 0 && b->blocks_per_sm != 5 && b->blocks_per_sm != 6 && b->blocks_per_sm != 8)
     return set_error(SWR_ERR_INVALID, "swr: blocks_per_sm must be 0, 5, 6 or 8");
   if (s->dev.num_lights == 0)
@@ -1074,10 +1154,13 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   RenderWorkspace* ws = workspace_of(s);
   if (!ws) return set_error(SWR_ERR_ALLOC, "swr: workspace");
   const uint64_t npix_total = (uint64_t)o->width * o->height;
-  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
+  // the vertex tables take 1.5 KB per sample of a chunk
+  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kBdptChunkSamples / o->spp));
   int rc;
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->contrib, ws->contrib_n, px_per_chunk * o->spp, sizeof(float4)))) return rc;
+  if ((rc = ensure(&ws->bd_vtx, ws->bd_vtx_n, px_per_chunk * o->spp * 6 * kBdptMax, sizeof(float4)))) return rc;
+  if ((rc = ensure(&ws->bd_head, ws->bd_head_n, px_per_chunk * o->spp, sizeof(uint4)))) return rc;
   if (!ws->ctrl) {
     SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
     SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
@@ -1108,14 +1191,20 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   B.vj = o->max_depth;
   B.lj = b->light_jumps;
   B.md = b->max_depth;
-  B.batch = b->shade_batch ? b->shade_batch : kBdptBatch;
-  auto kern = k_bdpt<0>;
-  if (b->blocks_per_sm == 5) kern = k_bdpt<5>;
-  else if (b->blocks_per_sm == 6) kern = k_bdpt<6>;
-  else if (b->blocks_per_sm == 8) kern = k_bdpt<8>;
-  int per_sm = 0;
+  B.batch = (b->shade_batch & 0xFFu) ? (b->shade_batch & 0xFFu) : kBdptBatch;
+  B.cbatch = ((b->shade_batch >> 8) & 0xFFu) ? ((b->shade_batch >> 8) & 0xFFu) : kConnectBatch;
+  B.vtx = (float4*)ws->bd_vtx;
+  B.head = (uint4*)ws->bd_head;
+  auto kern = k_bdpt_paths<0>;
+  auto kconn = k_bdpt_connect<0>;
+  if (b->blocks_per_sm == 5) kern = k_bdpt_paths<5>, kconn = k_bdpt_connect<5>;
+  else if (b->blocks_per_sm == 6) kern = k_bdpt_paths<6>, kconn = k_bdpt_connect<6>;
+  else if (b->blocks_per_sm == 8) kern = k_bdpt_paths<8>, kconn = k_bdpt_connect<8>;
+  int per_sm = 0, per_sm_c = 0;
   SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTraceBlock, 0));
+  SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, kconn, kTraceBlock, 0));
   const unsigned grid = (unsigned)(s->num_sms * std::max(per_sm, 1));
+  const unsigned grid_c = (unsigned)(s->num_sms * std::max(per_sm_c, 1));
   for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
     const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
     F.pixel0 = (uint32_t)p0;
@@ -1127,7 +1216,9 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
     *ws->host_ctrl = init;
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
     k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    B.nsamp = np * o->spp;
     kern<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
+    kconn<<<grid_c, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
     k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
     SWR_CUDA(cudaGetLastError());
     if (want_samples)
