@@ -112,7 +112,9 @@ typedef struct swr_render_opts {
   uint32_t mode;           /* SWR_MODE_* */
   uint32_t rr_depth;       /* physical mode: Russian roulette at path vertices >= rr_depth (0=off) */
   float rr_survive;        /* physical mode: survival probability, (0, 1] */
-  uint32_t wave_size;      /* paths in flight, 0 = 2^23 (capped by the samples of a chunk) */
+  uint32_t wave_size;      /* paths in flight, 0 = 2^23 (capped by the samples of a chunk); the
+                              bidirectional tracer: samples per chunk, 0 = as many as keep the
+                              chunk's vertex tables within 2 GB */
   uint32_t block_size;     /* threads per block of the shading kernel, 0 = automatic */
   uint32_t flags;          /* SWR_RENDER_* */
   uint32_t refill;         /* bounce traversal: idle lanes (1..32) that trigger a refill, 0 = 8 */

@@ -282,11 +282,11 @@ def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=
 
 
 def _scene_render_bdpt(self, cam, width, height, spp, vision_jumps, light_jumps, max_depth, seed=0, out=None,
-                       samples=None, refill=0, shade_batch=0, blocks_per_sm=0, stream=None):
+                       samples=None, refill=0, shade_batch=0, blocks_per_sm=0, chunk=0, stream=None):
     """BidirectionalPathTracer image (height, width, 3) into `out` (torch cuda tensor or numpy
     array); `samples` (optional, (height*width, spp, 4)) receives the per-sample contributions."""
     flags = N.RENDER_SAMPLES_OUT if samples is not None else 0
-    o = N.RenderOpts(width, height, spp, vision_jumps, seed, N.MODE_REFERENCE, 0, 1.0, 0, 0, flags, refill, 0, 0)
+    o = N.RenderOpts(width, height, spp, vision_jumps, seed, N.MODE_REFERENCE, 0, 1.0, chunk, 0, flags, refill, 0, 0)
     b = N.BdptOpts(light_jumps, max_depth, shade_batch, blocks_per_sm)
     if out is None:
         import torch

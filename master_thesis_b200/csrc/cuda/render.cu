@@ -447,16 +447,16 @@ constexpr int kBdptMax = 16;
 // 5.84 / 4.62 / 4.23 / 3.95 / 3.95 ms at refill 4 (identical images)
 constexpr uint32_t kBdptBatch = 20;
 constexpr uint32_t kConnectBatch = 16;
-constexpr uint64_t kBdptChunkSamples = 1ull << 20;
+constexpr uint64_t kBdptTableBytes = 2048ull << 20;
 
 struct BdptArgs {
   uint32_t vj, lj, md;
   uint32_t batch;     // lanes of a warp whose trace finished that advance their samples together
   uint32_t cbatch;    // the same for the connection queries
   uint32_t nsamp;     // samples of the chunk (pixels x spp)
-  float4* vtx;        // [3 * 2 * kBdptMax * nsamp]: point, normal, throughput of vertex slot k of
-                      // sample q at (3k + field) * nsamp + q; vision vertex i is slot i, light
-                      // vertex i slot kBdptMax + i
+  float4* vtx;        // [3 * (vj + max(lj, 1)) * nsamp]: point, normal, throughput of vertex slot
+                      // k of sample q at (3k + field) * nsamp + q; vision vertex i is slot i,
+                      // light vertex i slot vj + i
   uint4* head;        // [nsamp] first vision slot, vision end, light count, 1 = already resolved
 };
 
@@ -570,7 +570,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
           const float cs = swrx::vdot(n, vision ? nd : prev);
           c = swrx::vmul(c, mk(__fmul_rn(m.m0.x, cs), __fmul_rn(m.m0.y, cs), __fmul_rn(m.m0.z, cs)));
         }
-        bd_put(B, (vision ? 0u : (uint32_t)kBdptMax) + i, q, p, n, c);
+        bd_put(B, (vision ? 0u : B.vj) + i, q, p, n, c);
         const bool light_hit = __float_as_uint(m.m1.w) != 0u && swrx::vdot(n, prev) <= 0.0f;
         ++i;
         if (light_hit || i >= (vision ? B.vj : B.lj)) {
@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
         ln = swrx::vadd(ln, swrx::vscale(b2, n2));
         ln = swrx::vnormalize(ln);
         const float4 lc = __ldg(sc.mats + 3 * (size_t)L.z);
-        bd_put(B, (uint32_t)kBdptMax, q, lp, ln, mk(lc.x, lc.y, lc.z));
+        bd_put(B, B.vj, q, lp, ln, mk(lc.x, lc.y, lc.z));
         o = lp;
         d = swrx::hemisphere_dir(ln, U.u[1], U.u[2]);
         c = mk(1.0f, 1.0f, 1.0f);
@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
     if (pending) {  // the query of pair (vi, li) is answered
       if (tr.hit.slot == 0xFFFFFFFFu) {  // not occluded
         const float cs = swrx::vdot(dn, bd_get(B, vi, 1, q));
-        const f3 vc = bd_get(B, vi, 2, q), lc = bd_get(B, kBdptMax + li, 2, q);
+        const f3 vc = bd_get(B, vi, 2, q), lc = bd_get(B, B.vj + li, 2, q);
         acc = swrx::vadd(acc, mk(__fmul_rn(__fmul_rn(vc.x, lc.x), cs), __fmul_rn(__fmul_rn(vc.y, lc.y), cs),
                                  __fmul_rn(__fmul_rn(vc.z, lc.z), cs)));
       }
@@ -715,7 +715,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
         continue;
       }
       const f3 vp = bd_get(B, vi, 0, q), vn = bd_get(B, vi, 1, q);
-      const f3 lp = bd_get(B, kBdptMax + li, 0, q), ln = bd_get(B, kBdptMax + li, 1, q);
+      const f3 lp = bd_get(B, B.vj + li, 0, q), ln = bd_get(B, B.vj + li, 1, q);
       const f3 a = swrx::vadd(vp, swrx::vscale(0.01f, vn));
       const f3 b = swrx::vadd(lp, swrx::vscale(0.01f, ln));
       const f3 dd = swrx::vsub(b, a);
@@ -1154,12 +1154,18 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   RenderWorkspace* ws = workspace_of(s);
   if (!ws) return set_error(SWR_ERR_ALLOC, "swr: workspace");
   const uint64_t npix_total = (uint64_t)o->width * o->height;
-  // the vertex tables take 1.5 KB per sample of a chunk
-  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kBdptChunkSamples / o->spp));
+  // samples per chunk: by default as many as keep the vertex tables (48 B per vertex slot and
+  // sample) within 2 GB. Measured on the Cornell BDPT image (1 M samples, 10 slots): chunks of
+  // 2^16 / 2^18 / 2^19 / 2^20 samples -> 6.85 / 3.40 / 2.95 / 2.71 ms; tables small enough for L2
+  // do not pay for the per-chunk launches and synchronisation.
+  const uint64_t slots = (uint64_t)o->max_depth + std::max<uint32_t>(b->light_jumps, 1u);
+  const uint64_t chunk = o->wave_size ? (uint64_t)o->wave_size
+                                      : std::max<uint64_t>(1u << 14, kBdptTableBytes / (48 * slots));
+  const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, chunk / o->spp));
   int rc;
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->contrib, ws->contrib_n, px_per_chunk * o->spp, sizeof(float4)))) return rc;
-  if ((rc = ensure(&ws->bd_vtx, ws->bd_vtx_n, px_per_chunk * o->spp * 6 * kBdptMax, sizeof(float4)))) return rc;
+  if ((rc = ensure(&ws->bd_vtx, ws->bd_vtx_n, px_per_chunk * o->spp * 3 * slots, sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->bd_head, ws->bd_head_n, px_per_chunk * o->spp, sizeof(uint4)))) return rc;
   if (!ws->ctrl) {
     SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
