@@ -18,10 +18,10 @@ def _close(a, b):
     return np.all(np.abs(a - b) <= RTOL * np.maximum(np.abs(b), 1e-6) + 1e-7)
 
 
-def _render(sc, cam, W, H, spp, vj, lj, md, seed, refill=0, shade_batch=0):
+def _render(sc, cam, W, H, spp, vj, lj, md, seed, refill=0, shade_batch=0, chunk=0):
     samples = torch.empty((W * H, spp, 4), dtype=torch.float32, device="cuda")
     img = sc.render_bdpt(cam, W, H, spp, vj, lj, md, seed=seed, samples=samples, refill=refill,
-                         shade_batch=shade_batch)
+                         shade_batch=shade_batch, chunk=chunk)
     torch.cuda.synchronize()
     return img.cpu().numpy().reshape(-1, 3), samples.cpu().numpy()
 
@@ -40,13 +40,16 @@ def test_gpu_bdpt_matches_reference_golden(name):
     assert (np.abs(ref).sum(-1) > 0).mean() > 0.05
 
 
-@pytest.mark.parametrize("refill,shade_batch", [(0, 0), (1, 1), (32, 1), (4, 16), (2, 32)])
-def test_gpu_bdpt_matches_oracle_on_terrain(tmp_path, refill, shade_batch):
+@pytest.mark.parametrize("refill,shade_batch,chunk", [(0, 0, 0), (1, 1, 0), (32, 1, 0), (4, 16, 0),
+                                                     (2, 32 | (1 << 8), 0), (0, 0, 100), (8, 8 | (24 << 8), 7)])
+def test_gpu_bdpt_matches_oracle_on_terrain(tmp_path, refill, shade_batch, chunk):
+    """Launch shapes and chunkings (chunk: samples per chunk of the vertex tables, rounded down
+    to whole pixels; 100 and 7 give many chunks) all give the oracle's result."""
     s = scenes.terrain(3, str(tmp_path), cells=64, tile=16, spheres=6, sphere_subdiv=2, lights=3)
     sd = swr.load_scene(s["scene"], s["basepath"])
     W, H, spp, vj, lj, md, seed = 40, 28, 3, 6, 4, 7, 5
     cam = swr.load_camera(s["camera"], W, H)
-    img, ps = _render(swr.Scene(sd), cam, W, H, spp, vj, lj, md, seed, refill, shade_batch)
+    img, ps = _render(swr.Scene(sd), cam, W, H, spp, vj, lj, md, seed, refill, shade_batch, chunk)
     vi, pi, org = swr.camera_arrays(cam)
     ops, opp = O.render_bdpt(O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org), W, H, spp, vj, lj, md, seed)
     assert _close(ps[..., :3], ops[..., :3])
