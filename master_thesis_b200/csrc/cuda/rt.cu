@@ -27,8 +27,6 @@
 #include "swr_internal.cuh"
 
 namespace swr {
-int device_input(const float* p, size_t bytes, cudaStream_t stream, void** tmp, const float** dev);
-
 namespace {
 
 using swrx::f3;
