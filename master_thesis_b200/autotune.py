@@ -8,6 +8,12 @@ build; the leaf size and the SAH leaf cost are build options measured separately
 
     cfg = tune_render(scene, cam, width, height, spp, depth, mode=...)   # -> dict of render kwargs
     cfg = tune_batch(batch, jobs)                                        # -> dict of batch kwargs
+    cfg = tune_bdpt(scene, cam, width, height, spp, vj, lj, md)          # -> dict of render_bdpt kwargs
+    cfg = tune_rt(scene, cam, width, height, spp, vision_jumps)          # -> dict of rt.render kwargs
+
+For the per-lane kernels (the bidirectional tracer, the RayTrace frame) the knobs are the number
+of lanes of a warp that run their stage code together, the idle-lane refill threshold and the
+register budget.
 """
 import itertools
 import json
@@ -21,6 +27,9 @@ CACHE = os.environ.get("SWR_TUNE_CACHE", os.path.join(os.path.expanduser("~"), "
 RENDER_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16], block_size=[256],
                    trace_blocks=[0])
 BATCH_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16])
+BDPT_GRID = dict(shade_batch=[12 | (16 << 8), 20 | (16 << 8), 24 | (16 << 8), 20 | (8 << 8), 20 | (24 << 8)],
+                 refill=[4, 8], blocks_per_sm=[0])
+RT_GRID = dict(shade_batch=[8, 12, 16, 20], refill=[2, 4], blocks_per_sm=[0, 6])
 
 
 def _load():
@@ -92,3 +101,26 @@ def tune_batch(batch, jobs, reps=1, force=False, grid=None):
     def run(cfg):
         batch.render(jj, **cfg)
     return _search(key, grid or BATCH_GRID, run, reps, force)
+
+
+def tune_bdpt(scene, cam, width, height, spp, vision_jumps, light_jumps, max_depth, reps=2, force=False, grid=None):
+    st = scene.stats()
+    key = "bdpt|%s|tris=%d|px=%d|spp=%d|jumps=%d/%d/%d" % (torch.cuda.get_device_name(), st["triangles"],
+                                                          width * height, spp, vision_jumps, light_jumps, max_depth)
+    out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+
+    def run(cfg):
+        scene.render_bdpt(cam, width, height, spp, vision_jumps, light_jumps, max_depth, out=out, **cfg)
+    return _search(key, grid or BDPT_GRID, run, reps, force)
+
+
+def tune_rt(scene, cam, width, height, spp, vision_jumps, reps=2, force=False, grid=None):
+    from . import rt
+    st = scene.stats()
+    key = "rt|%s|tris=%d|px=%d|spp=%d|jumps=%d" % (torch.cuda.get_device_name(), st["triangles"], width * height,
+                                                   spp, vision_jumps)
+    out = torch.empty((height, width, 4), dtype=torch.uint8, device="cuda")
+
+    def run(cfg):
+        rt.render(scene, cam, width, height, spp, vision_jumps, rgba=out, want_rgb=False, **cfg)
+    return _search(key, grid or RT_GRID, run, reps, force)

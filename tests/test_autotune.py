@@ -38,3 +38,28 @@ def test_tune_render_on_gpu(tmp_path, monkeypatch):
     assert best["wave_size"] in (1 << 12, 1 << 14) and best["refill"] == 8
     img = sc.render(c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL, **best)
     assert float(img.max()) > 0
+
+
+@pytest.mark.gpu
+def test_tune_per_lane_kernels_on_gpu(tmp_path, monkeypatch):
+    """The bidirectional tracer and the RayTrace frame: the tuned launch shape renders the same
+    image as the library's defaults."""
+    import numpy as np
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import rt, scenes
+    monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tune.json"))
+    s = scenes.cornell(2, str(tmp_path))
+    sc = swr.Scene(swr.load_scene(s["scene"], s["basepath"]))
+    cam = swr.load_camera(s["camera"], 48, 32)
+    b = autotune.tune_bdpt(sc, cam, 48, 32, 4, 5, 5, 5, grid=dict(shade_batch=[1, 20 | (16 << 8)], refill=[4]))
+    assert b["shade_batch"] in (1, 20 | (16 << 8))
+    img = sc.render_bdpt(cam, 48, 32, 4, 5, 5, 5, seed=3, **b)
+    ref = sc.render_bdpt(cam, 48, 32, 4, 5, 5, 5, seed=3)
+    assert torch.equal(img, ref)
+    r = autotune.tune_rt(sc, cam, 48, 32, 3, 5, grid=dict(shade_batch=[4, 16], refill=[4], blocks_per_sm=[0, 6]))
+    a = rt.render(sc, cam, 48, 32, 3, 5, want_rgb=False, **r)[1]
+    d = rt.render(sc, cam, 48, 32, 3, 5, want_rgb=False)[1]
+    assert torch.equal(a, d) and int(a.max()) > 0
+    db = json.loads((tmp_path / "tune.json").read_text())
+    assert any(k.startswith("bdpt|") for k in db) and any(k.startswith("rt|") for k in db)
