@@ -84,11 +84,11 @@ typedef struct swr_scene_desc {
 } swr_scene_desc;
 
 typedef struct swr_build_opts {
-  uint32_t sah_bins;       /* host builder: SAH bins, 0 = 32 */
+  uint32_t sah_bins;       /* host builder: SAH bins, 0 = 64 */
   uint32_t max_leaf;       /* triangles per leaf, 1..3; 0 = 3 */
   uint32_t threads;        /* host builder threads, 0 = all */
   uint32_t leaf_cost_pct;  /* SAH cost of a triangle test relative to a wide-node visit, in
-                              percent (1..400); 0 = 30 */
+                              percent (1..400); 0 = 80 */
   uint32_t builder;        /* SWR_BUILD_HOST (binned SAH on the host) or SWR_BUILD_DEVICE
                               (clustering and collapse on the GPU); same closest hits either way */
   uint32_t radius;         /* device builder: clustering search radius 1..256, 0 = 16 */
