@@ -65,6 +65,26 @@ uint32_t twin_ref_tree(const float* boxes, uint32_t n, uint32_t* out) {
   return m;
 }
 
+// the merge sequence itself: left/right child of every node (2n - 1 entries each, -1 for
+// leaves) from the build chosen by mode (0 automatic, 1 flat, 2 kd-tree indexed)
+void twin_ref_merges(const float* boxes, uint32_t n, int mode, int32_t* left, int32_t* right) {
+  std::vector<swr::Box> b(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    b[i].empty = false;
+    for (int k = 0; k < 3; ++k) {
+      b[i].lo[k] = boxes[6 * i + k];
+      b[i].hi[k] = boxes[6 * i + 3 + k];
+    }
+  }
+  swr::RefTree t;
+  const swr::RefBuild how = mode == 1 ? swr::RefBuild::kFlat : mode == 2 ? swr::RefBuild::kIndexed : swr::RefBuild::kAuto;
+  swr::ref_bvh_leaf_order(b, &t, how);
+  for (size_t i = 0; i < t.left.size(); ++i) {
+    left[i] = t.left[i];
+    right[i] = t.right[i];
+  }
+}
+
 // copies the packed wide-BVH node words (20 per node) into out (if not null); returns the count
 uint32_t twin_node_words(void* t, uint32_t* out) {
   const auto& w = ((Twin*)t)->pk.nodes;

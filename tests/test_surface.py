@@ -82,6 +82,11 @@ def test_reference_bvh_topology_reproduced(tmp_path):
         ref = refdump.tree(boxes, str(tmp_path / ("t%d" % n)))
         mine = _my_tree(boxes)
         assert np.array_equal(ref, mine), n
+    # a lattice of equal spacings (ties at every step), as terrain tiles give
+    g = np.stack(np.meshgrid(np.arange(24), np.arange(24), indexing="ij"), -1).reshape(-1, 2).astype(np.float32)
+    c = np.stack([g[:, 0] / 16, rng.integers(0, 2, g.shape[0]) / 64, g[:, 1] / 16], 1).astype(np.float32)
+    boxes = np.concatenate([c - 1 / 32, c + 1 / 32], 1).astype(np.float32)
+    assert np.array_equal(refdump.tree(boxes, str(tmp_path / "lattice")), _my_tree(boxes))
 
 
 def _my_tree(boxes):
