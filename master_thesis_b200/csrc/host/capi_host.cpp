@@ -169,7 +169,7 @@ std::vector<uint32_t> object_order(const float* boxes, uint32_t n, bool exact) {
     b[o].lo = v3(boxes[6 * o], boxes[6 * o + 1], boxes[6 * o + 2]);
     b[o].hi = v3(boxes[6 * o + 3], boxes[6 * o + 4], boxes[6 * o + 5]);
   }
-  return ref_bvh_leaf_order(b);
+  return ref_bvh_leaf_order(b, nullptr, RefBuild::kAuto, 0);
 }
 
 }  // namespace swr

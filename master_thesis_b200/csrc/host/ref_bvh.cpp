@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 namespace swr {
 
@@ -160,8 +161,10 @@ inline float prune_bound(float lb) { return lb * 0.99999f - 1e-36f; }
 
 class IndexedBuild {
  public:
-  IndexedBuild(const std::vector<Box>& boxes, std::vector<int32_t>& left, std::vector<int32_t>& right)
-      : n_((int32_t)boxes.size()),
+  IndexedBuild(const std::vector<Box>& boxes, std::vector<int32_t>& left, std::vector<int32_t>& right,
+               unsigned threads)
+      : threads_(threads),
+        n_((int32_t)boxes.size()),
         total_(2 * n_ - 1),
         cen_(total_),
         box_(total_),
@@ -187,7 +190,21 @@ class IndexedBuild {
     std::vector<int32_t> ids(n_);
     for (int32_t i = 0; i < n_; ++i) ids[i] = i;
     rebuild(ids);
-    for (int32_t i = 0; i < n_; ++i) nearest(i);
+    // every leaf's nearest node: independent queries over the same tree, split across threads
+    const unsigned nth = std::max(1u, std::min(threads_, (unsigned)(n_ / 1024)));
+    if (nth > 1) {
+      std::vector<std::thread> pool;
+      for (unsigned t = 0; t < nth; ++t)
+        pool.emplace_back([this, t, nth] {
+          std::vector<std::pair<int32_t, float>> stack;
+          for (int32_t i = (int32_t)((int64_t)n_ * t / nth); i < (int32_t)((int64_t)n_ * (t + 1) / nth); ++i)
+            nearest_into(i, stack, nn_[i], nd_[i]);
+        });
+      for (std::thread& th : pool) th.join();
+      for (int32_t i = 0; i < n_; ++i) pointed_[nn_[i]].push_back(i);
+    } else {
+      for (int32_t i = 0; i < n_; ++i) nearest(i);
+    }
     for (size_t v = nodes_.size(); v-- > 0;) {  // children come after their parent
       Node& node = nodes_[v];
       node.maxnd = node.child < 0 ? leaf_max(node)
@@ -261,6 +278,7 @@ class IndexedBuild {
   static constexpr int kLeafSize = 8;  // leaves of a fresh tree
   static constexpr int kLeafCap = 32;  // a leaf that inserts fill up is split
 
+  const unsigned threads_;
   const int32_t n_, total_;
   Centres cen_;
   std::vector<Box> box_;
@@ -436,17 +454,26 @@ class IndexedBuild {
 
   // nearest live node of k (smallest float distance, then smallest id)
   void nearest(int32_t k) {
+    int32_t j;
+    float d;
+    nearest_into(k, stack_, j, d);
+    assign(k, j, d);
+  }
+
+  // the nearest live node of k and its distance; reads the tree only
+  void nearest_into(int32_t k, std::vector<std::pair<int32_t, float>>& stack, int32_t& out_id,
+                    float& out_d) const {
     float q[3];
     centre(k, q);
     // (distance, id) as one key: distances are >= +0, so their bit patterns order like the
     // values, and the smallest key is the smallest distance, then the smallest id
     const uint64_t none = ((uint64_t)bits(kInf) << 32) | 0xFFFFFFFFu;
     uint64_t best = none;
-    stack_.clear();
-    stack_.emplace_back(0, 0.0f);
-    while (!stack_.empty()) {
-      const auto [v, lb] = stack_.back();
-      stack_.pop_back();
+    stack.clear();
+    stack.emplace_back(0, 0.0f);
+    while (!stack.empty()) {
+      const auto [v, lb] = stack.back();
+      stack.pop_back();
       if (prune_bound(lb) > key_dist(best)) continue;
       const Node& node = nodes_[v];
       if (node.child < 0) {
@@ -462,10 +489,11 @@ class IndexedBuild {
       const float l0 = lower_bound(q, nodes_[node.child]);
       const float l1 = lower_bound(q, nodes_[node.child + 1]);
       const int32_t near = l0 <= l1 ? node.child : node.child + 1;
-      stack_.emplace_back(2 * node.child + 1 - near, l0 <= l1 ? l1 : l0);
-      stack_.emplace_back(near, l0 <= l1 ? l0 : l1);
+      stack.emplace_back(2 * node.child + 1 - near, l0 <= l1 ? l1 : l0);
+      stack.emplace_back(near, l0 <= l1 ? l0 : l1);
     }
-    assign(k, (int32_t)(uint32_t)best, key_dist(best));
+    out_id = (int32_t)(uint32_t)best;
+    out_d = key_dist(best);
   }
 
   static uint32_t bits(float f) {
@@ -536,7 +564,8 @@ bool indexable(const std::vector<Box>& boxes) {
 
 }  // namespace
 
-std::vector<uint32_t> ref_bvh_leaf_order(const std::vector<Box>& boxes, RefTree* tree, RefBuild how) {
+std::vector<uint32_t> ref_bvh_leaf_order(const std::vector<Box>& boxes, RefTree* tree, RefBuild how,
+                                         unsigned threads) {
   const int32_t n = (int32_t)boxes.size();
   std::vector<uint32_t> order;
   if (n == 0) return order;
@@ -546,7 +575,7 @@ std::vector<uint32_t> ref_bvh_leaf_order(const std::vector<Box>& boxes, RefTree*
                        (how == RefBuild::kAuto && n >= kRefIndexedMin);
   if (n > 1) {
     if (indexed && indexable(boxes)) {
-      IndexedBuild(boxes, left, right).run();
+      IndexedBuild(boxes, left, right, threads ? threads : std::max(1u, std::thread::hardware_concurrency())).run();
     } else {
       build_flat(boxes, left, right);
     }

@@ -29,8 +29,10 @@ enum class RefBuild { kAuto, kFlat, kIndexed };
 constexpr int32_t kRefIndexedMin = 1024;
 
 // Builds the tree over the given leaf boxes (in input order) and returns the element indices in
-// left-first DFS order. If tree is non-null the full topology is returned too.
+// left-first DFS order. If tree is non-null the full topology is returned too. threads: host
+// threads for the kd-tree build's first nearest-node queries (0 = all cores); the rest of the
+// build is sequential.
 std::vector<uint32_t> ref_bvh_leaf_order(const std::vector<Box>& boxes, RefTree* tree = nullptr,
-                                         RefBuild how = RefBuild::kAuto);
+                                         RefBuild how = RefBuild::kAuto, unsigned threads = 1);
 
 }  // namespace swr

@@ -465,7 +465,7 @@ HostScene SceneBuilder::finish() {
   if (nobj > 0 && nobj <= opt_.max_exact_order) {
     std::vector<Box> boxes(nobj);
     for (size_t o = 0; o < nobj; ++o) boxes[o] = s.objects[o].aabb;
-    s.obj_dfs = ref_bvh_leaf_order(boxes);
+    s.obj_dfs = ref_bvh_leaf_order(boxes, nullptr, RefBuild::kAuto, 0);
   } else {
     s.obj_dfs.resize(nobj);
     for (size_t o = 0; o < nobj; ++o) s.obj_dfs[o] = (uint32_t)o;

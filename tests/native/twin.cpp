@@ -66,7 +66,8 @@ uint32_t twin_ref_tree(const float* boxes, uint32_t n, uint32_t* out) {
 }
 
 // the merge sequence itself: left/right child of every node (2n - 1 entries each, -1 for
-// leaves) from the build chosen by mode (0 automatic, 1 flat, 2 kd-tree indexed)
+// leaves) from the build chosen by mode (0 automatic, 1 flat, 2 kd-tree indexed, 3 kd-tree indexed
+// with its first queries on 4 threads)
 void twin_ref_merges(const float* boxes, uint32_t n, int mode, int32_t* left, int32_t* right) {
   std::vector<swr::Box> b(n);
   for (uint32_t i = 0; i < n; ++i) {
@@ -77,8 +78,8 @@ void twin_ref_merges(const float* boxes, uint32_t n, int mode, int32_t* left, in
     }
   }
   swr::RefTree t;
-  const swr::RefBuild how = mode == 1 ? swr::RefBuild::kFlat : mode == 2 ? swr::RefBuild::kIndexed : swr::RefBuild::kAuto;
-  swr::ref_bvh_leaf_order(b, &t, how);
+  const swr::RefBuild how = mode == 1 ? swr::RefBuild::kFlat : mode >= 2 ? swr::RefBuild::kIndexed : swr::RefBuild::kAuto;
+  swr::ref_bvh_leaf_order(b, &t, how, mode == 3 ? 4 : 1);
   for (size_t i = 0; i < t.left.size(); ++i) {
     left[i] = t.left[i];
     right[i] = t.right[i];

@@ -73,6 +73,16 @@ def test_indexed_build_merges_like_flat(name, boxes):
     assert np.all(fl[0][n:] < np.arange(n, 2 * n - 1)) and np.all(fl[0][n:] < fl[1][n:])
 
 
+def test_indexed_build_with_threaded_first_queries():
+    rng = np.random.default_rng(4)
+    g = np.stack(np.meshgrid(np.arange(64), np.arange(64), indexing="ij"), -1).reshape(-1, 2).astype(np.float32)
+    terrain = np.stack([g[:, 0] / 32, rng.integers(0, 4, len(g)) / 128, g[:, 1] / 32], 1)
+    spheres = rng.uniform(0, 2, (64, 3)) * [1, 0.4, 1]
+    b = _boxes(np.concatenate([terrain, spheres]), 1 / 64)
+    fl, ix = _merges(b, 1), _merges(b, 3)
+    assert np.array_equal(fl[0], ix[0]) and np.array_equal(fl[1], ix[1])
+
+
 @pytest.mark.parametrize("n", [2, 3, 5, 17, 63, 64, 65, 130])
 def test_indexed_build_small_inputs(n):
     rng = np.random.default_rng(n)
