@@ -11,15 +11,17 @@
 //   k_inst_objbox    one warp per object: the reference's object box (first vertex padded by
 //                    1e-4, then std::min/std::max), lanes over contiguous vertex ranges combined
 //                    in order so that equal coordinates keep the first one, as sequentially.
-//   (host)           the scene-level leaf order of the object boxes gives the tie ranks' bases.
-//   k_inst_derive    one thread per triangle: edges, dot products, reference triangle box,
-//                    corner normals and rank, written to the triangle's BVH slot; the scene
-//                    extent is reduced for the traversal boxes' margin.
+//   k_inst_derive    one thread per triangle: edges, dot products, reference triangle box and
+//                    corner normals, written to the triangle's BVH slot; the scene extent is
+//                    reduced for the traversal boxes' margin.
 //   k_inst_prims     traversal boxes (reference boxes widened by the margin of scene_pack.cpp).
 //   k_refit          one launch per tree level, deepest first: each wide node's child boxes from
 //                    its children's exact boxes or its leaves' traversal boxes, requantised on a
 //                    new grid; the topology and the slot assignment are kept.
 //   k_inst_lights    the light-triangle tables of the bidirectional tracer.
+//   (host)           meanwhile, the scene-level leaf order of the object boxes (copied back right
+//                    after k_inst_objbox) gives the tie ranks' bases,
+//   k_inst_rank      and one thread per triangle writes its rank into its record.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -57,9 +59,13 @@ struct Instance {
   std::vector<swr_object_transform> xf;
   bool exact = true;
   std::vector<void*> allocs;
+  float* host_boxes = nullptr;          // pinned [6 * objects]: object boxes copied back
+  cudaEvent_t boxes_ready = nullptr;    // recorded after that copy
   Instance() { std::memset(&v, 0, sizeof(v)); }
   ~Instance() {
     for (void* p : allocs) cudaFree(p);
+    if (host_boxes) cudaFreeHost(host_boxes);
+    if (boxes_ready) cudaEventDestroy(boxes_ready);
   }
   template <class T>
   int alloc(T** p, size_t n) {
@@ -213,10 +219,10 @@ __global__ void k_inst_derive(InstView I, DevScene sc, float4* __restrict__ tris
     const float d00 = dot0(e0, e0), d01 = dot0(e0, e1), d11 = dot0(e1, e1);
     const float den = fsub(fmul(d00, d11), fmul(d01, d01));
     const uint32_t obj = I.tri_obj[t];
-    const uint32_t rank = I.base[obj] + I.local_rank[t];
     tris[3 * (size_t)s + 0] = make_float4(a[0], a[1], a[2], e0[0]);
     tris[3 * (size_t)s + 1] = make_float4(e0[1], e0[2], e1[0], e1[1]);
-    tris[3 * (size_t)s + 2] = make_float4(e1[2], __uint_as_float(t), __uint_as_float(rank), __uint_as_float(obj));
+    // the rank word is written by k_inst_rank once the object order is known
+    tris[3 * (size_t)s + 2] = make_float4(e1[2], __uint_as_float(t), __uint_as_float(0u), __uint_as_float(obj));
     shade[4 * (size_t)s + 0] = make_float4(d00, d01, d11, den);
     shade[4 * (size_t)s + 1] = I.vnrm[ia];
     shade[4 * (size_t)s + 2] = I.vnrm[ib];
@@ -249,6 +255,15 @@ __global__ void k_inst_derive(InstView I, DevScene sc, float4* __restrict__ tris
       }
     }
   }
+}
+
+// the tie rank of triangle t (its object's base plus its place in its mesh's leaf order), into
+// the rank word of its record
+__global__ void k_inst_rank(InstView I, DevScene sc, float4* __restrict__ tris) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= I.nt) return;
+  const uint32_t s = sc.slot_of[t];
+  reinterpret_cast<uint32_t*>(tris + 3 * (size_t)s + 2)[2] = I.base[I.tri_obj[t]] + I.local_rank[t];
 }
 
 // traversal boxes: the reference triangle boxes widened by the margin scene_pack.cpp uses
@@ -432,6 +447,12 @@ int attach(swr_scene* s, const swr_host_scene* hs, const swr_scene_desc& d) {
   if ((rc = I->alloc(&I->v.prim_box, 6 * (size_t)s->dev.num_slots))) return rc;
   if ((rc = I->alloc(&I->v.node_box, 6 * (size_t)s->dev.num_nodes))) return rc;
   if ((rc = I->alloc(&I->v.ext, 6))) return rc;
+  if (cudaMallocHost(&I->host_boxes, 6 * sizeof(float) * std::max<size_t>(I->v.no, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    I->host_boxes = nullptr;
+    return set_error(SWR_ERR_ALLOC, "CUDA: pinned host allocation failed");
+  }
+  SWR_CUDA(cudaEventCreateWithFlags(&I->boxes_ready, cudaEventDisableTiming));
   // tree levels from the node records: inner children of node n are child_base + i
   const uint32_t nn = s->dev.num_nodes;
   std::vector<uint32_t> words((size_t)nn * 20);
@@ -510,21 +531,11 @@ int swr_scene_set_transforms(swr_scene* s, const swr_object_transform* xf, uint3
   swr::k_inst_vertices<<<swr::blocks(I->v.nv, 256), 256, 0, stream>>>(I->v);
   swr::k_inst_objbox<<<swr::blocks((size_t)I->v.no * 32, 256), 256, 0, stream>>>(I->v, (float*)s->d_obj_boxes);
   SWR_CUDA(cudaGetLastError());
-  // tie ranks: the scene-level order of the moved objects' boxes (SceneBuilder::finish)
-  std::vector<float> boxes(6 * (size_t)n);
-  SWR_CUDA(cudaMemcpyAsync(boxes.data(), s->d_obj_boxes, boxes.size() * sizeof(float), cudaMemcpyDeviceToHost,
+  // the object boxes come back first; the triangle records, traversal boxes, refit and light
+  // tables (none of which needs the tie ranks) run on the GPU while the host orders the objects
+  SWR_CUDA(cudaMemcpyAsync(I->host_boxes, s->d_obj_boxes, 6 * sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost,
                            stream));
-  SWR_CUDA(cudaStreamSynchronize(stream));
-  for (float b : boxes)
-    if (!std::isfinite(b)) return set_error(SWR_ERR_INVALID, "swr: the transforms give non-finite coordinates");
-  const std::vector<uint32_t> order = swr::object_order(boxes.data(), n, I->exact);
-  std::vector<uint32_t> base(n, 0);
-  uint32_t acc = 0;
-  for (uint32_t o : order) {
-    base[o] = acc;
-    acc += I->obj_num_tris[o];
-  }
-  SWR_CUDA(cudaMemcpyAsync(I->v.base, base.data(), base.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+  SWR_CUDA(cudaEventRecord(I->boxes_ready, stream));
   const unsigned init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
   SWR_CUDA(cudaMemcpyAsync(I->v.ext, init, sizeof(init), cudaMemcpyHostToDevice, stream));
   swr::k_inst_derive<<<swr::blocks(I->v.nt, 256), 256, 0, stream>>>(I->v, s->dev, (float4*)s->d_tris,
@@ -536,6 +547,24 @@ int swr_scene_set_transforms(swr_scene* s, const swr_object_transform* xf, uint3
     if (e > b) swr::k_refit<<<swr::blocks(e - b, 128), 128, 0, stream>>>(I->v, (uint32_t*)s->d_nodes, b, e);
   }
   if (I->v.nlt) swr::k_inst_lights<<<swr::blocks(I->v.nlt, 128), 128, 0, stream>>>(I->v, (float4*)s->d_light_tris);
+  SWR_CUDA(cudaGetLastError());
+  // tie ranks: the scene-level order of the moved objects' boxes (SceneBuilder::finish)
+  SWR_CUDA(cudaEventSynchronize(I->boxes_ready));
+  const float* boxes = I->host_boxes;
+  for (size_t i = 0; i < 6 * (size_t)n; ++i)
+    if (!std::isfinite(boxes[i])) {
+      SWR_CUDA(cudaStreamSynchronize(stream));
+      return set_error(SWR_ERR_INVALID, "swr: the transforms give non-finite coordinates");
+    }
+  const std::vector<uint32_t> order = swr::object_order(boxes, n, I->exact);
+  std::vector<uint32_t> base(n, 0);
+  uint32_t acc = 0;
+  for (uint32_t o : order) {
+    base[o] = acc;
+    acc += I->obj_num_tris[o];
+  }
+  SWR_CUDA(cudaMemcpyAsync(I->v.base, base.data(), base.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+  swr::k_inst_rank<<<swr::blocks(I->v.nt, 256), 256, 0, stream>>>(I->v, s->dev, (float4*)s->d_tris);
   SWR_CUDA(cudaGetLastError());
   std::copy(xf, xf + n, I->xf.begin());
   SWR_CUDA(cudaStreamSynchronize(stream));  // the host arrays above go out of scope
