@@ -365,7 +365,9 @@ int swr_scene_create_from_host(const swr_host_scene* hs, const swr_build_opts* o
  * reference's triangle and object boxes, the light tables and the tie ranks (the scene-level
  * order of the moved objects' boxes) are rederived and the BVH is refit in place (topology kept,
  * boxes recomputed bottom-up and requantised). Hits and renders afterwards equal those of a scene
- * loaded from a file with the same placements. xf: [num_objects], host memory. */
+ * loaded from a file with the same placements. The host computes the objects' order while the GPU
+ * rederives and refits; the call returns once its work on stream has finished. xf: [num_objects],
+ * host memory. */
 int swr_scene_set_transforms(swr_scene* scene, const swr_object_transform* xf, uint32_t num_objects,
                              void* stream);
 

@@ -454,17 +454,23 @@ struct BdptArgs {
   uint32_t batch;     // lanes of a warp whose trace finished that advance their samples together
   uint32_t cbatch;    // the same for the connection queries
   uint32_t nsamp;     // samples of the chunk (pixels x spp)
-  float4* vtx;        // [3 * (vj + max(lj, 1)) * nsamp]: point, normal, throughput of vertex slot
-                      // k of sample q at (3k + field) * nsamp + q; vision vertex i is slot i,
+  float4* vtx;        // [3 * (vj + max(lj, 1)) * nsamp]: connection point (the vertex moved 0.01
+                      // along its normal), normal (vision vertices only) and throughput of vertex
+                      // slot k of sample q at (3k + field) * nsamp + q; vision vertex i is slot i,
                       // light vertex i slot vj + i
   uint4* head;        // [nsamp] first vision slot, vision end, light count, 1 = already resolved
 };
 
 enum BdptPhase : uint32_t { kVision = 0, kVisionDone = 1, kLight = 2 };
 
-__device__ __forceinline__ void bd_put(const BdptArgs& B, uint32_t slot, uint32_t q, f3 p, f3 n, f3 c) {
-  B.vtx[(size_t)(3 * slot + 0) * B.nsamp + q] = make_float4(p.x, p.y, p.z, 0.0f);
-  B.vtx[(size_t)(3 * slot + 1) * B.nsamp + q] = make_float4(n.x, n.y, n.z, 0.0f);
+// A connection runs from vision point + 0.01 * normal to light point + 0.01 * normal
+// (bidirectional_path_tracer.cpp:56-57); those points are stored, rounded as there. Only the
+// vision vertices' normals are read again (the cosine of a connection).
+__device__ __forceinline__ void bd_put(const BdptArgs& B, uint32_t slot, uint32_t q, f3 p, f3 n, f3 c,
+                                       bool vision) {
+  const f3 e = swrx::vadd(p, swrx::vscale(0.01f, n));
+  B.vtx[(size_t)(3 * slot + 0) * B.nsamp + q] = make_float4(e.x, e.y, e.z, 0.0f);
+  if (vision) B.vtx[(size_t)(3 * slot + 1) * B.nsamp + q] = make_float4(n.x, n.y, n.z, 0.0f);
   B.vtx[(size_t)(3 * slot + 2) * B.nsamp + q] = make_float4(c.x, c.y, c.z, 0.0f);
 }
 __device__ __forceinline__ f3 bd_get(const BdptArgs& B, uint32_t slot, uint32_t field, uint32_t q) {
@@ -570,7 +576,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
           const float cs = swrx::vdot(n, vision ? nd : prev);
           c = swrx::vmul(c, mk(__fmul_rn(m.m0.x, cs), __fmul_rn(m.m0.y, cs), __fmul_rn(m.m0.z, cs)));
         }
-        bd_put(B, (vision ? 0u : B.vj) + i, q, p, n, c);
+        bd_put(B, (vision ? 0u : B.vj) + i, q, p, n, c, vision);
         const bool light_hit = __float_as_uint(m.m1.w) != 0u && swrx::vdot(n, prev) <= 0.0f;
         ++i;
         if (light_hit || i >= (vision ? B.vj : B.lj)) {
@@ -615,7 +621,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
         ln = swrx::vadd(ln, swrx::vscale(b2, n2));
         ln = swrx::vnormalize(ln);
         const float4 lc = __ldg(sc.mats + 3 * (size_t)L.z);
-        bd_put(B, B.vj, q, lp, ln, mk(lc.x, lc.y, lc.z));
+        bd_put(B, B.vj, q, lp, ln, mk(lc.x, lc.y, lc.z), false);
         o = lp;
         d = swrx::hemisphere_dir(ln, U.u[1], U.u[2]);
         c = mk(1.0f, 1.0f, 1.0f);
@@ -634,7 +640,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
 }
 
 
-// Connections of one sample (bidirectional_path_tracer.cpp:70-96): for vi from the first vision
+// Connections of one sample (bidirectional_path_tracer.cpp:51-70): for vi from the first vision
 // slot, for li from 0, every pair with vi + li <= maxDepth is joined by an occlusion query between
 // the two points lifted by 0.01 along their normals; an unoccluded pair adds
 // (vision throughput * light throughput) * cos at the vision vertex. The sum, in that order, is
@@ -714,10 +720,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
         ++li;
         continue;
       }
-      const f3 vp = bd_get(B, vi, 0, q), vn = bd_get(B, vi, 1, q);
-      const f3 lp = bd_get(B, B.vj + li, 0, q), ln = bd_get(B, B.vj + li, 1, q);
-      const f3 a = swrx::vadd(vp, swrx::vscale(0.01f, vn));
-      const f3 b = swrx::vadd(lp, swrx::vscale(0.01f, ln));
+      const f3 a = bd_get(B, vi, 0, q), b = bd_get(B, B.vj + li, 0, q);
       const f3 dd = swrx::vsub(b, a);
       const float dist2 = swrx::vdot(dd, dd);
       dn = swrx::vnormalize(dd);
