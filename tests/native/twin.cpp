@@ -93,6 +93,13 @@ uint32_t twin_node_words(void* t, uint32_t* out) {
   return (uint32_t)w.size();
 }
 
+// copies the record slot -> triangle id map into out (if not null); returns the slot count
+uint32_t twin_slot_ids(void* t, uint32_t* out) {
+  const auto& v = ((Twin*)t)->pk.slot_to_id;
+  if (out) std::memcpy(out, v.data(), v.size() * 4);
+  return (uint32_t)v.size();
+}
+
 uint32_t twin_depth(void* t) { return ((Twin*)t)->pk.depth; }
 uint32_t twin_nodes(void* t) { return ((Twin*)t)->pk.num_nodes; }
 

@@ -87,3 +87,39 @@ def test_twin_physical_mode_matches_fp64_oracle(tmp_path):
     m = ps[..., :3].astype(np.float64).mean(1)
     # same paths, float vs double arithmetic: agreement to float rounding
     assert np.max(np.abs(m - pp64) / (np.abs(pp64) + 1e-3)) < 1e-4
+
+
+def test_host_builder_output_independent_of_thread_count(tmp_path):
+    """The host builder splits passes over large ranges and subtrees across threads; the tree,
+    its records and the slot order are the same for any thread count (a 524k-triangle terrain,
+    large enough for the split passes)."""
+    import ctypes
+    from master_thesis_b200 import _native as N
+    from helpers import build_twin
+    s = scenes.terrain(2, str(tmp_path), cells=512, tile=32, spheres=8, sphere_subdiv=2, lights=2)
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    L = ctypes.CDLL(build_twin())
+    P = ctypes.c_void_p
+    L.twin_create.restype = P
+    L.twin_create.argtypes = [P, P]
+    L.twin_destroy.argtypes = [P]
+    L.twin_node_words.argtypes = [P, P]
+    L.twin_node_words.restype = ctypes.c_uint32
+    L.twin_slot_ids.argtypes = [P, P]
+    L.twin_slot_ids.restype = ctypes.c_uint32
+    d = sd.desc()
+    out = []
+    for threads in (1, 3, 0):
+        o = N.BuildOpts(0, 0, threads, 0, 0, 0)
+        h = L.twin_create(ctypes.byref(d), ctypes.byref(o))
+        assert h
+        words = np.empty(L.twin_node_words(h, None), np.uint32)
+        L.twin_node_words(h, words.ctypes.data)
+        ids = np.empty(L.twin_slot_ids(h, None), np.uint32)
+        L.twin_slot_ids(h, ids.ctypes.data)
+        L.twin_destroy(h)
+        out.append((words, ids))
+    assert sd.num_triangles > 2 ** 19
+    assert np.array_equal(np.sort(out[0][1]), np.arange(sd.num_triangles, dtype=np.uint32))
+    for words, ids in out[1:]:
+        assert np.array_equal(words, out[0][0]) and np.array_equal(ids, out[0][1])
