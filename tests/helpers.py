@@ -67,7 +67,8 @@ class Twin:
         self._o = N.BuildOpts(sah_bins, max_leaf, 0, 0)
         self._h = Twin._lib.twin_create(ctypes.byref(self._d), ctypes.byref(self._o))
         if not self._h:
-            raise RuntimeError("twin_create failed: " + N.lib.swr_last_error().decode())
+            Twin._lib.swr_last_error.restype = ctypes.c_char_p  # the twin keeps its own error
+            raise RuntimeError("twin_create failed: " + Twin._lib.swr_last_error().decode())
 
     def __del__(self):
         if getattr(self, "_h", None):

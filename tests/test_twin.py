@@ -123,3 +123,48 @@ def test_host_builder_output_independent_of_thread_count(tmp_path):
     assert np.array_equal(np.sort(out[0][1]), np.arange(sd.num_triangles, dtype=np.uint32))
     for words, ids in out[1:]:
         assert np.array_equal(words, out[0][0]) and np.array_equal(ids, out[0][1])
+
+
+def _degenerate_scene(kind, rng):
+    """Triangles whose box centres are equal (stacked copies, copies on a lattice) or lie on one
+    line, as two objects."""
+    n = 1500
+    if kind == "stacked":  # copies of a few triangles: every centroid equal inside a copy group
+        base = rng.uniform(-1, 1, (4, 3, 3))
+        v = base[rng.integers(0, 4, n)]
+    elif kind == "collinear":  # triangles whose centroids lie on one line along x
+        x = rng.uniform(-1, 1, n)
+        v = np.stack([np.stack([x, np.zeros(n), np.zeros(n)], 1),
+                      np.stack([x + 0.01, np.full(n, 0.3), np.zeros(n)], 1),
+                      np.stack([x + 0.02, np.zeros(n), np.full(n, 0.3)], 1)], 1)
+    else:  # "points": one triangle shape placed on a coarse lattice, many copies at each place
+        c = np.round(rng.uniform(-1, 1, (n, 3)) * 3) / 3
+        v = c[:, None, :] + rng.uniform(-0.2, 0.2, (1, 3, 3))
+    v = v.astype(np.float32).reshape(-1, 3)
+    nrm = np.tile(np.float32([0, 1, 0]), (v.shape[0], 1))
+    tri = np.arange(v.shape[0], dtype=np.uint32).reshape(-1, 3)
+    tri_obj = (np.arange(n) >= n // 2).astype(np.uint32)
+    from master_thesis_b200.api import MAT_DTYPE, SceneData
+    mats = np.zeros(2, MAT_DTYPE)
+    mats["color"] = 0.5
+    mats["diffuse_t"] = 1.0
+    mats["refraction_index"] = 1.0
+    return SceneData(v, nrm, tri, tri_obj, np.array([0, 3 * (n // 2), 3 * n], np.uint32), mats,
+                     tri_rank=np.arange(n, dtype=np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["stacked", "collinear", "points"])
+@pytest.mark.parametrize("sah_bins", [0, 8])
+def test_twin_degenerate_geometry_matches_oracle(kind, sah_bins):
+    """The host builder's fallbacks (equal centroids: median split; empty centroid extents) and
+    the sparse SAH sweep of small ranges, through the traversal, against the oracle."""
+    rng = np.random.default_rng(len(kind) + sah_bins)
+    sd = _degenerate_scene(kind, rng)
+    tw = Twin(sd, sah_bins=sah_bins)
+    osc = O.OracleScene.from_scene_data(sd)
+    ro, rd = rays_uniform(20000, sd.vpos.min(0) - 0.2, sd.vpos.max(0) + 0.2, seed=5)
+    tri, d2, t = tw.trace(ro, rd)
+    otri, od2, ot = osc.trace(ro, rd)
+    assert np.array_equal(tri, otri)
+    assert np.array_equal(d2.view(np.uint32), od2.view(np.uint32))
+    assert np.mean(otri != 0xFFFFFFFF) > 0.01
