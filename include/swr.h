@@ -367,7 +367,8 @@ int swr_scene_create_from_host(const swr_host_scene* hs, const swr_build_opts* o
  * boxes recomputed bottom-up and requantised). Hits and renders afterwards equal those of a scene
  * loaded from a file with the same placements. The host computes the objects' order while the GPU
  * rederives and refits; the call returns once its work on stream has finished. xf: [num_objects],
- * host memory. */
+ * host memory. Placements whose products overflow to non-finite coordinates fail with
+ * SWR_ERR_INVALID and leave the scene unusable until a call with valid placements succeeds. */
 int swr_scene_set_transforms(swr_scene* scene, const swr_object_transform* xf, uint32_t num_objects,
                              void* stream);
 
