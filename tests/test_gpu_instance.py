@@ -161,3 +161,12 @@ def test_set_transforms_rejects_bad_requests(tmp_path):
     bad[2, 0] = np.nan
     with pytest.raises(swr.SwrError):
         moving.set_transforms(bad)
+    # finite placements whose products overflow: refused after the fact; valid ones then restore
+    # exact answers
+    huge = _xf(*p0)
+    huge[3, 0:6] = np.float32(3e38)  # position and scale: some vertex coordinate exceeds 3.4e38
+    with pytest.raises(swr.SwrError):
+        moving.set_transforms(huge)
+    moving.set_transforms(_xf(*p0))
+    ro, rd = rays_uniform(5000, (-1.6, -1.6, -1.6), (1.6, 1.6, 1.6), seed=4)
+    assert np.array_equal(_hits(moving, ro, rd), _hits(plain, ro, rd))
