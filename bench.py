@@ -62,6 +62,10 @@ CONFIGS = {
     # (swr_scene_set_transforms) and one 1920x1080 x 16 spp render per frame
     "c7": dict(kind="animate", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=16,
                depth=8, seed=2024, step=0.01),
+    # the same scene with a 480x270 x 4 spp image, for profiler captures of the update and
+    # device-builder kernels (about 2 GB on the device)
+    "c7s": dict(kind="animate", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=480, H=270, spp=4,
+                depth=8, seed=2024, step=0.01),
     # differentiable: tessellated Cornell (~49k triangles), 512x512, 32 spp primal + 32 spp adjoint, depth 6
     "c4": dict(kind="diff", W=512, H=512, spp=32, depth=6, seed=11),
     # batched inverse rendering: 64 scenes (5k-200k triangles, 128^2-512^2), 16 spp primal/adjoint, depth 5,
