@@ -22,10 +22,13 @@
 // -(y - x)), so with dmin the smallest pair distance, the smallest k whose nearest distance is
 // dmin has no partner at dmin before it (that partner would be a smaller such k), and its
 // nearest node is the smallest id at dmin after it: exactly the reference's (i, j). The pick is a
-// tournament-tree minimum of (nd[k], k). After a merge, the nodes that pointed at a or b query a
-// kd-tree for their new nearest node, c queries for its own, and a reverse query finds the nodes
-// to which c is strictly closer than their current nearest (c has the largest id, so it never
-// wins a tie). The kd-tree keeps, per subtree, a box around its live centres and the largest
+// tournament-tree minimum of (nd[k], k). After a merge, c queries a kd-tree for its nearest node,
+// and a reverse query finds the nodes to which c is strictly closer than their current nearest
+// (c has the largest id, so it never wins a tie). The nodes that pointed at a or b keep their old
+// distance as a lower bound (removals only lengthen nearest distances; c is covered by the reverse
+// query) and query again only when they reach the top of the tournament: a node at the top with a
+// current nearest node is the reference's pick, since every other node's true key is at least its
+// stored one. The kd-tree keeps, per subtree, a box around its live centres and the largest
 // nearest-distance inside; both queries prune with a lower bound on the float distance (the
 // geometric bound in double, less a relative 1e-5 and an absolute 1e-36 for rounding and
 // underflow), so every node that the exact float comparison would accept is examined.
@@ -173,7 +176,7 @@ class IndexedBuild {
         alive_(total_, 0),
         leaf_of_(total_, -1),
         pointed_(total_),
-        stamp_(total_, -1),
+        valid_(total_, 1),
         left_(left),
         right_(right) {
     for (int32_t i = 0; i < n_; ++i) {
@@ -212,9 +215,17 @@ class IndexedBuild {
     }
     for (int32_t i = 0; i < n_; ++i) tour_set(i);
     int32_t live = n_;
-    std::vector<int32_t> redo, closer;
+    std::vector<int32_t> closer;
     for (int32_t c = n_; c < total_; ++c) {
-      const int32_t a = tour_[1];
+      // the smallest (nd, id); a node whose nearest node has gone holds a lower bound there and
+      // is looked up again when it comes to the top
+      int32_t a = tour_[1];
+      while (!valid_[a]) {
+        nearest(a);
+        refresh_leaf(leaf_of_[a]);
+        tour_set(a);
+        a = tour_[1];
+      }
       const int32_t b = nn_[a];
       left_[c] = a;
       right_[c] = b;
@@ -235,25 +246,20 @@ class IndexedBuild {
       } else {
         insert(c);
       }
-      // nodes whose nearest node was a or b look again (c is already in the index)
-      redo.clear();
+      // nodes whose nearest node was a or b keep that distance as a lower bound: removing nodes
+      // only lengthens a nearest distance, and c (the one new node) is handled below
       for (int32_t dead : {a, b}) {
         for (int32_t k : pointed_[dead])
-          if (alive_[k] && nn_[k] == dead && stamp_[k] != c) {
-            stamp_[k] = c;
-            redo.push_back(k);
-          }
+          if (alive_[k] && nn_[k] == dead) valid_[k] = 0;
         std::vector<int32_t>().swap(pointed_[dead]);
       }
-      for (int32_t k : redo) nearest(k);
       nearest(c);
-      for (int32_t k : redo) refresh_leaf(leaf_of_[k]);
       refresh_leaf(leaf_of_[c]);
-      // nodes to which c is strictly closer than their nearest node
+      // nodes to which c is strictly closer than their nearest distance (or its lower bound):
+      // c is then their nearest node
       closer.clear();
       reverse(c, closer);
       for (int32_t k : closer) refresh_leaf(leaf_of_[k]);
-      for (int32_t k : redo) tour_set(k);
       for (int32_t k : closer) tour_set(k);
       tour_set(c);
     }
@@ -287,7 +293,7 @@ class IndexedBuild {
   std::vector<uint8_t> alive_;
   std::vector<int32_t> leaf_of_;
   std::vector<std::vector<int32_t>> pointed_;  // k with nn[k] == i at some time (checked on use)
-  std::vector<int32_t> stamp_;
+  std::vector<uint8_t> valid_;  // 0: nn[k] has gone and nd[k] is a lower bound of the nearest distance
   std::vector<int32_t>& left_;
   std::vector<int32_t>& right_;
   std::vector<Node> nodes_;
@@ -449,6 +455,7 @@ class IndexedBuild {
   void assign(int32_t k, int32_t j, float d) {
     nn_[k] = j;
     nd_[k] = d;
+    valid_[k] = 1;
     pointed_[j].push_back(k);
   }
 
