@@ -332,9 +332,10 @@ int swr_render_adjoint_batch(swr_batch* batch, const swr_adjoint_job* jobs, uint
  * that every device holds from the moment it loads the library until the process exits.
  * Limits: rgb_out (and samples_out when SWR_RENDER_SAMPLES_OUT is set) must be device memory;
  * spp <= 2^21; wave_size <= 65536 (0 = 65536); block_size 0 or 256; trace_blocks 0; no flag other
- * than SWR_RENDER_SAMPLES_OUT; larger requests are rejected with SWR_ERR_UNSUPPORTED. The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before capturing any stream on the device. All calls share the
+ * than SWR_RENDER_SAMPLES_OUT; larger requests are rejected with SWR_ERR_UNSUPPORTED. Every call
+ * looks up the array's device address (cudaGetSymbolAddress) with the scene's device current, so
+ * a cudaDeviceReset by the application between calls leaves no stale address; the first call on a
+ * device may load the module, so make it before capturing any stream on the device. All calls share the
  * one array, so calls that overlap on the GPU (other streams or host threads) race on it and must
  * be serialised by the caller. Results equal swr_render's for the same arguments. */
 int swr_render_noalloc(swr_scene* scene, const swr_camera* cam, const swr_render_opts* opts,
@@ -367,8 +368,9 @@ int swr_scene_create_from_host(const swr_host_scene* hs, const swr_build_opts* o
  * boxes recomputed bottom-up and requantised). Hits and renders afterwards equal those of a scene
  * loaded from a file with the same placements. The host computes the objects' order while the GPU
  * rederives and refits; the call returns once its work on stream has finished. xf: [num_objects],
- * host memory. Placements whose products overflow to non-finite coordinates fail with
- * SWR_ERR_INVALID and leave the scene unusable until a call with valid placements succeeds. */
+ * host memory. Placements whose products overflow to a non-finite world coordinate or normal (in
+ * any vertex, not only where the reference's boxes would show it) fail with SWR_ERR_INVALID and
+ * leave the scene unusable until a call with valid placements succeeds. */
 int swr_scene_set_transforms(swr_scene* scene, const swr_object_transform* xf, uint32_t num_objects,
                              void* stream);
 

@@ -95,7 +95,9 @@ def build_oracle(verbose=False):
     reference harness binaries (test infrastructure)."""
     oracle = os.path.join(ROOT, "oracle")
     _run(["make", "-s", "-C", oracle, "oracle"], verbose)
-    if os.path.isdir("/root/reference/software_renderer"):
+    # the reference checkout: SWR_REFERENCE, else the Makefile's default (absent on GPU machines)
+    ref = _run(["make", "-s", "-C", oracle, "print-ref"], False).strip()
+    if os.path.isdir(os.path.join(ref, "software_renderer")):
         _run(["make", "-s", "-j8", "-C", oracle, "ref"], verbose)
 
 

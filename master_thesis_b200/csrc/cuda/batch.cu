@@ -524,7 +524,9 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
       Q[k].hit = (uint2*)p; p += (size_t)cap * sizeof(uint2);
     }
   }
+  // zero-filled first: the struct's bytes, padding included, are the graph cache's key
   BArgs A;
+  std::memset(&A, 0, sizeof(A));
   A.jobs = (const BJob*)b->jobs;
   A.scenes = (const DevScene*)b->scenes;
   A.njobs = n;

@@ -49,6 +49,7 @@ struct InstView {
   float* node_box;              // [6 * nodes] exact union boxes
   uint32_t* order;              // nodes by level, deepest level first
   unsigned* ext;                // [6] ordered-int scene extent
+  unsigned* bad;                // [1] set when a world vertex or normal comes out non-finite
   uint32_t nv, nt, no, nlt;
 };
 
@@ -59,7 +60,7 @@ struct Instance {
   std::vector<swr_object_transform> xf;
   bool exact = true;
   std::vector<void*> allocs;
-  float* host_boxes = nullptr;          // pinned [6 * objects]: object boxes copied back
+  float* host_boxes = nullptr;          // pinned [6 * objects + 1]: object boxes, then the bad flag
   cudaEvent_t boxes_ready = nullptr;    // recorded after that copy
   Instance() { std::memset(&v, 0, sizeof(v)); }
   ~Instance() {
@@ -117,8 +118,14 @@ __global__ void k_inst_vertices(InstView I) {
   float r[4];
   xform(m, pv, r);
   I.vpos[v] = make_float4(r[0], r[1], r[2], 0.0f);
+  // The object box check on the host misses a NaN in any vertex but an object's first one (the
+  // reference's min/max keep the running bound against a NaN), and it never sees the normals:
+  // every product that leaves finite coordinates non-finite is flagged here.
+  bool bad = !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
   xform(m, nv, r);
   I.vnrm[v] = make_float4(r[0], r[1], r[2], 0.0f);
+  bad |= isfinite(n.x) && isfinite(n.y) && isfinite(n.z) && !(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]));
+  if (bad) *I.bad = 1u;
 }
 
 // AABB::addPoint (aabb.cpp:26-37): the first point padded by 1e-4, then std::min(a,b) =
@@ -447,7 +454,8 @@ int attach(swr_scene* s, const swr_host_scene* hs, const swr_scene_desc& d) {
   if ((rc = I->alloc(&I->v.prim_box, 6 * (size_t)s->dev.num_slots))) return rc;
   if ((rc = I->alloc(&I->v.node_box, 6 * (size_t)s->dev.num_nodes))) return rc;
   if ((rc = I->alloc(&I->v.ext, 6))) return rc;
-  if (cudaMallocHost(&I->host_boxes, 6 * sizeof(float) * std::max<size_t>(I->v.no, 1)) != cudaSuccess) {
+  if ((rc = I->alloc(&I->v.bad, 1))) return rc;
+  if (cudaMallocHost(&I->host_boxes, sizeof(float) * (6 * std::max<size_t>(I->v.no, 1) + 1)) != cudaSuccess) {
     cudaGetLastError();
     I->host_boxes = nullptr;
     return set_error(SWR_ERR_ALLOC, "CUDA: pinned host allocation failed");
@@ -528,6 +536,7 @@ int swr_scene_set_transforms(swr_scene* s, const swr_object_transform* xf, uint3
   std::vector<float> mats(16 * (size_t)n);
   for (uint32_t o = 0; o < n; ++o) swr::object_matrix(xf[o], mats.data() + 16 * (size_t)o);
   SWR_CUDA(cudaMemcpyAsync(I->v.mats, mats.data(), mats.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+  SWR_CUDA(cudaMemsetAsync(I->v.bad, 0, sizeof(unsigned), stream));
   swr::k_inst_vertices<<<swr::blocks(I->v.nv, 256), 256, 0, stream>>>(I->v);
   swr::k_inst_objbox<<<swr::blocks((size_t)I->v.no * 32, 256), 256, 0, stream>>>(I->v, (float*)s->d_obj_boxes);
   SWR_CUDA(cudaGetLastError());
@@ -535,6 +544,7 @@ int swr_scene_set_transforms(swr_scene* s, const swr_object_transform* xf, uint3
   // tables (none of which needs the tie ranks) run on the GPU while the host orders the objects
   SWR_CUDA(cudaMemcpyAsync(I->host_boxes, s->d_obj_boxes, 6 * sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost,
                            stream));
+  SWR_CUDA(cudaMemcpyAsync(I->host_boxes + 6 * (size_t)n, I->v.bad, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
   SWR_CUDA(cudaEventRecord(I->boxes_ready, stream));
   const unsigned init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
   SWR_CUDA(cudaMemcpyAsync(I->v.ext, init, sizeof(init), cudaMemcpyHostToDevice, stream));
@@ -551,11 +561,13 @@ int swr_scene_set_transforms(swr_scene* s, const swr_object_transform* xf, uint3
   // tie ranks: the scene-level order of the moved objects' boxes (SceneBuilder::finish)
   SWR_CUDA(cudaEventSynchronize(I->boxes_ready));
   const float* boxes = I->host_boxes;
-  for (size_t i = 0; i < 6 * (size_t)n; ++i)
-    if (!std::isfinite(boxes[i])) {
-      SWR_CUDA(cudaStreamSynchronize(stream));
-      return set_error(SWR_ERR_INVALID, "swr: the transforms give non-finite coordinates");
-    }
+  unsigned bad = 0;
+  std::memcpy(&bad, boxes + 6 * (size_t)n, sizeof(bad));
+  for (size_t i = 0; i < 6 * (size_t)n && !bad; ++i) bad = !std::isfinite(boxes[i]);
+  if (bad) {
+    SWR_CUDA(cudaStreamSynchronize(stream));
+    return set_error(SWR_ERR_INVALID, "swr: the transforms give non-finite coordinates or normals");
+  }
   const std::vector<uint32_t> order = swr::object_order(boxes, n, I->exact);
   std::vector<uint32_t> base(n, 0);
   uint32_t acc = 0;

@@ -1265,20 +1265,17 @@ static_assert(kNoAllocContribOffset + kNoAllocChunkSamples * sizeof(float4) <= k
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device. In host
-// code the array's name is only a stand-in for the symbol, never a device address.
-static int noalloc_scratch(int device, char** out) {
-  static std::mutex mu;
-  static char* addr[64] = {nullptr};
-  if (device < 0 || device >= 64) return set_error(SWR_ERR_UNSUPPORTED, "swr: device index above 63");
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    addr[device] = (char*)p;
-  }
-  *out = addr[device];
+// Device address of g_noalloc_scratch on the current device. In host code the array's name is
+// only a stand-in for the symbol, never a device address. The address is looked up on every call
+// rather than cached: the lookup allocates nothing once the module is loaded, and a cached address
+// would go stale if the host application reset the device (cudaDeviceReset reloads the module,
+// possibly elsewhere). The first call on a device may load the module (lazy loading), so that
+// call should come before any stream capture.
+static int noalloc_scratch(char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+  *out = (char*)p;
   return SWR_OK;
 }
 
@@ -1314,7 +1311,7 @@ int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
     return set_error(SWR_ERR_INVALID, "swr: swr_render_noalloc needs device output buffers (staging host "
                                       "memory would need a device allocation)");
   char* base = nullptr;
-  int rc = noalloc_scratch(s->device, &base);
+  int rc = noalloc_scratch(&base);
   if (rc) return rc;
 
   const uint64_t npix_total = (uint64_t)o->width * o->height;

@@ -15,6 +15,20 @@ REF_CLI = os.path.join(REF_DIR, "SoftwareRenderer")
 _KINDS = {"f": np.float32, "u": np.uint32}
 
 
+def reference_root():
+    """The reference checkout the harness is built from: SWR_REFERENCE, else oracle/Makefile's REF."""
+    ref = os.environ.get("SWR_REFERENCE")
+    if ref:
+        return ref
+    p = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True)
+    return p.stdout.strip()
+
+
+def reference_available():
+    """True when the reference sources and the compiled harness are both present."""
+    return os.path.isdir(os.path.join(reference_root(), "software_renderer")) and os.path.exists(HARNESS)
+
+
 def read(path):
     with open(path, "rb") as f:
         buf = f.read()

@@ -23,8 +23,8 @@ def _has_gpu():
 
 def pytest_collection_modifyitems(config, items):
     gpu = _has_gpu()
-    ref = os.path.isdir("/root/reference/software_renderer") and \
-        os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_harness"))
+    from oracle import refdump
+    ref = refdump.reference_available()
     for it in items:
         if "gpu" in it.keywords and not gpu:
             it.add_marker(pytest.mark.skip(reason="no CUDA GPU"))

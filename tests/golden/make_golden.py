@@ -21,7 +21,7 @@ from oracle import refdump  # noqa: E402
 from master_thesis_b200 import scenes  # noqa: E402
 from helpers import rays_uniform  # noqa: E402
 
-REF = "/root/reference"
+REF = refdump.reference_root()
 OUT = os.path.dirname(os.path.abspath(__file__))
 W, H, SPP, DEPTH, SEED = 32, 24, 4, 5, 20240601
 BD_VISION, BD_LIGHT, BD_MAX = 5, 5, 5  # res/renderer/SoftwareRendererBidirectionalPathTracer.renderer

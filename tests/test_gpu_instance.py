@@ -170,3 +170,28 @@ def test_set_transforms_rejects_bad_requests(tmp_path):
     moving.set_transforms(_xf(*p0))
     ro, rd = rays_uniform(5000, (-1.6, -1.6, -1.6), (1.6, 1.6, 1.6), seed=4)
     assert np.array_equal(_hits(moving, ro, rd), _hits(plain, ro, rd))
+
+
+def test_set_transforms_rejects_normals_that_overflow(tmp_path):
+    """A finite placement whose world positions stay finite while some world normals overflow: a
+    sphere of radius 1e-3 scaled by 3e38 in x and y and turned by a non-unit quaternion (|q|^2 =
+    1.414, 45 degrees about z), so the matrix rows hold +-3e38 and a normal near (1, 1, 0)/sqrt(2)
+    sums two of them past the float range. The object boxes are finite; the call must still fail,
+    and valid placements afterwards restore exact answers."""
+    root, base, cam_path, objs, rng = _setup(tmp_path)
+    pos, nrm, faces = scenes.icosphere_mesh(2)
+    write_obj(os.path.join(root, "res/obj/tiny.obj"), pos * np.float32(1e-3), nrm, faces)
+    objs = objs + [("tiny.obj", (0.5, 0.5, 0.5), None)]
+    p0 = _placements(rng, len(objs), 1.0)
+    path = _write_scene(root, "n", objs, *p0)
+    plain = swr.Scene(swr.load_scene(path, base))
+    moving = swr.Scene.from_file(path, base)
+    bad = _xf(*p0)
+    k = math.sqrt(1.414)
+    h = math.radians(22.5)
+    bad[-1] = np.array([0.0, 0.0, 0.0, 3e38, 3e38, 1.0, k * math.cos(h), 0.0, 0.0, k * math.sin(h)], np.float32)
+    with pytest.raises(swr.SwrError, match="normals"):
+        moving.set_transforms(bad)
+    moving.set_transforms(_xf(*p0))
+    ro, rd = rays_uniform(5000, (-1.6, -1.6, -1.6), (1.6, 1.6, 1.6), seed=6)
+    assert np.array_equal(_hits(moving, ro, rd), _hits(plain, ro, rd))

@@ -1,11 +1,14 @@
 """The oracle (C restatement) is pinned to the reference's own outputs: the golden fixtures were
 produced by the reference's code (tests/golden/make_golden.py); here the oracle must reproduce
 them bit for bit. When the compiled reference is available it is also compared live."""
+import os
+
 import numpy as np
 import pytest
 
 from helpers import GOLDEN_CASES, golden, golden_camera, golden_scene, ref_pixel_from_samples, rays_uniform
 from oracle import oracle as O
+from oracle import refdump
 
 
 PHILOX_KAT = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
@@ -96,11 +99,11 @@ def test_oracle_bdpt_matches_reference(name):
 @pytest.mark.reference
 def test_oracle_matches_live_reference_on_fresh_rays(tmp_path):
     """Fresh seeded rays through the compiled reference (not just the stored fixture)."""
-    from oracle import refdump
     import master_thesis_b200 as swr
-    base = "/root/reference/build/"
+    ref = refdump.reference_root()
+    base = os.path.join(ref, "build") + "/"
     for sc_name in ["cornell_box_with_ball", "labyrinth"]:
-        scene = "/root/reference/res/scene/%s.scene" % sc_name
+        scene = os.path.join(ref, "res/scene/%s.scene" % sc_name)
         D = swr.load_scene(scene, base)
         osc = O.OracleScene.from_scene_data(D)
         ro, rd = rays_uniform(20000, D.vpos.min(0) - 0.2, D.vpos.max(0) + 0.2, seed=123)

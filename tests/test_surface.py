@@ -8,8 +8,9 @@ import pytest
 import master_thesis_b200 as swr
 from master_thesis_b200 import scenes
 from helpers import GOLDEN_CASES, golden
+from oracle import refdump
 
-REF = "/root/reference"
+REF = refdump.reference_root()
 
 
 def _bits(a):

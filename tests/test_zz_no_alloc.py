@@ -77,3 +77,27 @@ def test_noalloc_samples_and_limits(tmp_path):
                                   torch.cuda.current_stream().cuda_stream)
     assert rc == N.SWR_ERR_INVALID
     sc.close()
+
+
+def test_noalloc_samples_vs_oracle(tmp_path):
+    """The allocation-free render against the oracle directly, per sample, over more samples than
+    one chunk of its fixed scratch holds (2^21), so the chunk loop is checked too."""
+    from oracle import oracle as O
+    s = scenes.cornell(7, str(tmp_path))
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    sc = swr.Scene(sd)
+    W, H, spp, depth, seed = 160, 120, 128, 5, 21
+    cam = swr.load_camera(s["camera"], W, H)
+    o = N.RenderOpts(W, H, spp, depth, seed, 0, 0, 1.0, 0, 0, N.RENDER_SAMPLES_OUT, 0, 0, 0)
+    out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    got = torch.zeros((H * W, spp, 4), dtype=torch.float32, device="cuda")
+    N.check(_noalloc(sc, cam, o, out, got))
+    torch.cuda.synchronize()
+    vi, pi, org = swr.camera_arrays(cam)
+    ps, pp = O.render_reference(O.OracleScene.from_scene_data(sd), O.camera(vi, pi, org), W, H, spp, depth, seed)
+    g = got.cpu().numpy()
+    assert np.array_equal(g[..., 3], ps[..., 3])
+    assert np.allclose(g[..., :3], ps[..., :3], rtol=RTOL, atol=ATOL)
+    assert np.allclose(out.cpu().numpy().reshape(-1, 3), pp, rtol=RTOL, atol=ATOL)
+    assert ps[..., 3].sum() > 0
+    sc.close()
