@@ -163,28 +163,45 @@ def profile_traffic():
         return json.load(f)
 
 
-def cpu_reference(cfg, files, threads, budget_s, impl_bin):
+def cpu_reference(cfg, files, threads, target_s, impl_bin, timed=1, warm=0):
     """Times the reference's own PathTracer or BidirectionalPathTracer (unmodified sources) on a
-    bounded pixel sample."""
+    bounded pixel sample (every k-th pixel of the image), sized by an untimed probe inside the same
+    process so that one pass takes about target_s; `warm` untimed and `timed` timed passes over
+    that sample follow one scene load."""
     W, H, spp, depth = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
-    fast = ["fast"] if cfg["kind"] == "terrain" else []
+    extra = ["fast"] if cfg["kind"] == "terrain" else []
     if cfg.get("renderer") == "bdpt":
-        fast += ["bdpt", str(cfg["light_jumps"]), str(cfg["max_depth"])]
+        extra += ["bdpt", str(cfg["light_jumps"]), str(cfg["max_depth"])]
+    extra += ["passes", str(timed), str(warm), "target", str(target_s)]
+    out = subprocess.run([impl_bin, files["basepath"], files["scene"], files["camera"], str(W), str(H), str(spp),
+                          str(depth), str(threads), str(W * H)] + extra, capture_output=True, text=True,
+                         timeout=3600)
+    if out.returncode != 0:
+        raise RuntimeError("ref_bench failed: " + out.stderr[-2000:])
+    return json.loads(out.stdout.strip().splitlines()[-1])
 
-    def run(pixels):
-        out = subprocess.run([impl_bin, files["basepath"], files["scene"], files["camera"], str(W), str(H), str(spp),
-                              str(depth), str(threads), str(pixels)] + fast, capture_output=True, text=True,
-                             timeout=1800)
-        if out.returncode != 0:
-            raise RuntimeError("ref_bench failed: " + out.stderr[-2000:])
-        return json.loads(out.stdout.strip().splitlines()[-1])
 
-    probe = run(max(threads, 8))
-    rate = probe["samples"] / max(probe["render_s"], 1e-6)
-    pixels = int(max(threads * 2, min(W * H, budget_s * rate / spp)))
-    res = run(pixels)
-    res["load_s_probe"] = probe["load_s"]
-    return res
+def scene_objects(scene_path):
+    """Number of objects a scene file lists (entries start at column 0, keys are indented)."""
+    with open(scene_path) as f:
+        return sum(1 for line in f if line.strip() and not line[0].isspace())
+
+
+def bench_config(cfg, files, world, workload, split="images"):
+    """The `config` object of the JSON line; both arms print the identical dict."""
+    W, H = cfg["W"], cfg["H"]
+    par = {"images": "independent images per GPU", "spp": "one image split by sample range over GPUs "
+           "(all_reduce of the image)", "tiles": "one image split by pixel tile over GPUs (all_gather)"}[split]
+    c = {"workload": workload, "objects": scene_objects(files["scene"]), "pixels": W * H, "spp": cfg["spp"],
+         "depth": cfg["depth"], "l2": "flushed between steps (256 MB write)",
+         "parallelism": par if world > 1 else "single GPU"}
+    if "triangles" in files:
+        c["triangles"] = int(files["triangles"])
+    if cfg.get("renderer") == "bdpt":
+        c.update(vision_jumps=cfg["depth"], light_jumps=cfg["light_jumps"], max_depth=cfg["max_depth"])
+    elif cfg.get("renderer") != "rt":
+        c["wave_size"] = cfg.get("wave_size", 0) or (1 << 23)
+    return c
 
 
 def traversal_microbench(scene, sd, n, steps, flush, stream):
@@ -338,16 +355,16 @@ def run_bdpt(args, cfg, files, workload):
         "metric": "Msamples/s (bidirectional path tracer)", "value": samples / (t / 1e3) / 1e6, "unit": "Msamples/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
-        "config": {"workload": workload, "vision_jumps": vj, "light_jumps": lj, "max_depth": md,
-                   "l2": "flushed between steps (256 MB write)"},
+        "config": bench_config(cfg, files, 1, workload),
         "e2e": {"value": samples / (sum(e2e) / len(e2e) / 1e3) / 1e6, "unit": "Msamples/s", "h2d_bytes_per_step": 96,
                 "d2h_bytes_per_step": W * H * 12},
         "clocks": clk, "cpu_baseline": cpu}))
 
 
-def rt_cpu_port(cfg, files, threads, budget_s):
-    """The oracle's CPU restatement of the RayTrace PathTracer timed on a bounded run of whole
-    image rows through the image centre (all host threads)."""
+def rt_cpu_port(cfg, files, threads, target_s, timed=1, warm=0):
+    """The oracle's CPU restatement of the RayTrace PathTracer timed on whole image rows through the
+    image centre (all host threads): an untimed probe row sizes the sample so that one pass takes
+    about target_s, then `warm` untimed and `timed` timed passes over it."""
     import master_thesis_b200 as swr
     from oracle import oracle as O
     W, H, spp, vj = cfg["W"], cfg["H"], cfg["spp"], cfg["depth"]
@@ -359,12 +376,43 @@ def rt_cpu_port(cfg, files, threads, budget_s):
     t0 = time.time()
     O.rt_render(osc, ocam, W, H, spp, vj, mid, mid + W, threads=threads)
     rate = W / max(time.time() - t0, 1e-6)
-    rows = int(max(1, min(H, budget_s * rate / W)))
+    rows = int(max(1, min(H, target_s * rate / W)))
     p0 = max(0, (H - rows) // 2) * W
-    t0 = time.time()
-    O.rt_render(osc, ocam, W, H, spp, vj, p0, p0 + rows * W, threads=threads)
-    dt = time.time() - t0
-    return {"msamples_per_s": rows * W * spp / dt / 1e6, "pixels": rows * W, "rows": rows, "seconds": dt}
+    for _ in range(warm):
+        O.rt_render(osc, ocam, W, H, spp, vj, p0, p0 + rows * W, threads=threads)
+    pass_s = []
+    for _ in range(timed):
+        t0 = time.time()
+        O.rt_render(osc, ocam, W, H, spp, vj, p0, p0 + rows * W, threads=threads)
+        pass_s.append(time.time() - t0)
+    dt = sum(pass_s)
+    return {"msamples_per_s": rows * W * spp * timed / dt / 1e6, "pixels": rows * W, "rows": rows, "seconds": dt,
+            "pass_s": pass_s, "timed_passes": timed, "warmup_passes": warm}
+
+
+def reference_line(args, cfg, files, workload, metric, r, kind, sample):
+    """The reference arm's JSON line: one step = one pass over the bounded pixel sample, timed on
+    the host cores; steps/warmup are the passes actually run."""
+    W, H, spp = cfg["W"], cfg["H"], cfg["spp"]
+    v = r["msamples_per_s"]
+    nproc = os.cpu_count() or 1
+    pass_ms = [1e3 * x for x in r["pass_s"]]
+    return {
+        "impl": "reference", "metric": metric, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
+        "steps": r["timed_passes"], "warmup": r["warmup_passes"], "ms_per_step": sum(pass_ms) / len(pass_ms),
+        "step": "one pass over the sampled pixels (%d of %d, %d spp each)" % (r["pixels"], W * H, spp),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene files)",
+        "config": bench_config(cfg, files, args.gpus, workload, args.split if args.gpus > 1 else "images"),
+        "sample_pixels": r["pixels"],
+        "full_image_ms_estimate": W * H * spp / (v * 1e6) * 1e3,
+        "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": nproc, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def reference_pass_target(args):
+    """Seconds per reference pass: about a minute of CPU rendering for the whole run."""
+    return min(10.0, max(0.2, 60.0 / max(1, args.steps + args.warmup)))
 
 
 def run_rt(args, cfg, files, workload):
@@ -421,8 +469,7 @@ def run_rt(args, cfg, files, workload):
         "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scene files)",
-        "config": {"workload": workload, "triangles": int(sd.num_triangles), "l2": "flushed between steps (256 MB write)",
-                   "launch": shape},
+        "config": bench_config(cfg, files, 1, workload), "launch": shape,
         "e2e": {"value": samples / (e2e / 1e3) / 1e6, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": W * H * 4},
         "gpu_launches": 1 * args.steps,
@@ -697,6 +744,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scene-dir", default=None)
     ap.add_argument("--tune", action="store_true", help="autotune the launch shape (cached) before timing")
+    ap.add_argument("--split", default="images", choices=["images", "spp", "tiles"],
+                    help="with N>1: independent images per GPU (weak scaling) or one image split by sample "
+                         "range / pixel tile over the GPUs (strong scaling)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if cfg["kind"] in ("batch", "diff", "inverse", "animate"):
@@ -741,16 +791,10 @@ def main():
         # cannot bring up: its CPU restatement (the oracle) stands in as the reference arm
         if rank != 0:
             return
-        r = rt_cpu_port(cfg, files, nproc, args.cpu_budget * max(1, args.steps // 5))
-        v = r["msamples_per_s"]
-        sample = "%d image rows (%d of %d pixels), %d spp, %d threads" % (r["rows"], r["pixels"], W * H, spp, nproc)
-        print(json.dumps({
-            "impl": "reference", "metric": metric, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": W * H * spp / (v * 1e6) * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene files)", "config": {"workload": workload},
-            "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": nproc, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        r = rt_cpu_port(cfg, files, nproc, reference_pass_target(args), args.steps, args.warmup)
+        sample = "%d image rows (%d of %d pixels), %d spp, %d threads; one pass per step" % (
+            r["rows"], r["pixels"], W * H, spp, nproc)
+        print(json.dumps(reference_line(args, cfg, files, workload, metric, r, "port", sample)))
         return
     if args.impl == "reference":
         if rank != 0:
@@ -759,17 +803,13 @@ def main():
         if not os.path.exists(refdump.REF_BENCH):
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench was not built"}))
             return
-        res = cpu_reference(cfg, files, nproc, args.cpu_budget * max(1, args.steps // 5), refdump.REF_BENCH)
-        v = res["msamples_per_s"]
-        sample = "%d of %d pixels (every k-th), %d spp, depth %d, %d threads" % (res["pixels"], W * H, spp, depth, nproc)
-        print(json.dumps({
-            "impl": "reference", "metric": metric, "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": W * H * spp / (v * 1e6) * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene files)", "config": {"workload": workload},
-            "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": nproc, "kind": "reference", "sample": sample},
-            "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_load_s": res["load_s"]}))
+        r = cpu_reference(cfg, files, nproc, reference_pass_target(args), refdump.REF_BENCH, args.steps,
+                          args.warmup)
+        sample = ("%d of %d pixels (every k-th), %d spp, depth %d, %d threads; one pass per step; reference "
+                  "load+build %.1f s" % (r["pixels"], W * H, spp, depth, nproc, r["load_s"]))
+        line = reference_line(args, cfg, files, workload, metric, r, "reference", sample)
+        line["reference_load_s"] = r["load_s"]
+        print(json.dumps(line))
         return
 
     import torch
@@ -802,14 +842,36 @@ def main():
     torch.cuda.synchronize()
     t4 = time.time()
     cam = swr.load_camera(files["camera"], W, H)
-    seed = 1000 + rank
+    # images: every rank renders its own image (seed 1000 + rank); spp / tiles: all ranks render
+    # one image (seed 1000) split by sample range or pixel tile (sharding.render_split)
+    split = args.split  # with one GPU a split renders the whole image as its one part
+    if split == "spp" and spp < world:
+        raise SystemExit("--split spp needs at least one sample per pixel per rank")
+    seed = 1000 + rank if split == "images" else 1000
     out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
     def render(o, **kw):
-        return scene.render(cam, W, H, spp, depth, seed=seed, out=o, stream=stream, return_profile=True,
-                            wave_size=cfg.get("wave_size", 0), **kw)
+        if split == "images":
+            return scene.render(cam, W, H, spp, depth, seed=seed, out=o, stream=stream, return_profile=True,
+                                wave_size=cfg.get("wave_size", 0), **kw)
+        profile = []
+
+        def part(pb, pc, sb, sc):
+            r, pr = scene.render(cam, W, H, sc, depth, seed=seed, stream=stream, return_profile=True,
+                                 wave_size=cfg.get("wave_size", 0), pixel_begin=pb, pixel_count=pc, sample_begin=sb,
+                                 spp_total=spp, **kw)
+            profile.append(pr)
+            return r.reshape(pc, 3)
+
+        img = sharding.render_split(part, W, H, spp, rank, world, split=split, device="cuda")
+        if isinstance(o, np.ndarray):
+            torch.from_numpy(o).copy_(img, non_blocking=True)  # pinned host memory
+            profile[-1]["d2h_bytes"] = W * H * 12
+        else:
+            o.copy_(img)
+        return o, profile[-1]
 
     for _ in range(max(args.warmup, 3)):
         render(out)
@@ -868,9 +930,10 @@ def main():
     barrier()
     clk = clocks.stop()
 
-    # the job's time is the slowest rank's (device time, each rank rendering its own images)
+    # the job's time is the slowest rank's (device time, each rank rendering its own images or
+    # its part of the shared image)
     total_ms, total_e2e_ms = sharding.max_over_ranks([sum(step_ms), sum(e2e_ms)])
-    samples = W * H * spp * world * args.steps
+    samples = W * H * spp * (world if split == "images" else 1) * args.steps
     value = samples / (total_ms / 1e3) / 1e6
     e2e_value = samples / (total_e2e_ms / 1e3) / 1e6
 
@@ -919,12 +982,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
-            "config": {"workload": workload, "triangles": int(sd.num_triangles), "objects": int(sd.num_objects),
-                       "pixels": W * H, "spp": spp, "depth": depth, "l2": "flushed between steps (256 MB write)",
-                       "parallelism": "independent images per GPU" if world > 1 else "single GPU",
-                       "wave_size": cfg.get("wave_size", 0) or (1 << 23),
-                       "bvh_nodes": stats["nodes"], "bvh_depth": stats["depth"]},
+            "scaling": "weak" if split == "images" else "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene files)",
+            "config": bench_config(cfg, files, world, workload, split),
+            "bvh": {"nodes": stats["nodes"], "depth": stats["depth"]},
             "e2e": {"value": e2e_value, "unit": "Msamples/s",
                     "h2d_bytes_per_step": int(e2e_prof[-1]["h2d_bytes"]),
                     "d2h_bytes_per_step": int(e2e_prof[-1]["d2h_bytes"]),

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define SWR_ABI_VERSION 2
+#define SWR_ABI_VERSION 3
 
 enum {
   SWR_OK = 0,
@@ -123,6 +123,22 @@ typedef struct swr_render_opts {
   uint32_t shade_batch;    /* adjoint: lanes of a warp with a pending hit that shade together
                               (1..32; fewer when no trace of the warp is in flight), 0 = the
                               library's choice; the wavefront renders ignore it */
+  /* Part of an image, for splitting one image over several calls or GPUs (the reference's
+   * engine splits one image over host threads by pixel, graphics_engine.cpp:49-56,73-74).
+   * Sample range (swr_render, swr_render_profiled, swr_render_adjoint): samples
+   * [sample_begin, sample_begin + spp) of every pixel of an image with spp_total samples per
+   * pixel; the random numbers are those of the whole image's samples and the output is scaled by
+   * the whole image's 1/spp_total (times 2 pi in reference mode), so the outputs of calls over a
+   * partition of [0, spp_total) sum to the whole image up to float summation order, and their
+   * adjoint gradients sum to the whole image's gradient. spp_total 0 = spp (the whole range).
+   * Pixel range (swr_render, swr_render_profiled): pixels [pixel_begin, pixel_begin +
+   * pixel_count) of the width x height image in row-major order; rgb_out then holds pixel_count
+   * pixels (and samples_out pixel_count * spp samples), bit-identical to those pixels of a whole
+   * image. pixel_count 0 = to the end of the image. The other entry points require all four 0. */
+  uint32_t sample_begin;
+  uint32_t spp_total;
+  uint32_t pixel_begin;
+  uint32_t pixel_count;
 } swr_render_opts;
 
 #define SWR_RENDER_SAMPLES_OUT 1u   /* write per-sample radiance to the samples buffer */

@@ -73,7 +73,8 @@ class RenderOpts(ctypes.Structure):
                 ("rr_depth", ctypes.c_uint32), ("rr_survive", ctypes.c_float),
                 ("wave_size", ctypes.c_uint32), ("block_size", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("refill", ctypes.c_uint32), ("trace_blocks", ctypes.c_uint32),
-                ("shade_batch", ctypes.c_uint32)]
+                ("shade_batch", ctypes.c_uint32), ("sample_begin", ctypes.c_uint32), ("spp_total", ctypes.c_uint32),
+                ("pixel_begin", ctypes.c_uint32), ("pixel_count", ctypes.c_uint32)]
 
 
 class RenderProfile(ctypes.Structure):

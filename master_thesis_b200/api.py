@@ -238,16 +238,24 @@ class Scene:
     def render(self, cam, width, height, spp, depth, seed=0, mode=N.MODE_REFERENCE, rr_depth=0,
                rr_survive=1.0, wave_size=0, block_size=0, out=None, samples=None, stream=None,
                profile=False, count=False, return_profile=False, static_fetch=False, refill=0,
-               trace_blocks=0):
+               trace_blocks=0, sample_begin=0, spp_total=0, pixel_begin=0, pixel_count=0):
         """Renders an image (height, width, 3) float32 into `out` (torch cuda tensor or numpy array;
-        a numpy array makes the library stage the result through the device)."""
+        a numpy array makes the library stage the result through the device).
+
+        Part of an image: samples [sample_begin, sample_begin + spp) of an image of spp_total
+        samples per pixel (scaled by that image's 1/spp_total, so parts over a partition of the
+        samples sum to the image), and/or pixels [pixel_begin, pixel_begin + pixel_count) in
+        row-major order (out then holds (pixel_count, 3) floats, bit-identical to those pixels of
+        the whole image)."""
         flags = (N.RENDER_SAMPLES_OUT if samples is not None else 0) | (N.RENDER_PROFILE if profile else 0) | \
             (N.RENDER_COUNT if count else 0) | (N.RENDER_STATIC_FETCH if static_fetch else 0)
         o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size, block_size, flags,
-                         refill, trace_blocks, 0)
+                         refill, trace_blocks, 0, sample_begin, spp_total, pixel_begin, pixel_count)
         if out is None:
             import torch
-            out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+            shape = (pixel_count or width * height - pixel_begin, 3) if (pixel_begin or pixel_count) else \
+                (height, width, 3)
+            out = torch.empty(shape, dtype=torch.float32, device="cuda")
         s = _stream_handle(stream)
         prof = N.RenderProfile()
         check(N.lib.swr_render_profiled(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(out), ptr(samples),
@@ -266,15 +274,17 @@ def _scene_set_emission(self, emission, stream=None):
 
 
 def _scene_render_adjoint(self, cam, width, height, spp, depth, dl_dimage, seed=0, rr_depth=0, rr_survive=1.0,
-                          refill=0, stream=None, return_ms=False, shade_batch=0):
+                          refill=0, stream=None, return_ms=False, shade_batch=0, sample_begin=0, spp_total=0):
     """Gradients (albedo [num_triangles,3], emission [num_objects,3]) of sum(dl_dimage * image) for
-    the physical-mode image rendered with the same arguments (path replay). Device tensors."""
+    the physical-mode image rendered with the same arguments (path replay). Device tensors. With a
+    sample range (sample_begin, spp_total) the gradient covers those samples only, weighted by the
+    whole image's 1/spp_total, so gradients over a partition of the samples sum to the image's."""
     import torch
     dl = dl_dimage.contiguous()
     ga = torch.empty((self.data.num_triangles, 3), dtype=torch.float32, device=dl.device)
     ge = torch.empty((self.data.num_objects, 3), dtype=torch.float32, device=dl.device)
     o = N.RenderOpts(width, height, spp, depth, seed, N.MODE_PHYSICAL, rr_depth, rr_survive, 0, 0, 0, refill, 0,
-                     shade_batch)
+                     shade_batch, sample_begin, spp_total, 0, 0)
     ms = ctypes.c_double(0.0)
     check(N.lib.swr_render_adjoint_timed(self._h, ctypes.byref(cam), ctypes.byref(o), ptr(dl), ptr(ga), ptr(ge),
                                          _stream_handle(stream), ctypes.byref(ms) if return_ms else None))

@@ -428,6 +428,8 @@ int add_job(int device, const swr_scene* scene, const swr_camera& cam, const swr
   if (o.mode > 1) return set_error(SWR_ERR_INVALID, "swr: unknown mode");
   if (o.mode == 1 && o.rr_depth && !(o.rr_survive > 0.0f && o.rr_survive <= 1.0f))
     return set_error(SWR_ERR_INVALID, "swr: rr_survive must be in (0, 1]");
+  if (o.sample_begin || o.spp_total || o.pixel_begin || o.pixel_count)
+    return set_error(SWR_ERR_UNSUPPORTED, "swr: batch jobs render whole images (the range fields must be 0)");
   uint32_t si = 0;
   while (si < uniq.size() && uniq[si] != scene) ++si;
   if (si == uniq.size()) {

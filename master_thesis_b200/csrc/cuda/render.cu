@@ -64,6 +64,9 @@ struct Frame {
   uint64_t seed;
   uint32_t pixel0;   // first pixel of the chunk
   uint32_t npix;     // pixels in the chunk
+  uint32_t out0;     // pixel whose result goes to the start of the output image (pixel ranges)
+  uint32_t sample0;  // image sample index of the call's first sample (sample ranges)
+  uint32_t spp_scale;  // samples per pixel of the whole image: the resolve's and adjoint's 1/spp
   uint32_t capacity;
   uint32_t refill;   // idle lanes that trigger a refill in the bounce traversal
   uint32_t batch;    // adjoint: lanes with a finished trace that shade together
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(kBlock)
       swrx::ShadeParams P;
       P.seed = F.seed;
       P.pixel = F.pixel0 + pixel;
-      P.sample = sample;
+      P.sample = F.sample0 + sample;
       P.depth = F.depth;
       P.mode = F.mode;
       P.rr_depth = F.rr_depth;
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(kTraceBlock)
   bool active = false, tracing = false, exhausted = false;
   uint32_t pend_slot = 0;
   float pend_t = 0.0f;
-  const float inv_spp = 1.0f / (float)F.spp;
+  const float inv_spp = 1.0f / (float)F.spp_scale;
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     if (!exhausted && (unsigned)__popc(idle) >= F.refill) {
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(kTraceBlock)
     swrx::ShadeParams P;
     P.seed = F.seed;
     P.pixel = F.pixel0 + pixel;
-    P.sample = sample;
+    P.sample = F.sample0 + sample;
     P.depth = F.depth;
     P.mode = 1;
     P.rr_depth = F.rr_depth;
@@ -746,9 +749,9 @@ __global__ void k_resolve(Frame F, float* __restrict__ img) {
     }
   }
   // reference: finalColor *= 2.0f * M_PI * (1.0f / float(spp)), scalar and products in double
-  const float inv = __fdiv_rn(1.0f, (float)F.spp);
+  const float inv = __fdiv_rn(1.0f, (float)F.spp_scale);
   const double s = (F.mode == 0) ? __dmul_rn(6.283185307179586, (double)inv) : (double)inv;
-  float* o = img + (size_t)(F.pixel0 + k) * 3;
+  float* o = img + (size_t)(F.pixel0 - F.out0 + k) * 3;
   o[0] = __double2float_rn(__dmul_rn((double)r, s));
   o[1] = __double2float_rn(__dmul_rn((double)g, s));
   o[2] = __double2float_rn(__dmul_rn((double)b, s));
@@ -837,6 +840,33 @@ enum { kTimeTrace = 0, kTimeShade = 1, kTimeCamera = 2, kTimeResolve = 3 };
 
 }  // namespace
 
+// The part of the image a call renders (swr_render_opts: sample_begin, spp_total, pixel_begin,
+// pixel_count). allow_pixels: the entry point supports pixel ranges; allow_samples: sample ranges.
+struct ImagePart {
+  uint32_t sample0 = 0, spp_scale = 0;
+  uint64_t pixel0 = 0, npix = 0;
+};
+
+static int image_part(const swr_render_opts* o, bool allow_samples, bool allow_pixels, ImagePart* part,
+                      const char* who) {
+  const uint64_t total = (uint64_t)o->width * o->height;
+  part->sample0 = o->sample_begin;
+  part->spp_scale = o->spp_total ? o->spp_total : o->spp;
+  part->pixel0 = o->pixel_begin;
+  part->npix = o->pixel_count ? o->pixel_count : (o->pixel_begin < total ? total - o->pixel_begin : 0);
+  const bool samples = o->sample_begin != 0 || o->spp_total != 0;
+  const bool pixels = o->pixel_begin != 0 || o->pixel_count != 0;
+  if (samples && !allow_samples) return set_error(SWR_ERR_UNSUPPORTED, std::string("swr: ") + who +
+                                                  " renders whole images (sample_begin and spp_total must be 0)");
+  if (pixels && !allow_pixels) return set_error(SWR_ERR_UNSUPPORTED, std::string("swr: ") + who +
+                                                " renders whole images (pixel_begin and pixel_count must be 0)");
+  if ((uint64_t)o->sample_begin + o->spp > part->spp_scale)
+    return set_error(SWR_ERR_INVALID, "swr: sample_begin + spp exceeds spp_total");
+  if (o->pixel_begin >= total || part->npix == 0 || (uint64_t)o->pixel_begin + part->npix > total)
+    return set_error(SWR_ERR_INVALID, "swr: pixel range outside the image");
+  return SWR_OK;
+}
+
 int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, float* rgb_out,
                 float* samples_out, void* stream_, swr_render_profile* prof) {
   if (!s || !cam || !o || !rgb_out) return set_error(SWR_ERR_INVALID, "swr: null argument");
@@ -854,6 +884,9 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   int block = o->block_size ? (int)o->block_size : 256;
   if (block != 128 && block != 256 && block != 512)
     return set_error(SWR_ERR_INVALID, "swr: block_size must be 128, 256 or 512");
+  ImagePart part;
+  int rc = image_part(o, true, true, &part, "swr_render");
+  if (rc) return rc;
   cudaStream_t stream = (cudaStream_t)stream_;
   SWR_CUDA(cudaSetDevice(s->device));
   RenderWorkspace* ws = workspace_of(s);
@@ -864,12 +897,12 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   timer.on = (o->flags & SWR_RENDER_PROFILE) != 0;
   const bool count = (o->flags & SWR_RENDER_COUNT) != 0;
 
-  const uint64_t npix_total = (uint64_t)o->width * o->height;
+  // the pixels this call renders (the whole image unless a pixel range is given)
+  const uint64_t npix_total = part.npix;
   const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
   uint32_t cap = o->wave_size ? o->wave_size : (1u << 23);
   cap = (uint32_t)std::min<uint64_t>(cap, px_per_chunk * o->spp);
   cap = std::max<uint32_t>(32, (cap + 255u) & ~255u);
-  int rc;
   const size_t qbytes = (size_t)cap * (4 * sizeof(float4) + sizeof(uint2)) * 2;
   if ((rc = ensure(&ws->qbuf, ws->qbytes, qbytes, 1))) return rc;
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
@@ -910,6 +943,9 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   F.W = o->width;
   F.H = o->height;
   F.spp = o->spp;
+  F.sample0 = part.sample0;
+  F.spp_scale = part.spp_scale;
+  F.out0 = (uint32_t)part.pixel0;
   F.depth = o->max_depth;
   F.mode = o->mode;
   F.rr_depth = (o->mode == 1) ? o->rr_depth : 0;
@@ -946,8 +982,9 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
   const unsigned shade_grid = (cap + block - 1) / block;
 
-  for (uint64_t p0 = 0; p0 < npix_total; p0 += px_per_chunk) {
-    const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - p0);
+  for (uint64_t q0 = 0; q0 < npix_total; q0 += px_per_chunk) {
+    const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - q0);
+    const uint64_t p0 = part.pixel0 + q0;  // image pixel of the chunk's first pixel
     F.pixel0 = (uint32_t)p0;
     F.npix = np;
     const uint64_t total = (uint64_t)np * o->spp;
@@ -1012,7 +1049,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     P.launches++;
     if (want_samples) {
       const size_t bytes = (size_t)np * o->spp * sizeof(float4);
-      SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)p0 * o->spp * 4, F.contrib, bytes,
+      SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)q0 * o->spp * 4, F.contrib, bytes,
                                host_samples ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream));
       if (host_samples) P.d2h_bytes += bytes;
     }
@@ -1065,6 +1102,9 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   if ((uint64_t)o->width * o->height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
   if (o->shade_batch > 32) return set_error(SWR_ERR_INVALID, "swr: shade_batch must be 0..32");
+  ImagePart part;
+  int rc = image_part(o, true, false, &part, "swr_render_adjoint");
+  if (rc) return rc;
   cudaStream_t stream = (cudaStream_t)stream_;
   SWR_CUDA(cudaSetDevice(s->device));
   if (is_host_pointer(dl) || is_host_pointer(g_alb) || is_host_pointer(g_em))
@@ -1072,7 +1112,6 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   RenderWorkspace* ws = workspace_of(s);
   const uint64_t npix_total = (uint64_t)o->width * o->height;
   const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
-  int rc;
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if (!ws->ctrl) {
     SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
@@ -1088,6 +1127,9 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   F.W = o->width;
   F.H = o->height;
   F.spp = o->spp;
+  F.sample0 = part.sample0;
+  F.spp_scale = part.spp_scale;
+  F.out0 = 0;
   F.depth = o->max_depth;
   F.mode = 1;
   F.rr_depth = o->rr_depth;
@@ -1141,6 +1183,11 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   if (o->max_depth == 0 || o->max_depth > (uint32_t)kBdptMax || b->light_jumps > (uint32_t)kBdptMax)
     return set_error(SWR_ERR_UNSUPPORTED, "swr: the bidirectional tracer supports 1..16 vision and 0..16 light jumps");
   if (b->max_depth == 0) return set_error(SWR_ERR_INVALID, "swr: bidirectional maxDepth must be positive");
+  {
+    ImagePart part;
+    const int prc = image_part(o, false, false, &part, "swr_render_bdpt");
+    if (prc) return prc;
+  }
   if ((uint64_t)o->width * o->height >= (1ull << 32)) return set_error(SWR_ERR_INVALID, "swr: image too large");
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
   if ((b->shade_batch & 0xFFu) > 32 || ((b->shade_batch >> 8) & 0xFFu) > 32 || (b->shade_batch >> 16))
@@ -1189,6 +1236,9 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   F.W = o->width;
   F.H = o->height;
   F.spp = o->spp;
+  F.sample0 = 0;
+  F.spp_scale = o->spp;
+  F.out0 = 0;
   F.depth = o->max_depth;
   F.mode = 0;
   F.rr_q = 1.0f;
@@ -1293,6 +1343,11 @@ int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
     return set_error(SWR_ERR_INVALID, "swr: image too large");
   if (o->flags & ~SWR_RENDER_SAMPLES_OUT)
     return set_error(SWR_ERR_UNSUPPORTED, "swr: swr_render_noalloc accepts only SWR_RENDER_SAMPLES_OUT");
+  {
+    ImagePart part;
+    const int prc = image_part(o, false, false, &part, "swr_render_noalloc");
+    if (prc) return prc;
+  }
   const bool want_samples = (o->flags & SWR_RENDER_SAMPLES_OUT) != 0;
   if (want_samples && !samples_out)
     return set_error(SWR_ERR_INVALID, "swr: SWR_RENDER_SAMPLES_OUT without a samples buffer");
@@ -1341,6 +1396,9 @@ int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   F.W = o->width;
   F.H = o->height;
   F.spp = o->spp;
+  F.sample0 = 0;
+  F.spp_scale = o->spp;
+  F.out0 = 0;
   F.depth = o->max_depth;
   F.mode = o->mode;
   F.rr_depth = (o->mode == 1) ? o->rr_depth : 0;

@@ -90,3 +90,48 @@ def render_physical_batch(batch, jobs, albedos, emissions, adjoint_seeds=None):
     for a, e in zip(albedos, emissions):
         params += [a, e]
     return _PhysicalRenderBatch.apply(batch, jobs, adjoint_seeds, *params)
+
+
+class _PhysicalRenderSplit(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, albedo, emission, scene, cam, width, height, spp, depth, seed, rr_depth, rr_survive, rank,
+                world):
+        from . import sharding
+        albedo = albedo.detach().contiguous()
+        emission = emission.detach().contiguous()
+        scene.set_albedo(albedo)
+        scene.set_emission(emission)
+        part = sharding.scene_part_renderer(scene, cam, width, height, spp, depth, seed=seed, mode=N.MODE_PHYSICAL,
+                                            rr_depth=rr_depth, rr_survive=rr_survive)
+        img = sharding.render_split(part, width, height, spp, rank, world, split="spp", device=albedo.device)
+        ctx.save_for_backward(albedo, emission)
+        ctx.args = (scene, cam, width, height, spp, depth, seed, rr_depth, rr_survive, rank, world)
+        return img
+
+    @staticmethod
+    def backward(ctx, grad):
+        from . import sharding
+        albedo, emission = ctx.saved_tensors
+        scene, cam, width, height, spp, depth, seed, rr_depth, rr_survive, rank, world = ctx.args
+        scene.set_albedo(albedo)
+        scene.set_emission(emission)
+        g = grad.contiguous()
+
+        def part(s0, count):
+            return scene.render_adjoint(cam, width, height, count, depth, g, seed=seed, rr_depth=rr_depth,
+                                        rr_survive=rr_survive, sample_begin=s0, spp_total=spp)
+
+        ga, ge = sharding.adjoint_split(part, spp, rank, world, [tuple(albedo.shape), tuple(emission.shape)],
+                                        device=albedo.device)
+        return ga, ge, None, None, None, None, None, None, None, None, None, None, None
+
+
+def render_physical_split(scene, cam, albedo, emission, width, height, spp, depth, seed=0, rr_depth=0,
+                          rr_survive=1.0, rank=0, world=1):
+    """render_physical with one image's samples split over `world` ranks (one process per GPU,
+    each holding the scene): the forward pass adds the ranks' sample ranges with one all_reduce
+    of the image, the backward pass adds their path-replay gradients with one all_reduce per
+    gradient, so every rank gets the whole image and the whole gradient (data-parallel inverse
+    rendering with identical optimiser steps on every rank)."""
+    return _PhysicalRenderSplit.apply(albedo, emission, scene, cam, width, height, spp, depth, seed, rr_depth,
+                                      rr_survive, rank, world)

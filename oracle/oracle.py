@@ -26,6 +26,12 @@ def _lib():
         [ctypes.c_uint32] * 2 + [P, P, ctypes.c_int]
     lib.swo_adjoint_physical64.argtypes = [P, P] + [ctypes.c_uint32] * 4 + [ctypes.c_uint64, ctypes.c_uint32,
                                                                             ctypes.c_double, P, P, P, ctypes.c_int]
+    U = ctypes.c_uint32
+    lib.swo_render_reference_part.argtypes = [P, P] + [U] * 6 + [ctypes.c_uint64] + [U] * 2 + [P, P, ctypes.c_int]
+    lib.swo_render_physical64_part.argtypes = [P, P] + [U] * 6 + [ctypes.c_uint64, U, ctypes.c_double] + \
+        [U] * 2 + [P, P, ctypes.c_int]
+    lib.swo_adjoint_physical64_part.argtypes = [P, P] + [U] * 6 + [ctypes.c_uint64, U, ctypes.c_double, P, P, P,
+                                                                     ctypes.c_int]
     lib.swo_render_bdpt.argtypes = [P, P] + [ctypes.c_uint32] * 6 + [ctypes.c_uint64] + [ctypes.c_uint32] * 2 + \
         [P, P, ctypes.c_int]
     lib.swo_render_bdpt.restype = ctypes.c_int
@@ -149,13 +155,17 @@ def camera(vi, pi, org):
     return c
 
 
-def render_reference(sc, cam, W, H, spp, depth, seed, p0=0, p1=None, threads=None):
+def render_reference(sc, cam, W, H, spp, depth, seed, p0=0, p1=None, threads=None, samples=None):
+    """Per-sample (r g b flag) [n, k, 4] and per-pixel [n, 3] radiance of pixels [p0, p1); with
+    samples=(s0, s1) only those samples of each pixel (k = s1 - s0), per-pixel values scaled by the
+    whole image's 2 pi / spp."""
     p1 = W * H if p1 is None else p1
+    s0, s1 = (0, spp) if samples is None else samples
     n = p1 - p0
-    ps = np.empty((n, spp, 4), np.float32)
+    ps = np.empty((n, s1 - s0, 4), np.float32)
     pp = np.empty((n, 3), np.float32)
-    lib().swo_render_reference(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, depth, seed, p0, p1,
-                               _p(ps), _p(pp), threads or _threads())
+    lib().swo_render_reference_part(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, s0, s1, depth, seed, p0, p1,
+                                    _p(ps), _p(pp), threads or _threads())
     return ps, pp
 
 
@@ -173,22 +183,32 @@ def render_bdpt(sc, cam, W, H, spp, vision_jumps, light_jumps, max_depth, seed, 
     return ps, pp
 
 
-def render_physical64(sc, cam, W, H, spp, depth, seed, rr_depth=0, rr_q=1.0, p0=0, p1=None, threads=None):
+def render_physical64(sc, cam, W, H, spp, depth, seed, rr_depth=0, rr_q=1.0, p0=0, p1=None, threads=None,
+                      samples=None):
+    """Physical-mode estimate per pixel in double (and the variance of the mean); with
+    samples=(s0, s1) only those samples, weighted by the whole image's 1/spp (variance unused)."""
     p1 = W * H if p1 is None else p1
+    s0, s1 = (0, spp) if samples is None else samples
     n = p1 - p0
     pp = np.empty((n, 3), np.float64)
     var = np.empty((n, 3), np.float64)
-    lib().swo_render_physical64(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, depth, seed, rr_depth,
-                                float(np.float32(rr_q)), p0, p1, _p(pp), _p(var), threads or _threads())
+    lib().swo_render_physical64_part(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, s0, s1, depth, seed,
+                                     rr_depth, float(np.float32(rr_q)), p0, p1, _p(pp), _p(var),
+                                     threads or _threads())
     return pp, var
 
 
-def adjoint_physical64(sc, cam, W, H, spp, depth, seed, dl_dimg, rr_depth=0, rr_q=1.0, threads=None):
+def adjoint_physical64(sc, cam, W, H, spp, depth, seed, dl_dimg, rr_depth=0, rr_q=1.0, threads=None,
+                       samples=None):
+    """Gradient of sum(dl_dimg * image) w.r.t. albedo and emission in double; with samples=(s0, s1)
+    only those samples' share (weights 1/spp of the whole image)."""
     dl = np.ascontiguousarray(dl_dimg, dtype=np.float32).reshape(-1, 3)
+    s0, s1 = (0, spp) if samples is None else samples
     ga = np.empty((sc.v0.shape[0], 3), np.float64)
     ge = np.empty((sc.obj_box.shape[0], 3), np.float64)
-    lib().swo_adjoint_physical64(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, depth, seed, rr_depth,
-                                 float(np.float32(rr_q)), _p(dl), _p(ga), _p(ge), threads or _threads())
+    lib().swo_adjoint_physical64_part(ctypes.byref(sc._s), ctypes.byref(cam), W, H, spp, s0, s1, depth, seed,
+                                      rr_depth, float(np.float32(rr_q)), _p(dl), _p(ga), _p(ge),
+                                      threads or _threads())
     return ga, ge
 
 

@@ -7,7 +7,13 @@
 // so it spans the whole frame.
 //
 //   ref_bench <basepath> <scene> <camera> <W> <H> <spp> <depth> <threads> <max_pixels> [fast]
-//             [bdpt <lightJumpCount> <maxDepth>]
+//             [bdpt <lightJumpCount> <maxDepth>] [passes <timed> <warmup>] [target <seconds>]
+//
+// With "passes", the scene is loaded once and the same pixel sample is rendered <warmup> untimed
+// times and then <timed> timed times (one timed pass = one bench step); the JSON line lists every
+// timed pass. Without it there is one timed pass and no warm-up. With "target", max_pixels is
+// only an upper bound: an untimed probe over a few pixels per thread measures the rate first, and
+// the sample is sized so that one pass takes about <seconds>.
 //
 // With "bdpt" the timed renderer is the reference's BidirectionalPathTracer (visionJumpCount =
 // depth) instead of its PathTracer.
@@ -163,9 +169,20 @@ int main(int argc, char** argv) {
   bool fast = false;
   bool bdpt = false;
   unsigned light_jumps = 0, max_depth = 0;
+  unsigned timed_passes = 1, warm_passes = 0;
+  double target_s = 0.0;
   for (int a = 10; a < argc; ++a) {
     const std::string k = argv[a];
     if (k == "fast") fast = true;
+    if (k == "passes" && a + 2 < argc) {
+      timed_passes = std::max(1, std::atoi(argv[a + 1]));
+      warm_passes = (unsigned)std::max(0, std::atoi(argv[a + 2]));
+      a += 2;
+    }
+    if (k == "target" && a + 1 < argc) {
+      target_s = std::atof(argv[a + 1]);
+      a += 1;
+    }
     if (k == "bdpt" && a + 2 < argc) {
       bdpt = true;
       light_jumps = (unsigned)std::atoi(argv[a + 1]);
@@ -225,8 +242,8 @@ int main(int argc, char** argv) {
   Matrix4f pi = cam->getProjectionMatrix(float(W) / float(H)).inverseMatrix();
   Vector3f origin = cutVector(vi * Vector4f({0.0f, 0.0f, 0.0f, 1.0f}));
   const uint64_t total = (uint64_t)W * H;
-  const uint64_t npix = std::min<uint64_t>(maxPixels, total);
-  const uint64_t stride = std::max<uint64_t>(1, total / std::max<uint64_t>(1, npix));
+  uint64_t npix = std::min<uint64_t>(maxPixels, total);
+  uint64_t stride = std::max<uint64_t>(1, total / std::max<uint64_t>(1, npix));
   std::atomic<uint64_t> counter(0);
   auto worker = [&]() {
     Renderer::PixelRenderData prd;
@@ -249,18 +266,45 @@ int main(int argc, char** argv) {
       for (unsigned i = 0; i < 3; ++i) engine.image[idx + i] = (char)(c[i] * 255.0f);
     }
   };
-  auto t2 = std::chrono::steady_clock::now();
-  std::vector<std::thread> th;
-  for (unsigned t = 0; t < threads; ++t) th.emplace_back(worker);
-  for (auto& t : th) t.join();
-  auto t3 = std::chrono::steady_clock::now();
+  // one pass: GraphicsEngine::render's worker threads over the pixel sample
+  auto pass = [&]() {
+    counter.store(0);
+    auto a = std::chrono::steady_clock::now();
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < threads; ++t) th.emplace_back(worker);
+    for (auto& t : th) t.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+  };
+  uint64_t probe_pixels = 0;
+  double probe_s = 0.0;
+  if (target_s > 0.0) {
+    const uint64_t cap = npix;
+    npix = std::min<uint64_t>(cap, std::max<uint64_t>(8, 4ull * threads));
+    stride = std::max<uint64_t>(1, total / npix);
+    probe_pixels = npix;
+    probe_s = pass();
+    const double rate = (double)npix / std::max(probe_s, 1e-6);
+    npix = std::min<uint64_t>(cap, std::max<uint64_t>(2ull * threads, (uint64_t)(rate * target_s)));
+    stride = std::max<uint64_t>(1, total / npix);
+  }
+  for (unsigned w = 0; w < warm_passes; ++w) pass();
+  std::vector<double> pass_s;
+  double render_s = 0.0;
+  for (unsigned r = 0; r < timed_passes; ++r) {
+    pass_s.push_back(pass());
+    render_s += pass_s.back();
+  }
   double load_s = std::chrono::duration<double>(t1 - t0).count();
-  double render_s = std::chrono::duration<double>(t3 - t2).count();
-  double samples = (double)npix * spp;
+  double samples = (double)npix * spp * timed_passes;
+  std::string passes = "[";
+  for (size_t r = 0; r < pass_s.size(); ++r) passes += (r ? ", " : "") + std::to_string(pass_s[r]);
+  passes += "]";
   std::printf(
       "{\"pixels\": %llu, \"spp\": %u, \"samples\": %.0f, \"threads\": %u, \"load_s\": %.6f, "
-      "\"render_s\": %.6f, \"msamples_per_s\": %.6f, \"fast_build\": %s}\n",
+      "\"render_s\": %.6f, \"msamples_per_s\": %.6f, \"fast_build\": %s, \"timed_passes\": %u, "
+      "\"warmup_passes\": %u, \"pass_s\": %s, \"probe_pixels\": %llu, \"probe_s\": %.6f}\n",
       (unsigned long long)npix, spp, samples, threads, load_s, render_s,
-      samples / render_s / 1e6, fast ? "true" : "false");
+      samples / render_s / 1e6, fast ? "true" : "false", timed_passes, warm_passes, passes.c_str(),
+      (unsigned long long)probe_pixels, probe_s);
   return 0;
 }

@@ -328,6 +328,7 @@ typedef struct {
   uint32_t W, H, spp, depth, p0;
   uint64_t seed;
   float *per_sample, *per_pixel;
+  uint32_t s0, spp_total; /* samples [s0, s0 + spp) of an image with spp_total samples per pixel */
 } render_ctx;
 
 static void render_range(void* c_, uint64_t b, uint64_t e) {
@@ -341,7 +342,7 @@ static void render_range(void* c_, uint64_t b, uint64_t e) {
     double sc;
     for (smp = 0; smp < c->spp; ++smp) {
       v3f col;
-      int lit = trace_single_path(c->s, o, d, c->depth, c->seed, pix, smp, &col);
+      int lit = trace_single_path(c->s, o, d, c->depth, c->seed, pix, c->s0 + smp, &col);
       float* ps = c->per_sample ? c->per_sample + (k * c->spp + smp) * 4 : NULL;
       if (lit) {
         fr += col.x;
@@ -355,7 +356,7 @@ static void render_range(void* c_, uint64_t b, uint64_t e) {
         ps[3] = lit ? 1.0f : 0.0f;
       }
     }
-    sc = 2.0 * M_PI * (double)(1.0f / (float)c->spp);
+    sc = 2.0 * M_PI * (double)(1.0f / (float)c->spp_total);
     c->per_pixel[3 * k + 0] = (float)((double)fr * sc);
     c->per_pixel[3 * k + 1] = (float)((double)fg * sc);
     c->per_pixel[3 * k + 2] = (float)((double)fb * sc);
@@ -365,7 +366,13 @@ static void render_range(void* c_, uint64_t b, uint64_t e) {
 void swo_render_reference(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
                           uint32_t spp, uint32_t depth, uint64_t seed, uint32_t p0, uint32_t p1,
                           float* per_sample, float* per_pixel, int threads) {
-  render_ctx c = {s, cam, W, H, spp, depth, p0, seed, per_sample, per_pixel};
+  swo_render_reference_part(s, cam, W, H, spp, 0, spp, depth, seed, p0, p1, per_sample, per_pixel, threads);
+}
+
+void swo_render_reference_part(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
+                               uint32_t spp_total, uint32_t s0, uint32_t s1, uint32_t depth, uint64_t seed,
+                               uint32_t p0, uint32_t p1, float* per_sample, float* per_pixel, int threads) {
+  render_ctx c = {s, cam, W, H, s1 - s0, depth, p0, seed, per_sample, per_pixel, s0, spp_total};
   parallel_for(p1 - p0, 4, threads, render_range, &c);
 }
 
@@ -740,6 +747,7 @@ typedef struct {
   double rr_q;
   uint64_t seed;
   double *pp, *var;
+  uint32_t s0, spp_total; /* samples [s0, s0 + spp) of an image with spp_total samples per pixel */
 } phys_ctx;
 
 static void phys_range(void* c_, uint64_t b, uint64_t e) {
@@ -751,16 +759,17 @@ static void phys_range(void* c_, uint64_t b, uint64_t e) {
     v3f o = ld3(c->cam->org);
     v3d sum = dk(0, 0, 0), sq = dk(0, 0, 0);
     for (smp = 0; smp < c->spp; ++smp) {
-      v3d L = path_physical64(c->s, o, d, c->depth, c->seed, pix, smp, c->rr_depth, c->rr_q, NULL);
+      v3d L = path_physical64(c->s, o, d, c->depth, c->seed, pix, c->s0 + smp, c->rr_depth, c->rr_q, NULL);
       sum = dadd(sum, L);
       sq = dadd(sq, dk(L.x * L.x, L.y * L.y, L.z * L.z));
     }
     {
       double n = (double)c->spp;
       v3d mean = dscl(1.0 / n, sum);
-      c->pp[3 * k + 0] = mean.x;
-      c->pp[3 * k + 1] = mean.y;
-      c->pp[3 * k + 2] = mean.z;
+      v3d part = dscl(1.0 / (double)c->spp_total, sum);
+      c->pp[3 * k + 0] = part.x;
+      c->pp[3 * k + 1] = part.y;
+      c->pp[3 * k + 2] = part.z;
       if (c->var) {
         double dn = n > 1 ? n * (n - 1.0) : 1.0;
         c->var[3 * k + 0] = fmax(0.0, sq.x - n * mean.x * mean.x) / dn;
@@ -775,7 +784,15 @@ void swo_render_physical64(const swo_scene* s, const swo_camera* cam, uint32_t W
                            uint32_t spp, uint32_t depth, uint64_t seed, uint32_t rr_depth,
                            double rr_q, uint32_t p0, uint32_t p1, double* per_pixel,
                            double* per_pixel_var, int threads) {
-  phys_ctx c = {s, cam, W, H, spp, depth, p0, rr_depth, rr_q, seed, per_pixel, per_pixel_var};
+  swo_render_physical64_part(s, cam, W, H, spp, 0, spp, depth, seed, rr_depth, rr_q, p0, p1, per_pixel,
+                             per_pixel_var, threads);
+}
+
+void swo_render_physical64_part(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
+                                uint32_t spp_total, uint32_t s0, uint32_t s1, uint32_t depth, uint64_t seed,
+                                uint32_t rr_depth, double rr_q, uint32_t p0, uint32_t p1, double* per_pixel,
+                                double* per_pixel_var, int threads) {
+  phys_ctx c = {s, cam, W, H, s1 - s0, depth, p0, rr_depth, rr_q, seed, per_pixel, per_pixel_var, s0, spp_total};
   parallel_for(p1 - p0, 4, threads, phys_range, &c);
 }
 
@@ -793,6 +810,7 @@ typedef struct {
   const float* dl;
   double *ga, *ge;
   pthread_mutex_t* mu;
+  uint32_t s0, spp_total; /* samples [s0, s0 + spp) of an image with spp_total samples per pixel */
 } adj_ctx;
 
 static void adj_range(void* c_, uint64_t b, uint64_t e) {
@@ -806,12 +824,12 @@ static void adj_range(void* c_, uint64_t b, uint64_t e) {
     uint32_t pix = (uint32_t)k, smp;
     v3f d = primary_dir(c->cam, pix % c->W, pix / c->W, c->W, c->H);
     v3f o = ld3(c->cam->org);
-    const double w = 1.0 / (double)c->spp;
+    const double w = 1.0 / (double)c->spp_total;
     v3d dl = dk(c->dl[3 * k] * w, c->dl[3 * k + 1] * w, c->dl[3 * k + 2] * w);
     for (smp = 0; smp < c->spp; ++smp) {
       v3d S;
       int j;
-      path_physical64(s, o, d, c->depth, c->seed, pix, smp, c->rr_depth, c->rr_q, &rec);
+      path_physical64(s, o, d, c->depth, c->seed, pix, c->s0 + smp, c->rr_depth, c->rr_q, &rec);
       if (!rec.emit) continue;
       {
         uint32_t ob = rec.emit_obj;
@@ -847,6 +865,14 @@ void swo_adjoint_physical64(const swo_scene* s, const swo_camera* cam, uint32_t 
                             uint32_t spp, uint32_t depth, uint64_t seed, uint32_t rr_depth,
                             double rr_q, const float* dl_dimg, double* g_albedo, double* g_emission,
                             int threads) {
+  swo_adjoint_physical64_part(s, cam, W, H, spp, 0, spp, depth, seed, rr_depth, rr_q, dl_dimg, g_albedo,
+                              g_emission, threads);
+}
+
+void swo_adjoint_physical64_part(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
+                                 uint32_t spp_total, uint32_t s0, uint32_t s1, uint32_t depth, uint64_t seed,
+                                 uint32_t rr_depth, double rr_q, const float* dl_dimg, double* g_albedo,
+                                 double* g_emission, int threads) {
   pthread_mutex_t mu;
   adj_ctx c;
   pthread_mutex_init(&mu, NULL);
@@ -856,7 +882,9 @@ void swo_adjoint_physical64(const swo_scene* s, const swo_camera* cam, uint32_t 
   c.cam = cam;
   c.W = W;
   c.H = H;
-  c.spp = spp;
+  c.spp = s1 - s0;
+  c.s0 = s0;
+  c.spp_total = spp_total;
   c.depth = depth;
   c.rr_depth = rr_depth;
   c.rr_q = rr_q;

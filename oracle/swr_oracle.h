@@ -55,6 +55,23 @@ void swo_adjoint_physical64(const swo_scene* s, const swo_camera* cam, uint32_t 
                             double rr_q, const float* dl_dimg, double* g_albedo, double* g_emission,
                             int threads);
 
+/* The three functions above for part of each pixel's samples: samples [s0, s1) of an image with
+ * spp_total samples per pixel, with the random numbers of those samples and the whole image's
+ * 1/spp_total weight (times 2 pi in reference mode). per_sample holds (s1 - s0) samples per pixel;
+ * per_pixel_var is only meaningful for the whole range. Parts over a partition of [0, spp_total)
+ * sum to the whole image and to its gradient. */
+void swo_render_reference_part(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
+                               uint32_t spp_total, uint32_t s0, uint32_t s1, uint32_t depth, uint64_t seed,
+                               uint32_t p0, uint32_t p1, float* per_sample, float* per_pixel, int threads);
+void swo_render_physical64_part(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
+                                uint32_t spp_total, uint32_t s0, uint32_t s1, uint32_t depth, uint64_t seed,
+                                uint32_t rr_depth, double rr_q, uint32_t p0, uint32_t p1, double* per_pixel,
+                                double* per_pixel_var, int threads);
+void swo_adjoint_physical64_part(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H,
+                                 uint32_t spp_total, uint32_t s0, uint32_t s1, uint32_t depth, uint64_t seed,
+                                 uint32_t rr_depth, double rr_q, const float* dl_dimg, double* g_albedo,
+                                 double* g_emission, int threads);
+
 /* BidirectionalPathTracer radiance for pixels [p0, p1): per sample (the contribution before the
  * 2 pi / spp scale; r g b 1) and per pixel. Returns -2 for a scene without light sources. */
 int swo_render_bdpt(const swo_scene* s, const swo_camera* cam, uint32_t W, uint32_t H, uint32_t spp,

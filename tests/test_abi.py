@@ -37,7 +37,7 @@ def test_binding_covers_header():
 
 
 def test_abi_version_and_errors():
-    assert N.lib.swr_abi_version() == 2
+    assert N.lib.swr_abi_version() == 3
     d = N.SceneDesc()
     h = ctypes.c_void_p()
     rc = N.lib.swr_scene_create(ctypes.byref(d), None, ctypes.byref(h))
