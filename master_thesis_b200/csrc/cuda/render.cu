@@ -964,6 +964,10 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 0, true> : k_trace_dyn<false, 0, true>)
                               : (count ? k_trace_dyn<true, 0, false> : k_trace_dyn<false, 0, false>);
       break;
+    case 8:
+      trace_kernel = postpone ? (count ? k_trace_dyn<true, 8, true> : k_trace_dyn<false, 8, true>)
+                              : (count ? k_trace_dyn<true, 8, false> : k_trace_dyn<false, 8, false>);
+      break;
     case 9:
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 9, true> : k_trace_dyn<false, 9, true>)
                               : (count ? k_trace_dyn<true, 9, false> : k_trace_dyn<false, 9, false>);
@@ -972,7 +976,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 10, true> : k_trace_dyn<false, 10, true>)
                               : (count ? k_trace_dyn<true, 10, false> : k_trace_dyn<false, 10, false>);
       break;
-    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0, 9 or 10");
+    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0, 8, 9 or 10");
   }
   if (static_fetch) trace_kernel = count ? k_trace<true> : k_trace<false>;
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
