@@ -698,20 +698,41 @@ def run_inverse(args, cfg):
             den += d.numel()
         return (num / max(den, 1)) ** 0.5
 
+    def rmse_weighted(ps):
+        # squared albedo error weighted by the pixels whose primary ray sees each triangle: what an
+        # image loss can recover
+        num, den = 0.0, 0.0
+        for p, h, c in zip(ps, hidden, cover):
+            w = c.double()
+            num += float((w[:, None] * (p.detach() - h).double() ** 2).sum())
+            den += 3.0 * float(w.sum())
+        return (num / max(den, 1.0)) ** 0.5
+
+    # parameter snapshots for the recovery curve (device copies, evaluated after the timed loop)
+    marks = sorted({0, 25, 50, 100, 150, cfg["adam_steps"]})
+    snaps = {0: [a.clone() for a in init]}
     warm = max(args.warmup, 3)
     first = None
     for i in range(warm):
         loss = step(i)
         first = float(loss.detach()) if first is None else first
+        if i + 1 in marks:
+            snaps[i + 1] = [p.detach().clone() for p in params]
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     last = None
     for i in range(warm, cfg["adam_steps"]):
         last = step(i)
+        if i + 1 in marks:
+            snaps[i + 1] = [p.detach().clone() for p in params]
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1)
+    curve = [{"step": k, "rmse_all": (sum(float(((a - h).double() ** 2).sum()) for a, h in zip(snaps[k], hidden)) /
+                                      sum(h.numel() for h in hidden)) ** 0.5,
+              "rmse_coverage_weighted": rmse_weighted(snaps[k]), "rmse_covering_4px": rmse_covered(snaps[k], 4)}
+             for k in sorted(snaps)]
     timed = cfg["adam_steps"] - warm
     init_err = [float(((a - h).double() ** 2).sum()) for a, h in zip(init, hidden)]
     init_seen = (sum(float((((a - h)[s_]).double() ** 2).sum()) for a, h, s_ in zip(init, hidden, seen)) /
@@ -729,7 +750,11 @@ def run_inverse(args, cfg):
                         "final_all": rmse(False), "initial_seen": init_seen, "final_seen": rmse(True),
                         "seen_triangles": int(sum(int(s_.sum()) for s_ in seen)), "triangles": tris,
                         "initial_covering_4px": rmse_covered(init, 4), "final_covering_4px": rmse_covered(params, 4),
-                        "triangles_covering_4px": int(sum(int((c >= 4).sum()) for c in cover))},
+                        "triangles_covering_4px": int(sum(int((c >= 4).sum()) for c in cover)),
+                        "initial_coverage_weighted": rmse_weighted(init), "final_coverage_weighted":
+                            rmse_weighted(params),
+                        "triangles_seen_by_primary_rays": int(sum(int((c > 0).sum()) for c in cover)),
+                        "curve": curve},
         "msamples_per_s_primal_plus_adjoint": 2 * samples * timed / (ms / 1e3) / 1e6, "setup_s": setup_s}))
 
 

@@ -92,6 +92,7 @@ typedef struct swr_build_opts {
   uint32_t builder;        /* SWR_BUILD_HOST (binned SAH on the host) or SWR_BUILD_DEVICE
                               (clustering and collapse on the GPU); same closest hits either way */
   uint32_t radius;         /* device builder: clustering search radius 1..256, 0 = 16 */
+  uint32_t width;          /* children per wide node, 2..8 (nodes keep 8 slots); 0 = 8 */
 } swr_build_opts;
 enum { SWR_BUILD_HOST = 0, SWR_BUILD_DEVICE = 1 };
 

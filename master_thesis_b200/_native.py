@@ -54,7 +54,7 @@ class SceneDesc(ctypes.Structure):
 class BuildOpts(ctypes.Structure):
     _fields_ = [("sah_bins", ctypes.c_uint32), ("max_leaf", ctypes.c_uint32),
                 ("threads", ctypes.c_uint32), ("leaf_cost_pct", ctypes.c_uint32),
-                ("builder", ctypes.c_uint32), ("radius", ctypes.c_uint32)]
+                ("builder", ctypes.c_uint32), ("radius", ctypes.c_uint32), ("width", ctypes.c_uint32)]
 
 
 BUILD_HOST = 0

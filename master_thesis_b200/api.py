@@ -155,18 +155,20 @@ def _stream_handle(stream):
 class Scene:
     """Device scene (wide BVH + triangle records) built from SceneData."""
 
-    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0, builder="host", radius=0):
-        """builder: "host" (binned SAH on the host) or "device" (clustering + collapse on the GPU)."""
+    def __init__(self, data, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0, builder="host", radius=0,
+                 width=0):
+        """builder: "host" (binned SAH on the host) or "device" (clustering + collapse on the GPU);
+        width: children per wide node (2..8, 0 = 8)."""
         self.data = data
         d = data.desc()
         b = {"host": N.BUILD_HOST, "device": N.BUILD_DEVICE}[builder]
-        o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius)
+        o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius, width)
         self._h = ctypes.c_void_p()
         check(N.lib.swr_scene_create(ctypes.byref(d), ctypes.byref(o), ctypes.byref(self._h)))
 
     @classmethod
     def from_file(cls, scene_path, basepath, sah_bins=0, max_leaf=0, threads=0, leaf_cost_pct=0, builder="host",
-                  radius=0):
+                  radius=0, width=0):
         """Scene loaded from a scene file, keeping the object-space meshes on the device so that
         set_transforms() can move its objects."""
         h = ctypes.c_void_p()
@@ -178,7 +180,7 @@ class Scene:
             xf = np.zeros((no, 10), np.float32)
             check(N.lib.swr_host_scene_transforms(h, ptr(xf)))
             b = {"host": N.BUILD_HOST, "device": N.BUILD_DEVICE}[builder]
-            o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius)
+            o = N.BuildOpts(sah_bins, max_leaf, threads, leaf_cost_pct, b, radius, width)
             self._h = ctypes.c_void_p()
             check(N.lib.swr_scene_create_from_host(h, ctypes.byref(o), ctypes.byref(self._h)))
             self._xf = xf

@@ -1,11 +1,14 @@
-"""Autotuner for the wavefront's launch shape.
+"""Autotuner for the BVH shape and the wavefront's launch shape.
 
-For a workload it times a small grid of the tunable knobs - paths in flight (wave size), the
-idle-lane refill threshold of the traversal, the shading block size and the traversal's register
-budget (for single-scene renders) - with CUDA events, keeps the fastest, and caches the choice in a
-JSON file keyed by the workload's shape and the GPU name. (The BVH node width is fixed at 8 in this
-build; the leaf size and the SAH leaf cost are build options measured separately.)
+For a workload it times a small grid of the tunable knobs with CUDA events, keeps the fastest, and
+caches the choice in a JSON file keyed by the workload's shape and the GPU name:
+  - the tree (tune_build): children per wide node (BVH width 4 or 8; the node record keeps 8
+    slots) and triangles per leaf, each candidate built and rendered;
+  - the launch (tune_render, tune_batch): paths in flight (wave size), the idle-lane refill
+    threshold of the traversal, the shading kernel's block size and the traversal's register
+    budget (resident blocks per SM).
 
+    bo = tune_build(scene_data, cam, width, height, spp, depth, mode=...)  # -> dict of Scene kwargs
     cfg = tune_render(scene, cam, width, height, spp, depth, mode=...)   # -> dict of render kwargs
     cfg = tune_batch(batch, jobs)                                        # -> dict of batch kwargs
     cfg = tune_bdpt(scene, cam, width, height, spp, vj, lj, md)          # -> dict of render_bdpt kwargs
@@ -24,8 +27,9 @@ import torch
 
 CACHE = os.environ.get("SWR_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "swr_b200", "tune.json"))
 
-RENDER_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16], block_size=[256],
-                   trace_blocks=[0])
+BUILD_GRID = dict(width=[4, 8], max_leaf=[2, 3])
+RENDER_GRID = dict(wave_size=[1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16], block_size=[128, 256, 512],
+                   trace_blocks=[0, 8])
 BATCH_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16])
 BDPT_GRID = dict(shade_batch=[12 | (16 << 8), 20 | (16 << 8), 24 | (16 << 8), 20 | (8 << 8), 20 | (24 << 8)],
                  refill=[4, 8], blocks_per_sm=[0])
@@ -76,6 +80,33 @@ def _search(key, grid, run, reps, force):
                "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
     _store(db)
     return results[0][1]
+
+
+def tune_build(data, cam, width, height, spp, depth, mode=0, rr_depth=0, rr_survive=1.0, reps=2, force=False,
+               grid=None, builder="host"):
+    """Tree options for a scene (SceneData): each candidate of the grid is built and one image
+    with the library's default launch shape is timed; returns the fastest as Scene kwargs."""
+    from .api import Scene
+    key = "build|%s|%s|tris=%d|objs=%d|px=%d|spp=%d|depth=%d|mode=%d" % (
+        torch.cuda.get_device_name(), builder, data.num_triangles, data.num_objects, width * height, spp, depth,
+        mode)
+    out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+    built = {}
+
+    def run(cfg):
+        k = tuple(sorted(cfg.items()))
+        if k not in built:
+            for sc in built.values():
+                sc.close()
+            built.clear()
+            built[k] = Scene(data, builder=builder, **cfg)
+        built[k].render(cam, width, height, spp, depth, mode=mode, rr_depth=rr_depth, rr_survive=rr_survive,
+                        out=out)
+    try:
+        return _search(key, grid or BUILD_GRID, run, reps, force)
+    finally:
+        for sc in built.values():
+            sc.close()
 
 
 def tune_render(scene, cam, width, height, spp, depth, mode=0, rr_depth=0, rr_survive=1.0, reps=2, force=False,

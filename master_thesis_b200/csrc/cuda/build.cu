@@ -215,7 +215,7 @@ struct Dp {
 };
 
 __device__ void eval_node(uint32_t v, uint32_t n, const float* __restrict__ node_box, const uint32_t* left,
-                          const uint32_t* right, Dp* dp, uint32_t max_leaf, float kprim) {
+                          const uint32_t* right, Dp* dp, uint32_t max_leaf, float kprim, int width) {
   const Box6 b = load_box(node_box, v);
   const float a = area(b);
   Dp r;
@@ -238,7 +238,7 @@ __device__ void eval_node(uint32_t v, uint32_t n, const float* __restrict__ node
       CR[k] = __ldcg(&R->c[k]);
     }
     r.count = __ldcg(&L->count) + __ldcg(&R->count);
-    for (int j = 2; j <= 8; ++j)
+    for (int j = 2; j <= width; ++j)
       for (int k = 1; k < j; ++k) {
         const float c = CL[k - 1] + CR[j - k - 1];
         if (c < D[j]) {
@@ -246,12 +246,12 @@ __device__ void eval_node(uint32_t v, uint32_t n, const float* __restrict__ node
           r.dist_k = (r.dist_k & ~(7u << (3 * (j - 2)))) | ((uint32_t)k << (3 * (j - 2)));
         }
       }
-    inner = a + D[8];
+    inner = a + D[width];
   }
   const float leaf = r.count <= max_leaf ? a * (float)r.count * kprim : INFINITY;
   if (leaf <= inner) r.flags |= 1u << 8;
   r.c[0] = fminf(leaf, inner);
-  for (int i = 2; i <= 8; ++i) {
+  for (int i = 2; i <= 8; ++i) {  // above width D is infinite: the width entry repeats as 'fewer'
     if (r.c[i - 2] <= D[i]) {
       r.c[i - 1] = r.c[i - 2];
       r.flags |= 1u << (i - 1);
@@ -264,11 +264,12 @@ __device__ void eval_node(uint32_t v, uint32_t n, const float* __restrict__ node
 
 __global__ void k_collapse_up(uint32_t n, const float* __restrict__ node_box, const uint32_t* __restrict__ left,
                               const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
-                              uint32_t* __restrict__ visits, Dp* __restrict__ dp, uint32_t max_leaf, float kprim) {
+                              uint32_t* __restrict__ visits, Dp* __restrict__ dp, uint32_t max_leaf, float kprim,
+                              int width) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t v = i;
-  eval_node(v, n, node_box, left, right, dp, max_leaf, kprim);
+  eval_node(v, n, node_box, left, right, dp, max_leaf, kprim, width);
   // each inner node is reached by exactly two threads (one per child), so the walk is bounded by
   // the tree height and never waits
   for (;;) {
@@ -277,7 +278,7 @@ __global__ void k_collapse_up(uint32_t n, const float* __restrict__ node_box, co
     __threadfence();                               // publish dp[v] before announcing it
     if (atomicAdd(&visits[p], 1u) == 0u) return;  // the sibling subtree is not done yet
     __threadfence();
-    eval_node(p, n, node_box, left, right, dp, max_leaf, kprim);
+    eval_node(p, n, node_box, left, right, dp, max_leaf, kprim, width);
     v = p;
   }
 }
@@ -298,6 +299,7 @@ struct EmitArgs {
   uint32_t* words;         // 20 per wide node
   uint32_t* prim_order;    // triangle slot -> primitive
   uint32_t* counters;      // [0] wide nodes, [1] triangle slots, [2] next-level tasks, [3] max depth
+  int width;               // children per wide node (2..8)
 };
 
 __device__ __forceinline__ int dist_k_of(const Dp& d, int j) { return (int)((d.dist_k >> (3 * (j - 2))) & 7u); }
@@ -320,9 +322,9 @@ __global__ void k_emit(EmitArgs A, const Task* __restrict__ tasks, uint32_t ntas
     uint32_t sn[16];
     int si[16];
     int sp = 0;
-    const int k = dist_k_of(A.dp[tk.bnode], 8);
+    const int k = dist_k_of(A.dp[tk.bnode], A.width);
     sn[sp] = A.right[tk.bnode];
-    si[sp++] = 8 - k;
+    si[sp++] = A.width - k;
     sn[sp] = A.left[tk.bnode];
     si[sp++] = k;
     while (sp > 0) {
@@ -581,7 +583,7 @@ int build_wide_bvh_device(const float* d_prim_boxes, uint32_t n, const DeviceBui
   const uint32_t root = host[5];
   // 3. collapse costs bottom-up
   k_collapse_up<<<blocks(n), kBlock, 0, stream>>>(n, node_box, left, right, parent, visits, dp, opt.max_leaf,
-                                                 (float)opt.prim_cost);
+                                                 (float)opt.prim_cost, (int)opt.width);
   SWR_CUDA(cudaGetLastError());
   // 4. wide nodes level by level. A wide node other than a single-leaf root has at least two
   // children and every leaf child holds a primitive, so there are at most n of them.
@@ -617,6 +619,7 @@ int build_wide_bvh_device(const float* d_prim_boxes, uint32_t n, const DeviceBui
   A.words = (uint32_t*)words;
   A.prim_order = out.d_prim_order;
   A.counters = counters;
+  A.width = (int)opt.width;
   uint32_t ntasks = 1, levels = 0;
   while (ntasks > 0) {
     if (++levels > 64) return set_error(SWR_ERR_UNSUPPORTED, "swr: BVH deeper than the traversal stack");

@@ -11,6 +11,7 @@ struct DeviceBuildOptions {
   uint32_t max_leaf = 3;    // triangles per leaf child (1..3)
   uint32_t radius = 16;     // clustering search radius in Morton order
   double prim_cost = 0.8;   // SAH cost of a triangle test relative to a wide-node visit
+  uint32_t width = 8;       // children per wide node (2..8)
 };
 
 struct DeviceBvh {

@@ -83,6 +83,7 @@ int device_pack(swr_scene* s, const swr_scene_desc* d, const swr_build_opts* opt
     if (opts->max_leaf) o.max_leaf = opts->max_leaf;
     if (opts->radius) o.radius = opts->radius;
     if (opts->leaf_cost_pct) o.prim_cost = opts->leaf_cost_pct / 100.0;
+    if (opts->width) o.width = opts->width;
   }
   cudaStream_t st = nullptr;
   void *boxes = nullptr, *tris = nullptr, *shade = nullptr, *tboxes = nullptr, *alb = nullptr;

@@ -59,8 +59,10 @@ int pack_scene(const swr_scene_desc* d, const swr_build_opts* opts, PackedScene&
     if (opts->leaf_cost_pct > 400)
       return set_error(SWR_ERR_INVALID, "swr: leaf_cost_pct must be 0..400");
     if (opts->leaf_cost_pct) wo.prim_cost = opts->leaf_cost_pct / 100.0;
+    if (opts->width) wo.width = opts->width;
   }
   if (wo.max_leaf > 3) return set_error(SWR_ERR_INVALID, "swr: max_leaf must be 1..3");
+  if (wo.width < 2 || wo.width > 8) return set_error(SWR_ERR_INVALID, "swr: width must be 2..8");
   if (opts && opts->radius > 256) return set_error(SWR_ERR_INVALID, "swr: radius must be 0..256");
   WideBvh bvh;
   if (host_bvh) {

@@ -110,9 +110,10 @@ struct HostScene {
 };
 
 struct LoadOptions {
-  // Meshes / object counts above this size do not get the reference's exact BVH leaf order
-  // (the reference's own builder is cubic in this size); ties then go to the lower index.
-  uint32_t max_exact_order = 1u << 15;
+  // Meshes / object counts above this size do not get the reference's exact BVH leaf order;
+  // ties then go to the lower index. (The reference's own builder is cubic in this size; the
+  // exact rebuild here takes about 0.2 s for 32k boxes, 1 s for 131k, 5 s for 524k on one core.)
+  uint32_t max_exact_order = 1u << 20;
   uint32_t threads = 0;  // mesh files parsed concurrently by load_scene_file; 0 = all cores
 };
 

@@ -104,9 +104,10 @@ struct Builder {
   unsigned hw;
   uint32_t max_leaf;
   double prim_cost;
+  int width;  // children per wide node (2..8)
 
-  Builder(const std::vector<PrimBox>& p, uint32_t b, int pd, unsigned threads, uint32_t ml, double pc)
-      : bins(b), par_depth(pd), hw(threads), max_leaf(ml), prim_cost(pc) {
+  Builder(const std::vector<PrimBox>& p, uint32_t b, int pd, unsigned threads, uint32_t ml, double pc, int w)
+      : bins(b), par_depth(pd), hw(threads), max_leaf(ml), prim_cost(pc), width(w) {
     const size_t n = p.size();
     refs.resize(n);
     const size_t nb = std::max<size_t>(1, 2 * n - 1);
@@ -267,8 +268,8 @@ struct Builder {
   // The collapse's dynamic program (Ylitie, Karras, Laine 2017, section 4.1) at node ni, from its
   // children's costs: as one child of a wide node, the subtree is either a leaf (at most
   // max_leaf triangles, cost area x count x prim_cost) or a wide node (area + the cheapest split
-  // of its subtree into at most 8 children); dist[j] = cheapest split of the two binary children
-  // into j children in total.
+  // of its subtree into at most `width` (8 unless built narrower) children); dist[j] = cheapest
+  // split of the two binary children into j children in total.
   void collapse(uint32_t ni, const Sub* L, const Sub* R, Sub& out) {
     const double INF = std::numeric_limits<double>::infinity();
     const BNode& b = nodes[ni];
@@ -278,7 +279,7 @@ struct Builder {
     const double leaf = tri_count[ni] <= max_leaf ? a * (double)tri_count[ni] * prim_cost : INF;
     double inner = INF;
     if (!b.count) {
-      for (int j = 2; j <= 8; ++j)
+      for (int j = 2; j <= width; ++j)
         for (int k = 1; k < j; ++k) {
           const double v = L->cost[k] + R->cost[j - k];
           if (v < D[j]) {
@@ -286,14 +287,14 @@ struct Builder {
             dist_k[(size_t)ni * 9 + j] = (uint8_t)k;
           }
         }
-      inner = a * 1.0 + D[8];
+      inner = a * 1.0 + D[width];
     }
     as_leaf[ni] = leaf <= inner ? 1 : 0;
     double* C = out.cost;
     C[0] = INF;
     C[1] = std::min(leaf, inner);
     uint16_t fw = 0;
-    for (int i = 2; i <= 8; ++i) {
+    for (int i = 2; i <= width; ++i) {
       if (C[i - 1] <= D[i]) {
         C[i] = C[i - 1];
         fw |= (uint16_t)(1u << i);
@@ -429,10 +430,11 @@ struct WideTask {
 WideBvh build_wide_bvh(const std::vector<PrimBox>& prims, const WideBvhOptions& opt) {
   if (prims.empty()) throw std::invalid_argument("BVH over zero primitives");
   if (opt.max_leaf < 1 || opt.max_leaf > 3) throw std::invalid_argument("max_leaf must be 1..3");
+  if (opt.width < 2 || opt.width > 8) throw std::invalid_argument("width must be 2..8");
   unsigned hw = opt.threads ? opt.threads : std::max(1u, std::thread::hardware_concurrency());
   int pd = 0;
   while ((1u << pd) < hw) ++pd;
-  Builder B(prims, std::max(4u, opt.sah_bins), pd + 1, hw, opt.max_leaf, opt.prim_cost);
+  Builder B(prims, std::max(4u, opt.sah_bins), pd + 1, hw, opt.max_leaf, opt.prim_cost, (int)opt.width);
   Sub root;
   B.build(0, 0, (uint32_t)prims.size(), 0, root);
   const uint32_t nb = B.next.load();
@@ -468,9 +470,10 @@ WideBvh build_wide_bvh(const std::vector<PrimBox>& prims, const WideBvhOptions& 
     if (bn[tk.bnode].count || B.as_leaf[tk.bnode]) {
       ch.push_back(tk.bnode);  // a scene small enough to be one leaf: a root with one leaf child
     } else {
-      const int k = B.dist_k[(size_t)tk.bnode * 9 + 8];
+      const int w = (int)opt.width;
+      const int k = B.dist_k[(size_t)tk.bnode * 9 + w];
       spread(bn[tk.bnode].left, k, ch);
-      spread(bn[tk.bnode].right, 8 - k, ch);
+      spread(bn[tk.bnode].right, w - k, ch);
     }
     float ulo[3] = {INFINITY, INFINITY, INFINITY}, uhi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t c : ch)

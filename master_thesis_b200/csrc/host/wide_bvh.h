@@ -19,6 +19,7 @@ struct WideBvhOptions {
   uint32_t max_leaf = 3;       // triangles per leaf child (1..3)
   uint32_t threads = 0;        // 0 = hardware concurrency
   double prim_cost = 0.8;      // SAH cost of a triangle test relative to a wide-node visit
+  uint32_t width = 8;          // children per wide node (2..8; the record always has 8 slots)
 };
 
 struct WideBvh {

@@ -44,7 +44,7 @@ class Twin:
     """CPU build of the kernels' traversal and shading code over the packed scene records."""
     _lib = None
 
-    def __init__(self, scene_data, sah_bins=0, max_leaf=0):
+    def __init__(self, scene_data, sah_bins=0, max_leaf=0, width=0):
         if Twin._lib is None:
             L = ctypes.CDLL(build_twin())
             P = ctypes.c_void_p
@@ -55,6 +55,8 @@ class Twin:
             L.twin_depth.restype = ctypes.c_uint32
             L.twin_nodes.argtypes = [P]
             L.twin_nodes.restype = ctypes.c_uint32
+            L.twin_node_words.argtypes = [P, P]
+            L.twin_node_words.restype = ctypes.c_uint32
             L.twin_trace.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P, ctypes.c_int]
             L.twin_render.argtypes = [P, P] + [ctypes.c_uint32] * 4 + [ctypes.c_uint64, ctypes.c_uint32,
                                                                         ctypes.c_uint32, ctypes.c_float,
@@ -64,7 +66,7 @@ class Twin:
             Twin._lib = L
         from master_thesis_b200 import _native as N
         self._d = scene_data.desc()
-        self._o = N.BuildOpts(sah_bins, max_leaf, 0, 0)
+        self._o = N.BuildOpts(sah_bins, max_leaf, 0, 0, 0, 0, width)
         self._h = Twin._lib.twin_create(ctypes.byref(self._d), ctypes.byref(self._o))
         if not self._h:
             Twin._lib.swr_last_error.restype = ctypes.c_char_p  # the twin keeps its own error
@@ -77,6 +79,16 @@ class Twin:
     @property
     def depth(self):
         return Twin._lib.twin_depth(self._h)
+
+    @property
+    def num_nodes(self):
+        return Twin._lib.twin_nodes(self._h)
+
+    def node_words(self):
+        """The compressed wide-BVH records, 20 words per node."""
+        out = np.empty(Twin._lib.twin_node_words(self._h, None), np.uint32)
+        Twin._lib.twin_node_words(self._h, out.ctypes.data)
+        return out
 
     def trace(self, ro, rd, counts=False, postpone=False):
         n = ro.shape[0]
@@ -154,3 +166,47 @@ def golden_camera(g):
     c.proj_inv[:] = g["cam_proj_inv"].reshape(-1).tolist()
     c.origin[:] = g["cam_origin"].reshape(-1).tolist()
     return c
+
+
+def grid_mesh_scene(root, cells=160):
+    """One OBJ mesh: a flat grid of cells x cells squares (2 * cells^2 triangles) in the y = 0
+    plane with dyadic coordinates (x, z = (i - cells/2) / 64), so that rays straight down onto its
+    edges and vertices hit several triangles at exactly the same squared distance (ties). Plus an
+    emissive quad above it. Returns (scene path, basepath)."""
+    from master_thesis_b200 import scenes
+    base = scenes._layout(root)
+    g = cells + 1
+    c = (np.arange(g, dtype=np.float64) - cells / 2) / 64.0
+    zz, xx = np.meshgrid(c, c, indexing="ij")
+    pos = np.stack([xx, np.zeros_like(xx), zz], -1).reshape(-1, 3)
+    nrm = np.tile([0.0, 1.0, 0.0], (g * g, 1))
+    faces = []
+    for r in range(cells):
+        for q in range(cells):
+            a = r * g + q
+            faces += [(a, a + g, a + 1), (a + 1, a + g, a + g + 1)]
+    scenes.write_obj(os.path.join(root, "res/obj/grid.obj"), pos, nrm, faces)
+    scenes.write_obj(os.path.join(root, "res/obj/quad.obj"), *scenes.quad_mesh())
+    path = os.path.join(root, "res/scene/grid.scene")
+    with open(path, "w") as f:
+        f.write(scenes._entry("grid.obj", (0, 0, 0), color=(0.7, 0.7, 0.7)))
+        f.write(scenes._entry("quad.obj", (0, 1.5, 0), scale=(0.3, 0.3, 0.3), rotation=(0, 0, 1, -np.pi / 2),
+                              color=(1, 1, 1), lightSource=10.0))
+    return path, base
+
+
+def rays_down_onto_grid_lines(n, cells, seed):
+    """Rays straight down from y = 1 onto points of the grid's edges (a coordinate on a grid line)
+    and vertices (both), all inside the grid."""
+    rng = np.random.default_rng(seed)
+    half = cells // 2
+    i = rng.integers(-half + 1, half, (n, 2)).astype(np.float64) / 64.0
+    f = rng.integers(0, 64, (n, 2)).astype(np.float64) / 4096.0  # dyadic offsets inside a cell
+    kind = rng.integers(0, 3, n)  # 0: on an x line, 1: on a z line, 2: on a vertex
+    x = i[:, 0] + np.where(kind == 1, f[:, 0], 0.0)
+    z = i[:, 1] + np.where(kind == 0, f[:, 1], 0.0)
+    ro = np.zeros((n, 4), np.float32)
+    rd = np.zeros((n, 4), np.float32)
+    ro[:, 0], ro[:, 1], ro[:, 2] = x, 1.0, z
+    rd[:, 1] = -1.0
+    return ro, rd

@@ -63,3 +63,28 @@ def test_tune_per_lane_kernels_on_gpu(tmp_path, monkeypatch):
     assert torch.equal(a, d) and int(a.max()) > 0
     db = json.loads((tmp_path / "tune.json").read_text())
     assert any(k.startswith("bdpt|") for k in db) and any(k.startswith("rt|") for k in db)
+
+
+def test_grids_name_the_tunable_knobs():
+    assert set(autotune.BUILD_GRID) == {"width", "max_leaf"} and 4 in autotune.BUILD_GRID["width"]
+    assert set(autotune.RENDER_GRID) == {"wave_size", "refill", "block_size", "trace_blocks"}
+    assert len(autotune.RENDER_GRID["block_size"]) > 1 and len(autotune.RENDER_GRID["trace_blocks"]) > 1
+
+
+@pytest.mark.gpu
+def test_tune_build_on_gpu(tmp_path, monkeypatch):
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import scenes
+    monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tune.json"))
+    sd, cam = scenes.random_scene(4, 3000)
+    c = swr.make_camera(cam["position"], cam["angle"], 64, 48, fov_deg=40)
+    best = autotune.tune_build(sd, c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL)
+    assert best["width"] in (4, 8) and best["max_leaf"] in (2, 3)
+    db = json.loads((tmp_path / "tune.json").read_text())
+    (entry,) = [v for k, v in db.items() if k.startswith("build|")]
+    assert len(entry["tried"]) == 4 and entry["best"] == best
+    # the chosen tree renders the same image as the default one (same closest hits)
+    a = swr.Scene(sd, **best).render(c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL)
+    b = swr.Scene(sd).render(c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL)
+    assert torch.equal(a, b)

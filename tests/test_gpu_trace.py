@@ -98,3 +98,22 @@ def test_gpu_terrain_microbench_rays_vs_oracle(tmp_path):
     assert np.array_equal(h[:, 2], od2.view(np.uint32))
     assert np.array_equal(h[:, 3], ot.view(np.uint32))
     assert 0.05 < float((otri != 0xFFFFFFFF).mean()) < 0.95
+
+
+def test_gpu_ties_on_a_large_single_mesh(tmp_path):
+    """Shared-edge and shared-vertex hits (exact ties in squared distance) on a 51,200-triangle
+    single mesh with exact reference ranks: the GPU picks the same triangle as the oracle."""
+    from helpers import grid_mesh_scene, rays_down_onto_grid_lines
+    path, base = grid_mesh_scene(str(tmp_path))
+    sd = swr.load_scene(path, base)
+    assert sd.ranks_exact
+    sc = swr.Scene(sd)
+    osc = O.OracleScene.from_scene_data(sd)
+    ro, rd = rays_down_onto_grid_lines(20000, 160, seed=8)
+    tri, _, d2, _ = _gpu_trace(sc, ro, rd)
+    otri, od2, _ = osc.trace(ro, rd)
+    assert np.array_equal(tri, otri)
+    assert np.array_equal(d2.view(np.uint32), od2.view(np.uint32))
+    ro2, rd2 = rays_uniform(20000, (-1.2, -0.5, -1.2), (1.2, 1.0, 1.2), seed=9)
+    tri2, _, _, _ = _gpu_trace(sc, ro2, rd2)
+    assert np.array_equal(tri2, osc.trace(ro2, rd2)[0])

@@ -270,3 +270,25 @@ def test_png_writer_round_trip(tmp_path, W, H):
     assert np.all(raw[:, 0] == 0) and np.array_equal(raw[:, 1:].reshape(H, W, 3), rgb)
     from PIL import Image
     assert np.array_equal(np.asarray(Image.open(p).convert("RGB")), rgb)
+
+
+def test_large_single_mesh_gets_exact_ranks(tmp_path):
+    """A single mesh of 51,200 triangles (above the former 32,768 limit) still gets the
+    reference's exact BVH leaf order for its tie ranks."""
+    from helpers import grid_mesh_scene
+    path, base = grid_mesh_scene(str(tmp_path))
+    D = swr.load_scene(path, base)
+    assert D.num_triangles == 51202 and D.ranks_exact
+    assert sorted(D.tri_rank.tolist()) == list(range(D.num_triangles))
+    # rays onto shared edges and vertices meet ties that the ranks decide: with ranks the oracle's
+    # winners differ from those of the triangle-index order for some rays
+    import copy
+    from helpers import rays_down_onto_grid_lines
+    from oracle import oracle as O
+    ro, rd = rays_down_onto_grid_lines(4000, 160, seed=8)
+    by_rank = O.OracleScene.from_scene_data(D).trace(ro, rd)[0]
+    plain = copy.copy(D)
+    plain.tri_rank = None
+    by_id = O.OracleScene.from_scene_data(plain).trace(ro, rd)[0]
+    assert (by_rank != 0xFFFFFFFF).all()
+    assert 0 < int((by_rank != by_id).sum()) < len(by_rank)

@@ -35,6 +35,28 @@ def test_twin_hits_match_oracle_random_rays(name, max_leaf, postpone):
     assert np.array_equal(t.view(np.uint32), ot.view(np.uint32))
 
 
+@pytest.mark.parametrize("width", [2, 4, 6])
+def test_twin_narrow_trees_match_oracle(tmp_path, width):
+    """Wide nodes built with at most `width` children (the 8-slot record keeps the rest empty):
+    the same closest hits, a deeper tree, more node visits than 8-wide."""
+    from master_thesis_b200 import scenes
+    s = scenes.terrain(5, str(tmp_path), cells=32, tile=16, spheres=4, sphere_subdiv=2, lights=1)
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    osc = O.OracleScene.from_scene_data(sd)
+    ro, rd = rays_uniform(20000, sd.vpos.min(0) - 0.1, sd.vpos.max(0) + 0.1, seed=12)
+    otri, od2, _ = osc.trace(ro, rd)
+    wide = Twin(sd)
+    narrow = Twin(sd, width=width)
+    tri, d2, _ = narrow.trace(ro, rd)
+    assert np.array_equal(tri, otri)
+    assert np.array_equal(d2.view(np.uint32), od2.view(np.uint32))
+    assert narrow.depth > wide.depth and narrow.num_nodes > wide.num_nodes
+    words = narrow.node_words().reshape(-1, 20)
+    children = np.array([bin(int(w[3]) >> 24).count("1") for w in words]) + \
+        np.array([sum(((int(w[6 + i // 4]) >> (8 * (i % 4))) & 0xFF) != 0 for i in range(8)) for w in words])
+    assert children.max() <= width
+
+
 def test_twin_axis_aligned_and_degenerate_rays():
     """Rays with zero direction components, rays starting on box faces and through shared edges
     (exact ties between the two triangles of a quad)."""
