@@ -9,8 +9,10 @@
 // exactly those of swr_render for it. Radiance is summed per pixel in 64-bit fixed point with
 // integer atomics (scale 2^32): order-independent, hence deterministic, and it needs 24 bytes per
 // pixel instead of 16 bytes per sample (a 256-scene batch has ~2e9 samples). The final per-pixel
-// scale is the single-scene one. The shade/trace rounds are captured once into a CUDA graph (eight
-// rounds per graph) that the host replays until the queue has drained.
+// scale is the single-scene one. The shade/trace rounds are captured once into a CUDA graph: a
+// conditional WHILE node whose body runs eight rounds and then k_bcheck, which ends the loop on
+// the device when the queue has drained (or, as a guard against a logic error, after a proven
+// bound on the rounds, recording a timeout). The host waits once per batch.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -48,11 +50,14 @@ struct BCtrl {
   unsigned int count[2];
   unsigned int cursor[2];
   unsigned int inj_n[2];
-  unsigned int pad[2];
+  unsigned int status;  // 1: the device-side round loop hit max_rounds without draining
+  unsigned int pad;
   unsigned long long inj_base[2];
   unsigned long long injected;
   unsigned long long total;
   unsigned long long rays;
+  unsigned long long rounds;      // shade/trace rounds run by the device-side loop
+  unsigned long long max_rounds;  // its bound (every path ends within depth rounds of injection)
 };
 
 struct BQueue {
@@ -372,6 +377,22 @@ __global__ void __launch_bounds__(kTB) k_badjoint(BArgs A, BCtrl* __restrict__ c
   }
 }
 
+// End of one iteration of the graph's round loop (eight shade/trace rounds, after which the
+// next shade reads parity 0): continue while paths are queued or samples wait for injection; stop
+// with status 1 once the proven bound on rounds is exceeded (never reached unless the wavefront
+// logic is broken), so the loop always ends.
+__global__ void k_bcheck(BCtrl* __restrict__ ctrl, cudaGraphConditionalHandle loop) {
+  BCtrl& c = *ctrl;
+  c.rounds += 8;
+  const bool drained = c.count[0] == 0u && c.inj_n[0] == 0u && c.injected == c.total;
+  unsigned go = drained ? 0u : 1u;
+  if (!drained && c.rounds > c.max_rounds) {
+    c.status = 1u;
+    go = 0u;
+  }
+  cudaGraphSetConditional(loop, go);
+}
+
 __global__ void k_bresolve(BArgs A) {
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= A.npix) return;
@@ -537,11 +558,17 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
   A.refill = refill;
   A.cam = (float4*)b->cam;
   A.accum = (unsigned long long*)b->accum;
+  uint32_t maxdepth = 0;
+  for (uint32_t k = 0; k < n; ++k) maxdepth = std::max(maxdepth, jobs[k].opts.max_depth);
+  // every path ends within max_depth rounds of its injection and each round injects up to the
+  // queue capacity, so this many rounds always suffice; more means a logic error
+  const uint64_t max_rounds = (samples / cap + 2) * (uint64_t)(maxdepth + 2) + 64;
   BCtrl init;
   std::memset(&init, 0, sizeof(init));
   init.total = samples;
   init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, samples);
   init.injected = init.inj_n[0];
+  init.max_rounds = max_rounds;
   SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
   *b->host_ctrl = init;
   SWR_CUDA(cudaMemcpyAsync(b->ctrl, b->host_ctrl, sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
@@ -560,7 +587,8 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
     }
   };
   if (use_graph) {
-    // the eight-round chunk as one graph, rebuilt whenever an argument baked into it changes
+    // the whole round loop as one graph (a WHILE node over eight rounds and k_bcheck), rebuilt
+    // whenever an argument baked into it changes
     std::vector<char> key(sizeof(A) + sizeof(Q) + 3 * sizeof(void*));
     {
       char* k = key.data();
@@ -573,36 +601,65 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
     if (!b->graph || key != b->graph_key) {
       if (b->graph) cudaGraphExecDestroy(b->graph);
       b->graph = nullptr;
-      cudaStream_t cs;
-      SWR_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-      cudaGraph_t g;
-      SWR_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      enqueue_rounds(cs);
-      SWR_CUDA(cudaStreamEndCapture(cs, &g));
-      SWR_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
-      cudaGraphDestroy(g);
-      cudaStreamDestroy(cs);
+      b->graph_key.clear();
+      cudaGraph_t g = nullptr;
+      cudaStream_t cs = nullptr;
+      auto build = [&]() -> int {
+        SWR_CUDA(cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle loop;
+        SWR_CUDA(cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        SWR_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        SWR_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        SWR_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        enqueue_rounds(cs);
+        k_bcheck<<<1, 1, 0, cs>>>((BCtrl*)b->ctrl, loop);
+        cudaGraph_t captured = nullptr;
+        SWR_CUDA(cudaStreamEndCapture(cs, &captured));
+        SWR_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
+        return SWR_OK;
+      };
+      const int brc = build();
+      if (cs) cudaStreamDestroy(cs);
+      if (g) cudaGraphDestroy(g);
+      if (brc) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        return brc;
+      }
       b->graph_key = key;
     }
-  }
-  uint64_t rounds = 0;
-  uint32_t maxdepth = 0;
-  for (uint32_t k = 0; k < n; ++k) maxdepth = std::max(maxdepth, jobs[k].opts.max_depth);
-  const uint64_t max_rounds = (samples / cap + 2) * (uint64_t)(maxdepth + 2) + 64;
-  for (;;) {
-    if (rounds > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
-    if (use_graph) SWR_CUDA(cudaGraphLaunch(b->graph, stream));
-    else enqueue_rounds(stream);
-    rounds += 8;
+    SWR_CUDA(cudaGraphLaunch(b->graph, stream));
     SWR_CUDA(cudaGetLastError());
-    SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, b->ctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
-    SWR_CUDA(cudaStreamSynchronize(stream));
-    const BCtrl& h = *b->host_ctrl;
-    // after an even number of rounds the next shade reads parity 0
-    if (h.count[0] == 0 && h.inj_n[0] == 0 && h.injected == h.total) break;
+  } else {
+    // without a graph the host runs the loop: eight rounds, then a look at the control block
+    uint64_t rounds = 0;
+    for (;;) {
+      if (rounds > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
+      enqueue_rounds(stream);
+      rounds += 8;
+      SWR_CUDA(cudaGetLastError());
+      SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, b->ctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
+      SWR_CUDA(cudaStreamSynchronize(stream));
+      const BCtrl& h = *b->host_ctrl;
+      // after an even number of rounds the next shade reads parity 0
+      if (h.count[0] == 0 && h.inj_n[0] == 0 && h.injected == h.total) break;
+    }
   }
   k_bresolve<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(A);
   SWR_CUDA(cudaGetLastError());
+  if (use_graph) {
+    // the one wait of the call: the device-side loop's status
+    SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, b->ctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
+    SWR_CUDA(cudaStreamSynchronize(stream));
+    if (b->host_ctrl->status) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
+  }
   return SWR_OK;
 }
 

@@ -38,7 +38,7 @@ struct Ctrl {
   unsigned int cursor[2];
   unsigned int inj_n[2];
   unsigned int first_n;  // rays of the first non-empty bounce-traversal launch of the chunk
-  unsigned int pad0;
+  unsigned int pixel0;   // image pixel of the chunk's first pixel (read by the shading kernel)
   unsigned long long inj_base[2];
   unsigned long long injected;
   unsigned long long total;
@@ -46,6 +46,10 @@ struct Ctrl {
   unsigned long long bounce_rays;
   unsigned long long nodes;
   unsigned long long tris;
+  unsigned long long rounds;      // shade/trace rounds run by the device-side loop
+  unsigned long long max_rounds;  // its bound (every path ends within depth rounds of injection)
+  unsigned int status;            // 1: the device-side loop hit max_rounds without draining
+  unsigned int pad;
 };
 
 struct Queue {
@@ -116,6 +120,7 @@ __global__ void __launch_bounds__(kBlock)
   const uint32_t n_in = ctrl->count[parity];
   const uint32_t n_inj = ctrl->inj_n[parity];
   const unsigned long long inj_base = ctrl->inj_base[parity];
+  const uint32_t pixel0 = ctrl->pixel0;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (blockIdx.x * kBlock >= n_in + n_inj) return;
@@ -168,7 +173,7 @@ __global__ void __launch_bounds__(kBlock)
     if (slot != kDeadSlot) {
       swrx::ShadeParams P;
       P.seed = F.seed;
-      P.pixel = F.pixel0 + pixel;
+      P.pixel = pixel0 + pixel;
       P.sample = F.sample0 + sample;
       P.depth = F.depth;
       P.mode = F.mode;
@@ -767,7 +772,67 @@ struct Workspace {
   void* bd_head = nullptr;  // bidirectional tracer: per-sample vertex counts
   Ctrl* ctrl = nullptr;
   Ctrl* host_ctrl = nullptr;
+  cudaGraphExec_t graph = nullptr;  // the device-side round loop of the last launch shape
+  std::vector<char> graph_key;
 };
+
+// End of one iteration of the device-side round loop (eight shade/trace rounds, after which the
+// next shade reads parity 0): continue while paths are queued or samples wait for injection; stop
+// with status 1 once the proven bound on rounds is exceeded (never reached unless the wavefront
+// logic is broken), so the loop always ends.
+__global__ void k_round_check(Ctrl* __restrict__ ctrl, cudaGraphConditionalHandle loop) {
+  Ctrl& c = *ctrl;
+  c.rounds += 8;
+  const bool drained = c.count[0] == 0u && c.inj_n[0] == 0u && c.injected == c.total;
+  unsigned go = drained ? 0u : 1u;
+  if (!drained && c.rounds > c.max_rounds) {
+    c.status = 1u;
+    go = 0u;
+  }
+  cudaGraphSetConditional(loop, go);
+}
+
+// (Re)builds ws->graph: a WHILE node whose body is `rounds` (eight shade/trace rounds, enqueued on
+// the given stream) followed by k_round_check. The key holds every argument baked into it.
+template <class Enqueue>
+int round_loop_graph(Workspace* ws, const std::vector<char>& key, Ctrl* ctrl, Enqueue rounds) {
+  if (ws->graph && key == ws->graph_key) return SWR_OK;
+  if (ws->graph) cudaGraphExecDestroy(ws->graph);
+  ws->graph = nullptr;
+  ws->graph_key.clear();
+  cudaGraph_t g = nullptr;
+  cudaStream_t cs = nullptr;
+  auto build = [&]() -> int {
+    SWR_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle loop;
+    SWR_CUDA(cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    SWR_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+    SWR_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    SWR_CUDA(cudaStreamBeginCaptureToGraph(cs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+    rounds(cs);
+    k_round_check<<<1, 1, 0, cs>>>(ctrl, loop);
+    cudaGraph_t captured = nullptr;
+    SWR_CUDA(cudaStreamEndCapture(cs, &captured));
+    SWR_CUDA(cudaGraphInstantiate(&ws->graph, g, 0));
+    return SWR_OK;
+  };
+  const int rc = build();
+  if (cs) cudaStreamDestroy(cs);
+  if (g) cudaGraphDestroy(g);
+  if (rc) {
+    if (ws->graph) cudaGraphExecDestroy(ws->graph);
+    ws->graph = nullptr;
+    return rc;
+  }
+  ws->graph_key = key;
+  return SWR_OK;
+}
 
 int ensure(void** p, size_t& have, size_t want, size_t elem) {
   if (have >= want && *p) return SWR_OK;
@@ -992,12 +1057,17 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     F.pixel0 = (uint32_t)p0;
     F.npix = np;
     const uint64_t total = (uint64_t)np * o->spp;
+    // every path ends within max_depth rounds of its injection and each round injects up to the
+    // queue capacity, so this many rounds always suffice; more means a logic error
+    const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
     Ctrl init;
     std::memset(&init, 0, sizeof(init));
     init.total = total;
     init.inj_base[0] = 0;
     init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, total);
     init.injected = init.inj_n[0];
+    init.pixel0 = (uint32_t)p0;
+    init.max_rounds = max_rounds;
     SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
     *ws->host_ctrl = init;
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
@@ -1007,43 +1077,88 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     SWR_CUDA(timer.end(stream));
     SWR_CUDA(cudaGetLastError());
     P.launches++;
-    uint64_t k = 0;
-    // every path ends within max_depth rounds of its injection and each round injects up to the
-    // queue capacity, so this many rounds always suffice; more means a logic error
-    const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
-    for (;;) {
-      if (k > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
-      const int kChunk = 8;
-      for (int c = 0; c < kChunk; ++c, ++k) {
-        const int p = (int)(k & 1);
-        SWR_CUDA(timer.begin(stream, kTimeShade));
-        switch (block) {
-          case 128: k_shade<128><<<shade_grid, 128, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
-          case 512: k_shade<512><<<shade_grid, 512, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
-          default: k_shade<256><<<shade_grid, 256, 0, stream>>>(s->dev, F, ws->ctrl, Q[p], Q[p ^ 1], p); break;
-        }
-        SWR_CUDA(timer.end(stream));
-        SWR_CUDA(timer.begin(stream, kTimeTrace));
-        trace_kernel<<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, Q[p ^ 1], p);
-        SWR_CUDA(timer.end(stream));
-        P.launches += 2;
-        P.trace_launches++;
+    // the shading and traversal kernels read the chunk's first pixel from the control block, so
+    // their arguments (and a graph made of them) are the same for every chunk
+    Frame FR = F;
+    FR.pixel0 = 0;
+    FR.npix = 0;
+    auto round = [&](cudaStream_t st, int p) {
+      switch (block) {
+        case 128: k_shade<128><<<shade_grid, 128, 0, st>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+        case 512: k_shade<512><<<shade_grid, 512, 0, st>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+        default: k_shade<256><<<shade_grid, 256, 0, st>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
       }
+    };
+    if (!timer.on) {
+      // the round loop on the device: one graph launch (a WHILE node over eight rounds and
+      // k_round_check), one look at the control block when it has drained
+      std::vector<char> key(sizeof(DevScene) + sizeof(Frame) + sizeof(Q) + 5 * sizeof(void*));
+      {
+        char* kp = key.data();
+        std::memset(kp, 0, key.size());
+        std::memcpy(kp, &s->dev, sizeof(DevScene));
+        std::memcpy(kp + sizeof(DevScene), &FR, sizeof(Frame));
+        std::memcpy(kp + sizeof(DevScene) + sizeof(Frame), Q, sizeof(Q));
+        const void* extra[5] = {ws->ctrl, (void*)trace_kernel, (void*)(uintptr_t)block, (void*)(uintptr_t)trace_grid,
+                                (void*)(uintptr_t)shade_grid};
+        std::memcpy(kp + sizeof(DevScene) + sizeof(Frame) + sizeof(Q), extra, sizeof(extra));
+      }
+      int grc = round_loop_graph(ws, key, ws->ctrl, [&](cudaStream_t st) {
+        for (int c = 0; c < 8; ++c) {
+          const int p = c & 1;
+          round(st, p);
+          trace_kernel<<<trace_grid, kTraceBlock, 0, st>>>(s->dev, FR, ws->ctrl, Q[p ^ 1], p);
+        }
+      });
+      if (grc) return grc;
+      SWR_CUDA(cudaGraphLaunch(ws->graph, stream));
       SWR_CUDA(cudaGetLastError());
       SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl, ws->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
       P.d2h_bytes += sizeof(Ctrl);
       SWR_CUDA(cudaStreamSynchronize(stream));
-      SWR_CUDA(timer.collect());
       const Ctrl& h = *ws->host_ctrl;
-      const int np_ = (int)(k & 1);
-      if (h.count[np_] == 0 && h.inj_n[np_] == 0 && h.injected == h.total) {
-        P.rays += h.rays;
-        P.bounce_rays += h.bounce_rays;
-        if (P.first_trace_rays == 0) P.first_trace_rays = h.first_n;
-        P.node_visits += h.nodes;
-        P.tri_tests += h.tris;
-        P.iterations += k;
-        break;
+      if (h.status) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
+      P.rays += h.rays;
+      P.bounce_rays += h.bounce_rays;
+      if (P.first_trace_rays == 0) P.first_trace_rays = h.first_n;
+      P.node_visits += h.nodes;
+      P.tri_tests += h.tris;
+      P.iterations += h.rounds;
+      P.launches += 2 * h.rounds + h.rounds / 8;
+      P.trace_launches += h.rounds;
+    } else {
+      // profiled: the host runs the loop so that every launch has its CUDA events
+      uint64_t k = 0;
+      for (;;) {
+        if (k > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
+        const int kChunk = 8;
+        for (int c = 0; c < kChunk; ++c, ++k) {
+          const int p = (int)(k & 1);
+          SWR_CUDA(timer.begin(stream, kTimeShade));
+          round(stream, p);
+          SWR_CUDA(timer.end(stream));
+          SWR_CUDA(timer.begin(stream, kTimeTrace));
+          trace_kernel<<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, FR, ws->ctrl, Q[p ^ 1], p);
+          SWR_CUDA(timer.end(stream));
+          P.launches += 2;
+          P.trace_launches++;
+        }
+        SWR_CUDA(cudaGetLastError());
+        SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl, ws->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+        P.d2h_bytes += sizeof(Ctrl);
+        SWR_CUDA(cudaStreamSynchronize(stream));
+        SWR_CUDA(timer.collect());
+        const Ctrl& h = *ws->host_ctrl;
+        const int np_ = (int)(k & 1);
+        if (h.count[np_] == 0 && h.inj_n[np_] == 0 && h.injected == h.total) {
+          P.rays += h.rays;
+          P.bounce_rays += h.bounce_rays;
+          if (P.first_trace_rays == 0) P.first_trace_rays = h.first_n;
+          P.node_visits += h.nodes;
+          P.tri_tests += h.tris;
+          P.iterations += k;
+          break;
+        }
       }
     }
     SWR_CUDA(timer.begin(stream, kTimeResolve));
@@ -1088,6 +1203,7 @@ void free_workspace(swr_scene* s) {
   if (ws->bd_head) cudaFree(ws->bd_head);
   if (ws->ctrl) cudaFree(ws->ctrl);
   if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
+  if (ws->graph) cudaGraphExecDestroy(ws->graph);
   delete ws;
   s->workspace = nullptr;
 }
@@ -1428,6 +1544,7 @@ int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
     init.total = total;
     init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, total);
     init.injected = init.inj_n[0];
+    init.pixel0 = (uint32_t)p0;
     // pageable source: the copy has been taken when the call returns
     SWR_CUDA(cudaMemcpyAsync(ctrl, &init, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
     k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ctrl);
