@@ -49,7 +49,7 @@ struct Ctrl {
   unsigned long long rounds;      // shade/trace rounds run by the device-side loop
   unsigned long long max_rounds;  // its bound (every path ends within depth rounds of injection)
   unsigned int status;            // 1: the device-side loop hit max_rounds without draining
-  unsigned int pad;
+  unsigned int cam_cursor;        // next pixel of the chunk for the camera kernel
 };
 
 struct Queue {
@@ -80,38 +80,88 @@ struct Frame {
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
+// Camera prefix of every pixel of the chunk (PathTracer::renderPixel's ray and the first bounces
+// of traceSinglePath up to the first front-facing hit, path_tracer.cpp:18-27,42-60): the same for
+// every sample of the pixel, so it is traced once per pixel. Persistent with per-lane refill, as
+// the bounce traversal: a lane keeps its pixel's resumable traversal and, after a back-facing hit,
+// restarts it 0.01 further along the ray; when at least F.refill lanes of the warp are idle they
+// take that many new pixels from the chunk's pixel cursor with one atomic.
 __global__ void __launch_bounds__(kTraceBlock) k_camera(DevScene sc, Frame F, Ctrl* __restrict__ ctrl) {
   __shared__ uint2 stack[swrx::kStackShared * kTraceBlock];
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned refill = F.refill ? F.refill : 8u;
+  const f3 org = mk(F.org[0], F.org[1], F.org[2]);
+  swrx::Traversal tr;
+  bool active = false, exhausted = false;
+  uint32_t k = 0, i = 0;
+  f3 d = mk(0.0f, 0.0f, 0.0f);
   unsigned traced = 0;
-  if (k < F.npix) {
-  const uint32_t pix = F.pixel0 + k;
-  const uint32_t px = pix % F.W, py = pix / F.W;
-  f3 o = mk(F.org[0], F.org[1], F.org[2]);
-  const f3 d = swrx::primary_dir(F.vi, F.pi, px, py, F.W, F.H);
-  float4 rec0 = make_float4(0, 0, 0, 0), rec1 = make_float4(0, 0, 0, __uint_as_float(kDeadSlot));
-  for (uint32_t i = 0; i < F.depth; ++i) {
-    swrx::Hit h;
-    ++traced;
-    if (!swrx::trace_closest<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, o, d,
-                                    stack + threadIdx.x, kTraceBlock, h, nullptr))
-      break;
-    const f3 p = swrx::hit_point(o, d, h.t);
-    const f3 n = swrx::shading_normal(sc.tris, sc.shade, h.slot, p);
-    if (swrx::vdot(n, d) > 0.0f) {
-      o = swrx::vadd(p, swrx::vscale(0.01f, d));
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= refill) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(&ctrl->cam_cursor, (unsigned)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= F.npix) exhausted = true;
+      if (!active) {
+        const unsigned j = base + __popc(idle & lt);
+        if (j < F.npix) {
+          k = j;
+          i = 0;
+          const uint32_t pix = F.pixel0 + k;
+          d = swrx::primary_dir(F.vi, F.pi, pix % F.W, pix / F.W, F.W, F.H);
+          tr.init(org, d, stack + threadIdx.x, kTraceBlock);
+          ++traced;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
       continue;
     }
-    rec0 = make_float4(o.x, o.y, o.z, h.t);
-    rec1 = make_float4(d.x, d.y, d.z, __uint_as_float(h.slot | (i << 27)));
-    break;
-  }
-  F.cam[2 * (size_t)k] = rec0;
-  F.cam[2 * (size_t)k + 1] = rec1;
+    if (active && tr.template step<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, nullptr)) {
+      // depth slot i traced: a miss ends the prefix, a back face uses up the slot
+      float4 rec0 = make_float4(0, 0, 0, 0), rec1 = make_float4(0, 0, 0, __uint_as_float(kDeadSlot));
+      bool done = true;
+      if (tr.hit.slot != 0xFFFFFFFFu) {
+        const f3 o = tr.o;
+        const f3 p = swrx::hit_point(o, d, tr.hit.t);
+        const f3 n = swrx::shading_normal(sc.tris, sc.shade, tr.hit.slot, p);
+        if (swrx::vdot(n, d) > 0.0f) {
+          if (i + 1 < F.depth) {
+            tr.init(swrx::vadd(p, swrx::vscale(0.01f, d)), d, stack + threadIdx.x, kTraceBlock);
+            ++i;
+            ++traced;
+            done = false;
+          }
+        } else {
+          rec0 = make_float4(o.x, o.y, o.z, tr.hit.t);
+          rec1 = make_float4(d.x, d.y, d.z, __uint_as_float(tr.hit.slot | (i << 27)));
+        }
+      }
+      if (done) {
+        F.cam[2 * (size_t)k] = rec0;
+        F.cam[2 * (size_t)k + 1] = rec1;
+        active = false;
+      }
+    }
   }
   // count the traced camera-prefix rays: warp sum, one atomic per warp
   for (int off = 16; off > 0; off >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, off);
-  if (lane_id() == 0 && traced) atomicAdd(&ctrl->rays, (unsigned long long)traced);
+  if (lane == 0 && traced) atomicAdd(&ctrl->rays, (unsigned long long)traced);
+}
+
+// persistent grid of the camera kernel for a chunk of np pixels
+static unsigned camera_grid(const swr_scene* s, uint32_t np) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_camera, kTraceBlock, 0) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const uint64_t need = ((uint64_t)np + kTraceBlock - 1) / kTraceBlock;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)s->num_sms * std::max(per_sm, 1)));
 }
 
 template <int kBlock>
@@ -1073,7 +1123,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
     P.h2d_bytes += sizeof(Ctrl);
     SWR_CUDA(timer.begin(stream, kTimeCamera));
-    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    k_camera<<<camera_grid(s, np), kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
     SWR_CUDA(timer.end(stream));
     SWR_CUDA(cudaGetLastError());
     P.launches++;
@@ -1277,7 +1327,7 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
     SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
     *ws->host_ctrl = init;
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
-    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    k_camera<<<camera_grid(s, np), kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
     k_adjoint<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, dl, g_alb, g_em);
     SWR_CUDA(cudaGetLastError());
   }
@@ -1394,7 +1444,7 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
     SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
     *ws->host_ctrl = init;
     SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
-    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+    k_camera<<<camera_grid(s, np), kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
     B.nsamp = np * o->spp;
     kern<<<grid, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
     kconn<<<grid_c, kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl, B);
@@ -1547,7 +1597,7 @@ int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
     init.pixel0 = (uint32_t)p0;
     // pageable source: the copy has been taken when the call returns
     SWR_CUDA(cudaMemcpyAsync(ctrl, &init, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
-    k_camera<<<(np + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(s->dev, F, ctrl);
+    k_camera<<<camera_grid(s, np), kTraceBlock, 0, stream>>>(s->dev, F, ctrl);
     SWR_CUDA(cudaGetLastError());
     uint64_t k = 0;
     const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
