@@ -254,8 +254,9 @@ def _events_ms(fn, steps, flush):
     return total / steps
 
 
-def run_batch(args, cfg):
-    """C3: all scenes in one batched wavefront vs one single-scene render call per scene."""
+def batch_vs_per_scene(args, cfg, tune):
+    """One batch of cfg's scenes: the batched wavefront against one single-scene render call per
+    scene, both timed with CUDA events (L2 flushed between steps); returns a dict."""
     import torch
     import master_thesis_b200 as swr
     from master_thesis_b200 import autotune, scenes
@@ -276,7 +277,7 @@ def run_batch(args, cfg):
     outs = [torch.empty((j["height"], j["width"], 3), dtype=torch.float32, device="cuda") for j in jobs]
     jobs = [dict(j, out=o) for j, o in zip(jobs, outs)]
     batch = swr.Batch()
-    tuned = autotune.tune_batch(batch, jobs) if args.tune else {}
+    tuned = autotune.tune_batch(batch, jobs) if tune else {}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     for _ in range(max(args.warmup, 3)):
         batch.render(jobs, **tuned)
@@ -290,15 +291,32 @@ def run_batch(args, cfg):
     per_scene()
     s_ms = _events_ms(per_scene, args.steps, flush)
     diff = max(float((a - b).abs().max() / b.abs().max().clamp_min(1e-12)) for a, b in zip(batched, outs))
+    batch.close()
+    for j in jobs:
+        j["scene"].close()
+    return {"workload": "%d scenes, %d triangles, %d samples, depth %d, physical mode" %
+                        (len(jobs), tris, samples, cfg["depth"]),
+            "msamples_per_s": samples / (b_ms / 1e3) / 1e6, "ms_per_step": b_ms, "tuned": tuned,
+            "per_scene_launches": {"msamples_per_s": samples / (s_ms / 1e3) / 1e6, "ms_per_step": s_ms},
+            "speedup_vs_per_scene": s_ms / b_ms, "max_rel_image_diff_vs_per_scene": diff, "setup_s": setup_s}
+
+
+def run_batch(args, cfg):
+    """C3: all scenes in one batched wavefront vs one single-scene render call per scene; the line
+    also carries the same comparison on the batch restricted to small jobs (configuration c3s)."""
+    main = batch_vs_per_scene(args, cfg, args.tune)
+    small = batch_vs_per_scene(args, CONFIGS["c3s"], args.tune) if cfg is not CONFIGS["c3s"] else None
     print(json.dumps({
-        "metric": "Msamples/s (batched, %d scenes)" % len(jobs), "value": samples / (b_ms / 1e3) / 1e6,
-        "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded in-memory scenes)",
-        "config": {"workload": "%d scenes, %d triangles, %d samples, depth %d, physical mode" %
-                   (len(jobs), tris, samples, cfg["depth"]), "tuned": tuned},
-        "per_scene_launches": {"value": samples / (s_ms / 1e3) / 1e6, "ms_per_step": s_ms},
-        "speedup_vs_per_scene": s_ms / b_ms, "max_rel_image_diff_vs_per_scene": diff, "setup_s": setup_s}))
+        "metric": "Msamples/s (batched, %d scenes)" % cfg["scenes"], "value": main["msamples_per_s"],
+        "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": main["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded in-memory scenes)",
+        "config": {"workload": main["workload"], "tuned": main["tuned"]},
+        "per_scene_launches": {"value": main["per_scene_launches"]["msamples_per_s"],
+                               "ms_per_step": main["per_scene_launches"]["ms_per_step"]},
+        "speedup_vs_per_scene": main["speedup_vs_per_scene"],
+        "max_rel_image_diff_vs_per_scene": main["max_rel_image_diff_vs_per_scene"], "setup_s": main["setup_s"],
+        "small_job_batch": small}))
 
 
 def run_bdpt(args, cfg, files, workload):
