@@ -279,6 +279,8 @@ def batch_vs_per_scene(args, cfg, tune):
     batch = swr.Batch()
     tuned = autotune.tune_batch(batch, jobs) if tune else {}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    if args.no_graph:  # the rounds launched from the host (kernels visible to a profiler one by one)
+        tuned = dict(tuned, use_graph=False)
     for _ in range(max(args.warmup, 3)):
         batch.render(jobs, **tuned)
     b_ms = _events_ms(lambda: batch.render(jobs, **tuned), args.steps, flush)
@@ -787,6 +789,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scene-dir", default=None)
     ap.add_argument("--tune", action="store_true", help="autotune the launch shape (cached) before timing")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="batched configurations: launch the shade/trace rounds from the host instead of one graph")
     ap.add_argument("--split", default="images", choices=["images", "spp", "tiles"],
                     help="with N>1: independent images per GPU (weak scaling) or one image split by sample "
                          "range / pixel tile over the GPUs (strong scaling)")

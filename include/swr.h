@@ -120,7 +120,7 @@ typedef struct swr_render_opts {
   uint32_t flags;          /* SWR_RENDER_* */
   uint32_t refill;         /* bounce traversal: idle lanes (1..32) that trigger a refill, 0 = 8 */
   uint32_t trace_blocks;   /* bounce traversal: resident blocks per SM targeted by the register
-                              budget, one of 0 (compiler's choice), 8, 9, 10 */
+                              budget, one of 0 (compiler's choice), 9, 10 */
   uint32_t shade_batch;    /* adjoint: lanes of a warp with a pending hit that shade together
                               (1..32; fewer when no trace of the warp is in flight), 0 = the
                               library's choice; the wavefront renders ignore it */

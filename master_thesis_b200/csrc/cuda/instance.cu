@@ -558,7 +558,6 @@ int swr_scene_set_transforms(swr_scene* s, const swr_object_transform* xf, uint3
   }
   if (I->v.nlt) swr::k_inst_lights<<<swr::blocks(I->v.nlt, 128), 128, 0, stream>>>(I->v, (float4*)s->d_light_tris);
   SWR_CUDA(cudaGetLastError());
-  if (int rrc = swr::refresh_traversal_nodes(s, stream)) return rrc;
   // tie ranks: the scene-level order of the moved objects' boxes (SceneBuilder::finish)
   SWR_CUDA(cudaEventSynchronize(I->boxes_ready));
   const float* boxes = I->host_boxes;

@@ -1052,6 +1052,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   const bool host_samples = want_samples && is_host_pointer(samples_out);
 
   Frame F;
+  std::memset(&F, 0, sizeof(F));  // every byte, padding included, is part of the round-loop graph's key
   std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
   std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
   std::memcpy(F.org, cam->origin, sizeof(F.org));
@@ -1079,10 +1080,6 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 0, true> : k_trace_dyn<false, 0, true>)
                               : (count ? k_trace_dyn<true, 0, false> : k_trace_dyn<false, 0, false>);
       break;
-    case 8:
-      trace_kernel = postpone ? (count ? k_trace_dyn<true, 8, true> : k_trace_dyn<false, 8, true>)
-                              : (count ? k_trace_dyn<true, 8, false> : k_trace_dyn<false, 8, false>);
-      break;
     case 9:
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 9, true> : k_trace_dyn<false, 9, true>)
                               : (count ? k_trace_dyn<true, 9, false> : k_trace_dyn<false, 9, false>);
@@ -1091,7 +1088,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       trace_kernel = postpone ? (count ? k_trace_dyn<true, 10, true> : k_trace_dyn<false, 10, true>)
                               : (count ? k_trace_dyn<true, 10, false> : k_trace_dyn<false, 10, false>);
       break;
-    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0, 8, 9 or 10");
+    default: return set_error(SWR_ERR_INVALID, "swr: trace_blocks must be 0, 9 or 10");
   }
   if (static_fetch) trace_kernel = count ? k_trace<true> : k_trace<false>;
   if (o->refill > 32) return set_error(SWR_ERR_INVALID, "swr: refill must be 0..32");
@@ -1560,6 +1557,7 @@ int render_noalloc_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
     }
   }
   Frame F;
+  std::memset(&F, 0, sizeof(F));  // every byte, padding included, is part of the round-loop graph's key
   std::memcpy(F.vi, cam->view_inv, sizeof(F.vi));
   std::memcpy(F.pi, cam->proj_inv, sizeof(F.pi));
   std::memcpy(F.org, cam->origin, sizeof(F.org));

@@ -16,24 +16,6 @@ int cuda_fail(cudaError_t err, const char* what) {
   return set_error(SWR_ERR_CUDA, std::string("CUDA: ") + what + ": " + cudaGetErrorString(err));
 }
 
-__global__ void k_expand_nodes(const float4* __restrict__ src, float4* __restrict__ dst, uint32_t n) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) swrx::expand_node(src + (size_t)i * swrx::kNodeF4, dst + (size_t)i * swrx::kTravNodeF4);
-}
-
-int refresh_traversal_nodes(swr_scene* s, cudaStream_t stream) {
-  if (swrx::kTravNodeF4 == swrx::kNodeF4) {  // the traversal reads the compressed records
-    s->dev.nodes = (const float4*)s->d_nodes;
-    return SWR_OK;
-  }
-  const uint32_t n = s->dev.num_nodes;
-  if (!s->d_trav_nodes) SWR_CUDA(cudaMalloc(&s->d_trav_nodes, std::max<size_t>(1, n) * swrx::kTravNodeF4 * 16));
-  if (n) k_expand_nodes<<<(n + 255) / 256, 256, 0, stream>>>((const float4*)s->d_nodes, (float4*)s->d_trav_nodes, n);
-  SWR_CUDA(cudaGetLastError());
-  s->dev.nodes = (const float4*)s->d_trav_nodes;
-  return SWR_OK;
-}
-
 bool is_host_pointer(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -328,6 +310,7 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
     SWR_CUDA(cudaMalloc(&s->d_scratch, s->scratch_bytes));
     SWR_CUDA(cudaMemset(s->d_scratch, 0, s->scratch_bytes));
     swr::DevScene& ds = s->dev;
+    ds.nodes = (const float4*)s->d_nodes;
     ds.tris = (const float4*)s->d_tris;
     ds.shade = (const float4*)s->d_shade;
     ds.tri_boxes = (const float*)s->d_tri_boxes;
@@ -342,8 +325,6 @@ int swr_scene_create(const swr_scene_desc* d, const swr_build_opts* opts, swr_sc
     ds.num_slots = (uint32_t)pk.slot_to_id.size();
     ds.num_objects = d->num_objects;
     ds.num_tris = d->num_triangles;
-    if ((rc = swr::refresh_traversal_nodes(s.get(), nullptr))) return rc;
-    SWR_CUDA(cudaStreamSynchronize(nullptr));
     s->depth = pk.depth;
     s->node_bytes = (uint64_t)pk.num_nodes * 80;
     s->tri_bytes = (uint64_t)ds.num_slots * 48;
@@ -362,7 +343,7 @@ void swr_scene_destroy(swr_scene* s) {
   if (!s) return;
   swr::free_workspace(s);
   swr::free_instance(s);
-  for (void* p : {s->d_nodes, s->d_trav_nodes, s->d_tris, s->d_shade, s->d_tri_boxes, s->d_obj_boxes, s->d_mats,
+  for (void* p : {s->d_nodes, s->d_tris, s->d_shade, s->d_tri_boxes, s->d_obj_boxes, s->d_mats,
                   s->d_albedo, s->d_slot_of, s->d_scratch, s->d_lights, s->d_light_tris})
     if (p) cudaFree(p);
   delete s;

@@ -34,8 +34,7 @@ struct DevScene {
 struct swr_scene {
   swr::DevScene dev;
   // owned device allocations
-  void* d_nodes = nullptr;       // compressed wide-BVH records (builders, refit)
-  void* d_trav_nodes = nullptr;  // the traversal's decoded copy (swrx::kNodeFormat != 0)
+  void* d_nodes = nullptr;
   void* d_tris = nullptr;
   void* d_shade = nullptr;
   void* d_tri_boxes = nullptr;
@@ -69,10 +68,6 @@ int cuda_fail(cudaError_t err, const char* what);
 
 // true when p is host memory that the device cannot address directly
 bool is_host_pointer(const void* p);
-
-// points dev.nodes at the records the traversal reads: the compressed records, or (re)made
-// decoded copies of them (swrx::kNodeFormat); call after every write to d_nodes (scene.cu)
-int refresh_traversal_nodes(swr_scene* s, cudaStream_t stream);
 
 // releases the render workspace of a scene (render.cu)
 void free_workspace(swr_scene* s);

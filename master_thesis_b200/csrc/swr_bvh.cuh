@@ -36,24 +36,6 @@ namespace swrx {
 
 constexpr int kNodeF4 = 5;
 constexpr int kTriF4 = 3;
-
-// Record the traversal reads per node. The builders and the refit write the compressed records
-// above (the scene's canonical tree); with kNodeFormat != 0 the traversal reads a decoded copy
-// made by expand_node, whose plane values are the same 8-bit grid values q stored as numbers, so
-// every box test computes fmaf(q, 2^e / d, (p - o) / d) with the same q and gives bit-identical
-// results (the same node visits and hits) without the byte-to-float conversions:
-//   kNodeFormat 0  the compressed 80-byte record itself
-//   kNodeFormat 1  128 bytes: f4[0], f4[1] as above, then per axis the 8 lo and the 8 hi values
-//                  as half-precision numbers (8 halves per float4)
-//   kNodeFormat 2  224 bytes: f4[0], f4[1] as above, then per axis lo[0..3] lo[4..7] hi[0..3]
-//                  hi[4..7] as floats
-//   kNodeFormat 3  the compressed record, its bytes turned into floats by a byte permute into the
-//                  significand of 2^23 and a subtraction of 2^23 instead of a conversion
-#ifndef SWR_NODE_FORMAT
-#define SWR_NODE_FORMAT 0
-#endif
-constexpr int kNodeFormat = SWR_NODE_FORMAT;
-constexpr int kTravNodeF4 = (kNodeFormat == 0 || kNodeFormat == 3) ? 5 : (kNodeFormat == 1 ? 8 : 14);
 constexpr int kStackShared = 8;   // entries per thread kept in shared memory
 constexpr int kStackTotal = 64;   // maximum traversal stack depth (checked at build time)
 constexpr float kPruneSlack = 1.0f + 1.0f / 1024.0f;
@@ -157,66 +139,7 @@ SWR_HD float4 ldg4(const float4* p) {
 // Byte k (0..3) of w as a float, exactly. (Measured on B200: the integer-to-float conversion is
 // slightly faster here than building 2^23 + byte with a byte-permute and subtracting 2^23, since
 // the traversal keeps the ALU and FMA pipes busier than the conversion pipe.)
-SWR_HD float byte_f(uint32_t w, int k) {
-#if defined(__CUDA_ARCH__)
-  if (kNodeFormat == 3) return __uint_as_float(__byte_perm(w, 0x00004B00u, 0x5440u | (uint32_t)k)) - 8388608.0f;
-#endif
-  return (float)((w >> (8 * k)) & 0xFFu);
-}
-
-// Half k (0 = low, 1 = high) of w, a half-precision number, as a float
-SWR_HD float half_f(uint32_t w, int k) {
-#if defined(__CUDA_ARCH__)
-  const uint32_t v = k ? (w >> 16) : w;
-  float r;
-  asm("{.reg .b16 lo, hi; mov.b32 {lo, hi}, %1; cvt.f32.f16 %0, lo;}" : "=f"(r) : "r"(v));
-  return r;
-#else
-  const uint32_t h = (k ? (w >> 16) : w) & 0xFFFFu;  // the values stored here: integers 0..255
-  if (h == 0) return 0.0f;
-  const int e = (int)(h >> 10) - 15;
-  return std::ldexp((float)((h & 0x3FFu) | 0x400u), e - 10);
-#endif
-}
-
-// 16-bit half-precision bit pattern of an integer 0..255 (exact: 11-bit significand)
-SWR_HD uint32_t half_of_byte(uint32_t b) {
-  if (b == 0) return 0u;
-  int e = 7;  // leading bit position
-  while (!((b >> e) & 1u)) --e;
-  return (uint32_t)((e + 15) << 10) | ((b << (10 - e)) & 0x3FFu);
-}
-
-// The traversal's record of one node from its compressed record (see kNodeFormat); dst holds
-// kTravNodeF4 float4. With kNodeFormat 0 it is a copy.
-SWR_HD void expand_node(const float4* src, float4* dst) {
-  dst[0] = src[0];
-  dst[1] = src[1];
-  if (kNodeFormat == 0 || kNodeFormat == 3) {
-    dst[2] = src[2];
-    dst[3] = src[3];
-    dst[4] = src[4];
-    return;
-  }
-  // plane words: lo_x0 lo_x1 lo_y0 lo_y1 | lo_z0 lo_z1 hi_x0 hi_x1 | hi_y0 hi_y1 hi_z0 hi_z1
-  const uint32_t w[12] = {f2bits(src[2].x), f2bits(src[2].y), f2bits(src[2].z), f2bits(src[2].w),
-                          f2bits(src[3].x), f2bits(src[3].y), f2bits(src[3].z), f2bits(src[3].w),
-                          f2bits(src[4].x), f2bits(src[4].y), f2bits(src[4].z), f2bits(src[4].w)};
-  for (int a = 0; a < 3; ++a)
-    for (int side = 0; side < 2; ++side) {
-      const uint32_t w0 = w[6 * side + 2 * a], w1 = w[6 * side + 2 * a + 1];
-      uint32_t q[8];
-      for (int i = 0; i < 8; ++i) q[i] = ((i < 4 ? w0 : w1) >> (8 * (i & 3))) & 0xFFu;
-      if (kNodeFormat == 1) {
-        uint32_t h[4];
-        for (int k = 0; k < 4; ++k) h[k] = half_of_byte(q[2 * k]) | (half_of_byte(q[2 * k + 1]) << 16);
-        dst[2 + 2 * a + side] = make_float4(bits2f(h[0]), bits2f(h[1]), bits2f(h[2]), bits2f(h[3]));
-      } else {
-        dst[2 + 4 * a + 2 * side] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-        dst[2 + 4 * a + 2 * side + 1] = make_float4((float)q[4], (float)q[5], (float)q[6], (float)q[7]);
-      }
-    }
-}
+SWR_HD float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
 
 // max / min of three floats, NaN operands ignored as by fmaxf / fminf
 SWR_HD float fmax3(float a, float b, float c) {
@@ -338,8 +261,9 @@ struct Traversal {
       if (ng.y & 0xFF000000u) st.push(ng);
       if (kStats) stats->nodes++;
 
-      const float4* np = nodes + (size_t)child * kTravNodeF4;
-      const float4 n0 = ldg4(np + 0), n1 = ldg4(np + 1);
+      const float4* np = nodes + (size_t)child * kNodeF4;
+      const float4 n0 = ldg4(np + 0), n1 = ldg4(np + 1), n2 = ldg4(np + 2);
+      const float4 n3 = ldg4(np + 3), n4 = ldg4(np + 4);
       const uint32_t hdr = f2bits(n0.w);
       const float ex = bits2f((hdr & 0xFFu) << 23);
       const float ey = bits2f(((hdr >> 8) & 0xFFu) << 23);
@@ -347,11 +271,28 @@ struct Traversal {
       const uint32_t imask = hdr >> 24;
       const float ax = ex * idx, ay = ey * idy, az = ez * idz;
       const float bx = (n0.x - o.x) * idx, by = (n0.y - o.y) * idy, bz = (n0.z - o.z) * idz;
+      // near/far plane bytes by direction sign
+      const uint32_t lox0 = f2bits(n2.x), lox1 = f2bits(n2.y), loy0 = f2bits(n2.z), loy1 = f2bits(n2.w);
+      const uint32_t loz0 = f2bits(n3.x), loz1 = f2bits(n3.y), hix0 = f2bits(n3.z), hix1 = f2bits(n3.w);
+      const uint32_t hiy0 = f2bits(n4.x), hiy1 = f2bits(n4.y), hiz0 = f2bits(n4.z), hiz1 = f2bits(n4.w);
+      const uint32_t nx0 = (oct & 1u) ? hix0 : lox0, nx1 = (oct & 1u) ? hix1 : lox1;
+      const uint32_t fx0 = (oct & 1u) ? lox0 : hix0, fx1 = (oct & 1u) ? lox1 : hix1;
+      const uint32_t ny0 = (oct & 2u) ? hiy0 : loy0, ny1 = (oct & 2u) ? hiy1 : loy1;
+      const uint32_t fy0 = (oct & 2u) ? loy0 : hiy0, fy1 = (oct & 2u) ? loy1 : hiy1;
+      const uint32_t nz0 = (oct & 4u) ? hiz0 : loz0, nz1 = (oct & 4u) ? hiz1 : loz1;
+      const uint32_t fz0 = (oct & 4u) ? loz0 : hiz0, fz1 = (oct & 4u) ? loz1 : hiz1;
       const uint32_t meta0 = f2bits(n1.z), meta1 = f2bits(n1.w);
       uint32_t inner = 0, trih = 0;
-      // one child slot: its near/far grid values per axis -> entry/exit distances -> hit bits
-      auto test = [&](int i, float qnx, float qny, float qnz, float qfx, float qfy, float qfz) {
-        const uint32_t m = ((i < 4 ? meta0 : meta1) >> ((i & 3) * 8)) & 0xFFu;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int sh = (i & 3) * 8;
+        const uint32_t m = ((i < 4 ? meta0 : meta1) >> sh) & 0xFFu;
+        const float qnx = byte_f(i < 4 ? nx0 : nx1, i & 3);
+        const float qny = byte_f(i < 4 ? ny0 : ny1, i & 3);
+        const float qnz = byte_f(i < 4 ? nz0 : nz1, i & 3);
+        const float qfx = byte_f(i < 4 ? fx0 : fx1, i & 3);
+        const float qfy = byte_f(i < 4 ? fy0 : fy1, i & 3);
+        const float qfz = byte_f(i < 4 ? fz0 : fz1, i & 3);
         const float tnx = fmaf(qnx, ax, bx), tny = fmaf(qny, ay, by), tnz = fmaf(qnz, az, bz);
         const float tfx = fmaf(qfx, ax, bx), tfy = fmaf(qfy, ay, by), tfz = fmaf(qfz, az, bz);
         const float tn = fmax3(tnx, tny, fmaxf(tnz, 0.0f));
@@ -360,53 +301,6 @@ struct Traversal {
         if (tn <= tf && (is_inner || m != 0u)) {
           if (is_inner) inner |= 1u << (i ^ (int)oct);
           else trih |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-        }
-      };
-      if (kNodeFormat == 0 || kNodeFormat == 3) {
-        const float4 n2 = ldg4(np + 2), n3 = ldg4(np + 3), n4 = ldg4(np + 4);
-        // near/far plane bytes by direction sign
-        const uint32_t lox0 = f2bits(n2.x), lox1 = f2bits(n2.y), loy0 = f2bits(n2.z), loy1 = f2bits(n2.w);
-        const uint32_t loz0 = f2bits(n3.x), loz1 = f2bits(n3.y), hix0 = f2bits(n3.z), hix1 = f2bits(n3.w);
-        const uint32_t hiy0 = f2bits(n4.x), hiy1 = f2bits(n4.y), hiz0 = f2bits(n4.z), hiz1 = f2bits(n4.w);
-        const uint32_t nx0 = (oct & 1u) ? hix0 : lox0, nx1 = (oct & 1u) ? hix1 : lox1;
-        const uint32_t fx0 = (oct & 1u) ? lox0 : hix0, fx1 = (oct & 1u) ? lox1 : hix1;
-        const uint32_t ny0 = (oct & 2u) ? hiy0 : loy0, ny1 = (oct & 2u) ? hiy1 : loy1;
-        const uint32_t fy0 = (oct & 2u) ? loy0 : hiy0, fy1 = (oct & 2u) ? loy1 : hiy1;
-        const uint32_t nz0 = (oct & 4u) ? hiz0 : loz0, nz1 = (oct & 4u) ? hiz1 : loz1;
-        const uint32_t fz0 = (oct & 4u) ? loz0 : hiz0, fz1 = (oct & 4u) ? loz1 : hiz1;
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-          test(i, byte_f(i < 4 ? nx0 : nx1, i & 3), byte_f(i < 4 ? ny0 : ny1, i & 3),
-               byte_f(i < 4 ? nz0 : nz1, i & 3), byte_f(i < 4 ? fx0 : fx1, i & 3),
-               byte_f(i < 4 ? fy0 : fy1, i & 3), byte_f(i < 4 ? fz0 : fz1, i & 3));
-      } else if (kNodeFormat == 1) {
-        // per axis one float4 of 8 lo halves and one of 8 hi halves; near = hi for a negative
-        // direction component
-        const float4 nxq = ldg4(np + 2 + ((oct & 1u) ? 1 : 0)), fxq = ldg4(np + 2 + ((oct & 1u) ? 0 : 1));
-        const float4 nyq = ldg4(np + 4 + ((oct & 2u) ? 1 : 0)), fyq = ldg4(np + 4 + ((oct & 2u) ? 0 : 1));
-        const float4 nzq = ldg4(np + 6 + ((oct & 4u) ? 1 : 0)), fzq = ldg4(np + 6 + ((oct & 4u) ? 0 : 1));
-        const uint32_t nx[4] = {f2bits(nxq.x), f2bits(nxq.y), f2bits(nxq.z), f2bits(nxq.w)};
-        const uint32_t ny[4] = {f2bits(nyq.x), f2bits(nyq.y), f2bits(nyq.z), f2bits(nyq.w)};
-        const uint32_t nz[4] = {f2bits(nzq.x), f2bits(nzq.y), f2bits(nzq.z), f2bits(nzq.w)};
-        const uint32_t fx[4] = {f2bits(fxq.x), f2bits(fxq.y), f2bits(fxq.z), f2bits(fxq.w)};
-        const uint32_t fy[4] = {f2bits(fyq.x), f2bits(fyq.y), f2bits(fyq.z), f2bits(fyq.w)};
-        const uint32_t fz[4] = {f2bits(fzq.x), f2bits(fzq.y), f2bits(fzq.z), f2bits(fzq.w)};
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-          test(i, half_f(nx[i >> 1], i & 1), half_f(ny[i >> 1], i & 1), half_f(nz[i >> 1], i & 1),
-               half_f(fx[i >> 1], i & 1), half_f(fy[i >> 1], i & 1), half_f(fz[i >> 1], i & 1));
-      } else {
-        // per axis lo[0..3] lo[4..7] hi[0..3] hi[4..7]; four slots at a time to bound registers
-        const int sx = (oct & 1u) ? 2 : 0, sy = (oct & 2u) ? 2 : 0, sz = (oct & 4u) ? 2 : 0;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float4 nxq = ldg4(np + 2 + sx + h), fxq = ldg4(np + 4 - sx + h);
-          const float4 nyq = ldg4(np + 6 + sy + h), fyq = ldg4(np + 8 - sy + h);
-          const float4 nzq = ldg4(np + 10 + sz + h), fzq = ldg4(np + 12 - sz + h);
-          test(4 * h + 0, nxq.x, nyq.x, nzq.x, fxq.x, fyq.x, fzq.x);
-          test(4 * h + 1, nxq.y, nyq.y, nzq.y, fxq.y, fyq.y, fzq.y);
-          test(4 * h + 2, nxq.z, nyq.z, nzq.z, fxq.z, fyq.z, fzq.z);
-          test(4 * h + 3, nxq.w, nyq.w, nzq.w, fxq.w, fyq.w, fzq.w);
         }
       }
       ng = make_uint2(f2bits(n1.x), (inner << 24) | imask);

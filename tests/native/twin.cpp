@@ -14,7 +14,6 @@ namespace {
 
 struct Twin {
   swr::PackedScene pk;
-  std::vector<float4> trav;  // the records the traversal reads (swrx::expand_node of pk.nodes)
 };
 
 }  // namespace
@@ -27,10 +26,6 @@ void* twin_create(const swr_scene_desc* d, const swr_build_opts* o) {
     delete t;
     return nullptr;
   }
-  const float4* src = (const float4*)t->pk.nodes.data();
-  t->trav.resize((size_t)t->pk.num_nodes * swrx::kTravNodeF4);
-  for (uint32_t i = 0; i < t->pk.num_nodes; ++i)
-    swrx::expand_node(src + (size_t)i * swrx::kNodeF4, t->trav.data() + (size_t)i * swrx::kTravNodeF4);
   return t;
 }
 
@@ -111,7 +106,6 @@ uint32_t twin_nodes(void* t) { return ((Twin*)t)->pk.num_nodes; }
 void twin_trace(void* tw, const float* ro, const float* rd, uint64_t n, uint32_t* tri, float* d2,
                 float* tt, uint32_t* counts, int postpone) {
   const swr::PackedScene& p = ((Twin*)tw)->pk;
-  const float4* trav = ((Twin*)tw)->trav.data();
   uint2 stack[swrx::kStackShared];
   for (uint64_t i = 0; i < n; ++i) {
     swrx::Hit h;
@@ -119,10 +113,10 @@ void twin_trace(void* tw, const float* ro, const float* rd, uint64_t n, uint32_t
     const swrx::f3 o = swrx::mk(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]);
     const swrx::f3 d = swrx::mk(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]);
     if (postpone)
-      swrx::trace_closest<true, true>(trav, p.tris.data(), p.tri_boxes.data(),
+      swrx::trace_closest<true, true>((const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(),
                                       p.obj_boxes.data(), o, d, stack, 1, h, &st);
     else
-      swrx::trace_closest<true, false>(trav, p.tris.data(), p.tri_boxes.data(),
+      swrx::trace_closest<true, false>((const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(),
                                        p.obj_boxes.data(), o, d, stack, 1, h, &st);
     tri[i] = h.id;
     d2[i] = h.d2;
@@ -140,8 +134,7 @@ void twin_render(void* tw, const swr_camera* cam, uint32_t W, uint32_t H, uint32
                  uint64_t seed, uint32_t mode, uint32_t rr_depth, float rr_q, uint32_t p0, uint32_t p1,
                  float* per_sample) {
   const swr::PackedScene& p = ((Twin*)tw)->pk;
-  const float4* trav = ((Twin*)tw)->trav.data();
-  const float4* nodes = trav;
+  const float4* nodes = (const float4*)p.nodes.data();
   uint2 stack[swrx::kStackShared];
   for (uint32_t pix = p0; pix < p1; ++pix) {
     swrx::f3 o = swrx::mk(cam->origin[0], cam->origin[1], cam->origin[2]);
@@ -226,12 +219,11 @@ void twin_render(void* tw, const swr_camera* cam, uint32_t W, uint32_t H, uint32
 // traceRay's closest hit (the ray-query rule) with the kernels' traversal code
 void twin_rt_trace(void* tw, const float* ro, const float* rd, uint64_t n, uint32_t* tri, float* t) {
   const swr::PackedScene& p = ((Twin*)tw)->pk;
-  const float4* trav = ((Twin*)tw)->trav.data();
   uint2 stack[swrx::kStackShared];
   for (uint64_t i = 0; i < n; ++i) {
     swrx::Hit h;
     swrx::trace_closest<false, false, swrx::kRuleRayQuery>(
-        trav, p.tris.data(), p.tri_boxes.data(), p.obj_boxes.data(),
+        (const float4*)p.nodes.data(), p.tris.data(), p.tri_boxes.data(), p.obj_boxes.data(),
         swrx::mk(ro[4 * i], ro[4 * i + 1], ro[4 * i + 2]), swrx::mk(rd[4 * i], rd[4 * i + 1], rd[4 * i + 2]), stack, 1,
         h, nullptr);
     tri[i] = h.id;
@@ -245,8 +237,7 @@ void twin_rt_render(void* tw, const swr_camera* cam, uint32_t W, uint32_t H, uin
                     uint32_t p0, uint32_t p1, float* rgb) {
   namespace rt = swrx::rt;
   const swr::PackedScene& p = ((Twin*)tw)->pk;
-  const float4* trav = ((Twin*)tw)->trav.data();
-  const float4* nodes = trav;
+  const float4* nodes = (const float4*)p.nodes.data();
   uint2 stack[swrx::kStackShared];
   auto trace = [&](swrx::f3 o, swrx::f3 d, swrx::Hit& h) {
     return swrx::trace_closest<false, false, swrx::kRuleRayQuery>(nodes, p.tris.data(), p.tri_boxes.data(),
