@@ -129,11 +129,15 @@ SWR_HD bool ref_intersect(f3 o, f3 d, f3 v0, f3 e0, f3 e1, float& t_out, float& 
   if (a > -EPS && a < EPS) return false;
   f3 s = vsub(o, v0);
   const float sh = vdot(s, h);
+#ifndef SWR_MT_PLAIN
   const float tiny = fabsf(a) * 0x1p-100f;
   if ((a > 0.0f ? sh < 0.0f : sh > 0.0f) && fabsf(sh) >= tiny) return false;  // u < 0
+#endif
   f3 q = vcross(s, e0);
   const float dq = vdot(d, q);
+#ifndef SWR_MT_PLAIN
   if ((a > 0.0f ? dq < 0.0f : dq > 0.0f) && fabsf(dq) >= tiny) return false;  // v < 0
+#endif
   float f = frcp(a);
   float u = fmul(f, sh);
   if (u < 0.0f || u > 1.0f) return false;
