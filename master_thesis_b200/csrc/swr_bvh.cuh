@@ -283,10 +283,6 @@ struct Traversal {
       const uint32_t fz0 = (oct & 4u) ? loz0 : hiz0, fz1 = (oct & 4u) ? loz1 : hiz1;
       const uint32_t meta0 = f2bits(n1.z), meta1 = f2bits(n1.w);
       uint32_t inner = 0, trih = 0;
-#ifdef SWR_NEAR_FIRST
-      float near_tn = INFINITY;
-      int near_k = 0;
-#endif
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int sh = (i & 3) * 8;
@@ -305,20 +301,8 @@ struct Traversal {
         if (tn <= tf && (is_inner || m != 0u)) {
           if (is_inner) inner |= 1u << (i ^ (int)oct);
           else trih |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-#ifdef SWR_NEAR_FIRST
-          if (is_inner && tn < near_tn) {
-            near_tn = tn;
-            near_k = i ^ (int)oct;
-          }
-#endif
         }
       }
-#ifdef SWR_NEAR_FIRST
-      if (inner & (inner - 1u)) {
-        st.push(make_uint2(f2bits(n1.x), ((inner & ~(1u << near_k)) << 24) | imask));
-        inner = 1u << near_k;
-      }
-#endif
       ng = make_uint2(f2bits(n1.x), (inner << 24) | imask);
       tg = make_uint2(f2bits(n1.y), trih);
       if (kPostpone) return false;

@@ -116,32 +116,17 @@ SWR_HD bool ref_slab(const float lo[3], const float hi[3], f3 o, f3 inv) {
 // Moller-Trumbore of the reference (triangle.cpp:21-45) with its EPS = 1e-7 and its order of
 // operations. On a hit returns t and the squared distance from the ray origin to the hit point
 // computed as ray.origin.distanceSquared(origin + t*dir) (graphics_object.cpp:77).
-//
-// The reciprocal f = 1/a is formed only for candidates that can still hit: u = f*(s.h) and
-// v = f*(d.q) are negative exactly when their second factor has the other sign than a and the
-// rounded product does not underflow to zero, which |x| >= |a|*2^-100 rules out (|f*x| is then
-// about 2^-100 or more). Those rejections are taken first from the same dot products, so results
-// are unchanged and most missed triangles skip the division.
 SWR_HD bool ref_intersect(f3 o, f3 d, f3 v0, f3 e0, f3 e1, float& t_out, float& d2_out) {
   const float EPS = 0.0000001f;
   f3 h = vcross(d, e1);
   float a = vdot(e0, h);
   if (a > -EPS && a < EPS) return false;
-  f3 s = vsub(o, v0);
-  const float sh = vdot(s, h);
-#ifndef SWR_MT_PLAIN
-  const float tiny = fabsf(a) * 0x1p-100f;
-  if ((a > 0.0f ? sh < 0.0f : sh > 0.0f) && fabsf(sh) >= tiny) return false;  // u < 0
-#endif
-  f3 q = vcross(s, e0);
-  const float dq = vdot(d, q);
-#ifndef SWR_MT_PLAIN
-  if ((a > 0.0f ? dq < 0.0f : dq > 0.0f) && fabsf(dq) >= tiny) return false;  // v < 0
-#endif
   float f = frcp(a);
-  float u = fmul(f, sh);
+  f3 s = vsub(o, v0);
+  float u = fmul(f, vdot(s, h));
   if (u < 0.0f || u > 1.0f) return false;
-  float v = fmul(f, dq);
+  f3 q = vcross(s, e0);
+  float v = fmul(f, vdot(d, q));
   if (v < 0.0f || fadd(u, v) > 1.0f) return false;
   float t = fmul(f, vdot(e1, q));
   if (!(t > EPS)) return false;
