@@ -27,6 +27,7 @@ RENDER_PROFILE = 2
 RENDER_COUNT = 4
 RENDER_STATIC_FETCH = 8
 RENDER_POSTPONE = 16
+RENDER_ONE_WAVEFRONT = 32
 
 
 class SwrError(RuntimeError):

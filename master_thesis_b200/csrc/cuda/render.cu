@@ -32,6 +32,8 @@ using swrx::mk;
 constexpr uint32_t kDeadSlot = 0xFFFFFFFFu;
 constexpr int kTraceBlock = 128;
 constexpr uint64_t kChunkSamples = 1ull << 27;
+// chunks of at least this many samples run as two concurrent sub-wavefronts (SWR_RENDER_ONE_WAVEFRONT)
+constexpr uint64_t kTwoWaveSamples = 1ull << 20;
 
 struct Ctrl {
   unsigned int count[2];
@@ -820,10 +822,12 @@ struct Workspace {
   void* stage = nullptr;  // device image for callers that pass a host output buffer
   void* bd_vtx = nullptr;   // bidirectional tracer: per-sample vertex tables
   void* bd_head = nullptr;  // bidirectional tracer: per-sample vertex counts
-  Ctrl* ctrl = nullptr;
-  Ctrl* host_ctrl = nullptr;
-  cudaGraphExec_t graph = nullptr;  // the device-side round loop of the last launch shape
-  std::vector<char> graph_key;
+  Ctrl* ctrl = nullptr;       // [2] control blocks (the second for a concurrent sub-wavefront)
+  Ctrl* host_ctrl = nullptr;  // [2] pinned copies
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // device-side round loop per sub-wavefront
+  std::vector<char> graph_key[2];
+  cudaStream_t side = nullptr;  // the second sub-wavefront's stream
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 // End of one iteration of the device-side round loop (eight shade/trace rounds, after which the
@@ -842,14 +846,15 @@ __global__ void k_round_check(Ctrl* __restrict__ ctrl, cudaGraphConditionalHandl
   cudaGraphSetConditional(loop, go);
 }
 
-// (Re)builds ws->graph: a WHILE node whose body is `rounds` (eight shade/trace rounds, enqueued on
+// (Re)builds graph: a WHILE node whose body is `rounds` (eight shade/trace rounds, enqueued on
 // the given stream) followed by k_round_check. The key holds every argument baked into it.
 template <class Enqueue>
-int round_loop_graph(Workspace* ws, const std::vector<char>& key, Ctrl* ctrl, Enqueue rounds) {
-  if (ws->graph && key == ws->graph_key) return SWR_OK;
-  if (ws->graph) cudaGraphExecDestroy(ws->graph);
-  ws->graph = nullptr;
-  ws->graph_key.clear();
+int round_loop_graph(cudaGraphExec_t& graph, std::vector<char>& graph_key, const std::vector<char>& key, Ctrl* ctrl,
+                     Enqueue rounds) {
+  if (graph && key == graph_key) return SWR_OK;
+  if (graph) cudaGraphExecDestroy(graph);
+  graph = nullptr;
+  graph_key.clear();
   cudaGraph_t g = nullptr;
   cudaStream_t cs = nullptr;
   auto build = [&]() -> int {
@@ -869,18 +874,18 @@ int round_loop_graph(Workspace* ws, const std::vector<char>& key, Ctrl* ctrl, En
     k_round_check<<<1, 1, 0, cs>>>(ctrl, loop);
     cudaGraph_t captured = nullptr;
     SWR_CUDA(cudaStreamEndCapture(cs, &captured));
-    SWR_CUDA(cudaGraphInstantiate(&ws->graph, g, 0));
+    SWR_CUDA(cudaGraphInstantiate(&graph, g, 0));
     return SWR_OK;
   };
   const int rc = build();
   if (cs) cudaStreamDestroy(cs);
   if (g) cudaGraphDestroy(g);
   if (rc) {
-    if (ws->graph) cudaGraphExecDestroy(ws->graph);
-    ws->graph = nullptr;
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
     return rc;
   }
-  ws->graph_key = key;
+  graph_key = key;
   return SWR_OK;
 }
 
@@ -1023,8 +1028,8 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->contrib, ws->contrib_n, px_per_chunk * o->spp, sizeof(float4)))) return rc;
   if (!ws->ctrl) {
-    SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
-    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
+    SWR_CUDA(cudaMalloc(&ws->ctrl, 2 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 2 * sizeof(Ctrl)));
   }
 
   Queue Q[2];
@@ -1098,83 +1103,149 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
   const unsigned shade_grid = (cap + block - 1) / block;
 
+  // Sub-wavefront h of a chunk: pixels [off, off + n) of it, queues of capw paths carved from the
+  // h-th half of the queue buffer (the whole buffer when the chunk runs as one wavefront), control
+  // block h; everything it launches goes to stream st. Graph path only.
+  auto launch_wave = [&](int h, cudaStream_t st, uint64_t p0, uint64_t off, uint32_t n, uint32_t capw) -> int {
+    Queue Qh[2];
+    {
+      char* b = (char*)ws->qbuf + (size_t)h * ((size_t)capw * (4 * sizeof(float4) + sizeof(uint2)) * 2);
+      for (int q = 0; q < 2; ++q) {
+        Qh[q].o = (float4*)b; b += (size_t)capw * sizeof(float4);
+        Qh[q].d = (float4*)b; b += (size_t)capw * sizeof(float4);
+        Qh[q].c = (float4*)b; b += (size_t)capw * sizeof(float4);
+        Qh[q].l = (float4*)b; b += (size_t)capw * sizeof(float4);
+        Qh[q].hit = (uint2*)b; b += (size_t)capw * sizeof(uint2);
+      }
+    }
+    Ctrl* ctrl = ws->ctrl + h;
+    Frame Fh = F;
+    Fh.pixel0 = (uint32_t)(p0 + off);
+    Fh.npix = n;
+    Fh.cam = F.cam + 2 * off;
+    Fh.contrib = F.contrib + off * o->spp;
+    Fh.capacity = capw;
+    const uint64_t total = (uint64_t)n * o->spp;
+    // every path ends within max_depth rounds of its injection and each round injects up to the
+    // queue capacity, so this many rounds always suffice; more means a logic error
+    Ctrl init;
+    std::memset(&init, 0, sizeof(init));
+    init.total = total;
+    init.inj_n[0] = (unsigned)std::min<uint64_t>(capw, total);
+    init.injected = init.inj_n[0];
+    init.pixel0 = Fh.pixel0;
+    init.max_rounds = (total / capw + 2) * (uint64_t)(o->max_depth + 2) + 64;
+    ws->host_ctrl[h] = init;
+    SWR_CUDA(cudaMemcpyAsync(ctrl, ws->host_ctrl + h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    P.h2d_bytes += sizeof(Ctrl);
+    k_camera<<<camera_grid(s, n), kTraceBlock, 0, st>>>(s->dev, Fh, ctrl);
+    SWR_CUDA(cudaGetLastError());
+    // the shading and traversal kernels read the first pixel from the control block, so their
+    // arguments (and a graph made of them) are the same for every chunk
+    Frame FR = Fh;
+    FR.pixel0 = 0;
+    FR.npix = 0;
+    const unsigned sgrid = (capw + block - 1) / block;
+    std::vector<char> key(sizeof(DevScene) + sizeof(Frame) + sizeof(Qh) + 5 * sizeof(void*));
+    {
+      char* kp = key.data();
+      std::memset(kp, 0, key.size());
+      std::memcpy(kp, &s->dev, sizeof(DevScene));
+      std::memcpy(kp + sizeof(DevScene), &FR, sizeof(Frame));
+      std::memcpy(kp + sizeof(DevScene) + sizeof(Frame), Qh, sizeof(Qh));
+      const void* extra[5] = {ctrl, (void*)trace_kernel, (void*)(uintptr_t)block, (void*)(uintptr_t)trace_grid,
+                              (void*)(uintptr_t)sgrid};
+      std::memcpy(kp + sizeof(DevScene) + sizeof(Frame) + sizeof(Qh), extra, sizeof(extra));
+    }
+    int grc = round_loop_graph(ws->graph[h], ws->graph_key[h], key, ctrl, [&](cudaStream_t cs) {
+      for (int c = 0; c < 8; ++c) {
+        const int q = c & 1;
+        switch (block) {
+          case 128: k_shade<128><<<sgrid, 128, 0, cs>>>(s->dev, FR, ctrl, Qh[q], Qh[q ^ 1], q); break;
+          case 512: k_shade<512><<<sgrid, 512, 0, cs>>>(s->dev, FR, ctrl, Qh[q], Qh[q ^ 1], q); break;
+          default: k_shade<256><<<sgrid, 256, 0, cs>>>(s->dev, FR, ctrl, Qh[q], Qh[q ^ 1], q); break;
+        }
+        trace_kernel<<<trace_grid, kTraceBlock, 0, cs>>>(s->dev, FR, ctrl, Qh[q ^ 1], q);
+      }
+    });
+    if (grc) return grc;
+    SWR_CUDA(cudaGraphLaunch(ws->graph[h], st));
+    SWR_CUDA(cudaGetLastError());
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(Fh, img);
+    SWR_CUDA(cudaGetLastError());
+    SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl + h, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    P.d2h_bytes += sizeof(Ctrl);
+    return SWR_OK;
+  };
+  // what a drained sub-wavefront reports
+  auto collect = [&](const Ctrl& hc) -> int {
+    if (hc.status) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
+    P.rays += hc.rays;
+    P.bounce_rays += hc.bounce_rays;
+    if (P.first_trace_rays == 0) P.first_trace_rays = hc.first_n;
+    P.node_visits += hc.nodes;
+    P.tri_tests += hc.tris;
+    P.iterations += hc.rounds;
+    P.launches += 2 + 2 * hc.rounds + hc.rounds / 8;  // camera, resolve, rounds, checks
+    P.trace_launches += hc.rounds;
+    return SWR_OK;
+  };
+
   for (uint64_t q0 = 0; q0 < npix_total; q0 += px_per_chunk) {
     const uint32_t np = (uint32_t)std::min<uint64_t>(px_per_chunk, npix_total - q0);
     const uint64_t p0 = part.pixel0 + q0;  // image pixel of the chunk's first pixel
     F.pixel0 = (uint32_t)p0;
     F.npix = np;
     const uint64_t total = (uint64_t)np * o->spp;
-    // every path ends within max_depth rounds of its injection and each round injects up to the
-    // queue capacity, so this many rounds always suffice; more means a logic error
-    const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
-    Ctrl init;
-    std::memset(&init, 0, sizeof(init));
-    init.total = total;
-    init.inj_base[0] = 0;
-    init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, total);
-    init.injected = init.inj_n[0];
-    init.pixel0 = (uint32_t)p0;
-    init.max_rounds = max_rounds;
-    SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
-    *ws->host_ctrl = init;
-    SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
-    P.h2d_bytes += sizeof(Ctrl);
-    SWR_CUDA(timer.begin(stream, kTimeCamera));
-    k_camera<<<camera_grid(s, np), kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
-    SWR_CUDA(timer.end(stream));
-    SWR_CUDA(cudaGetLastError());
-    P.launches++;
-    // the shading and traversal kernels read the chunk's first pixel from the control block, so
-    // their arguments (and a graph made of them) are the same for every chunk
-    Frame FR = F;
-    FR.pixel0 = 0;
-    FR.npix = 0;
-    auto round = [&](cudaStream_t st, int p) {
-      switch (block) {
-        case 128: k_shade<128><<<shade_grid, 128, 0, st>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
-        case 512: k_shade<512><<<shade_grid, 512, 0, st>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
-        default: k_shade<256><<<shade_grid, 256, 0, st>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
-      }
-    };
+    SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control blocks may still be in flight
     if (!timer.on) {
-      // the round loop on the device: one graph launch (a WHILE node over eight rounds and
-      // k_round_check), one look at the control block when it has drained
-      std::vector<char> key(sizeof(DevScene) + sizeof(Frame) + sizeof(Q) + 5 * sizeof(void*));
-      {
-        char* kp = key.data();
-        std::memset(kp, 0, key.size());
-        std::memcpy(kp, &s->dev, sizeof(DevScene));
-        std::memcpy(kp + sizeof(DevScene), &FR, sizeof(Frame));
-        std::memcpy(kp + sizeof(DevScene) + sizeof(Frame), Q, sizeof(Q));
-        const void* extra[5] = {ws->ctrl, (void*)trace_kernel, (void*)(uintptr_t)block, (void*)(uintptr_t)trace_grid,
-                                (void*)(uintptr_t)shade_grid};
-        std::memcpy(kp + sizeof(DevScene) + sizeof(Frame) + sizeof(Q), extra, sizeof(extra));
-      }
-      int grc = round_loop_graph(ws, key, ws->ctrl, [&](cudaStream_t st) {
-        for (int c = 0; c < 8; ++c) {
-          const int p = c & 1;
-          round(st, p);
-          trace_kernel<<<trace_grid, kTraceBlock, 0, st>>>(s->dev, FR, ws->ctrl, Q[p ^ 1], p);
+      // Large chunks run as two sub-wavefronts (half the pixels and half the paths in flight
+      // each) on two streams: when one's traversal launch runs out of rays and its SMs idle while
+      // the last rays finish, the other's kernels fill them. Per-pixel results do not depend on it.
+      const bool two = !(o->flags & SWR_RENDER_ONE_WAVEFRONT) && total >= kTwoWaveSamples && np >= 2 &&
+                       cap >= 512;
+      if (two) {
+        if (!ws->side) {
+          SWR_CUDA(cudaStreamCreateWithFlags(&ws->side, cudaStreamNonBlocking));
+          SWR_CUDA(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));
+          SWR_CUDA(cudaEventCreateWithFlags(&ws->join, cudaEventDisableTiming));
         }
-      });
-      if (grc) return grc;
-      SWR_CUDA(cudaGraphLaunch(ws->graph, stream));
-      SWR_CUDA(cudaGetLastError());
-      SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl, ws->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
-      P.d2h_bytes += sizeof(Ctrl);
-      SWR_CUDA(cudaStreamSynchronize(stream));
-      const Ctrl& h = *ws->host_ctrl;
-      if (h.status) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
-      P.rays += h.rays;
-      P.bounce_rays += h.bounce_rays;
-      if (P.first_trace_rays == 0) P.first_trace_rays = h.first_n;
-      P.node_visits += h.nodes;
-      P.tri_tests += h.tris;
-      P.iterations += h.rounds;
-      P.launches += 2 * h.rounds + h.rounds / 8;
-      P.trace_launches += h.rounds;
+        const uint32_t capw = (cap / 2) & ~255u;
+        const uint32_t n0 = np / 2;
+        SWR_CUDA(cudaEventRecord(ws->fork, stream));
+        SWR_CUDA(cudaStreamWaitEvent(ws->side, ws->fork, 0));
+        if ((rc = launch_wave(0, stream, p0, 0, n0, capw))) return rc;
+        if ((rc = launch_wave(1, ws->side, p0, n0, np - n0, capw))) return rc;
+        SWR_CUDA(cudaEventRecord(ws->join, ws->side));
+        SWR_CUDA(cudaStreamWaitEvent(stream, ws->join, 0));
+        SWR_CUDA(cudaStreamSynchronize(stream));
+        if ((rc = collect(ws->host_ctrl[0])) || (rc = collect(ws->host_ctrl[1]))) return rc;
+      } else {
+        if ((rc = launch_wave(0, stream, p0, 0, np, cap))) return rc;
+        SWR_CUDA(cudaStreamSynchronize(stream));
+        if ((rc = collect(ws->host_ctrl[0]))) return rc;
+      }
     } else {
-      // profiled: the host runs the loop so that every launch has its CUDA events
+      // profiled: one wavefront whose loop the host runs, so that every launch has its CUDA events
+      const uint64_t max_rounds = (total / cap + 2) * (uint64_t)(o->max_depth + 2) + 64;
+      Ctrl init;
+      std::memset(&init, 0, sizeof(init));
+      init.total = total;
+      init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, total);
+      init.injected = init.inj_n[0];
+      init.pixel0 = (uint32_t)p0;
+      init.max_rounds = max_rounds;
+      *ws->host_ctrl = init;
+      SWR_CUDA(cudaMemcpyAsync(ws->ctrl, ws->host_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+      P.h2d_bytes += sizeof(Ctrl);
+      SWR_CUDA(timer.begin(stream, kTimeCamera));
+      k_camera<<<camera_grid(s, np), kTraceBlock, 0, stream>>>(s->dev, F, ws->ctrl);
+      SWR_CUDA(timer.end(stream));
+      SWR_CUDA(cudaGetLastError());
+      P.launches++;
+      Frame FR = F;
+      FR.pixel0 = 0;
+      FR.npix = 0;
       uint64_t k = 0;
       for (;;) {
         if (k > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: wavefront did not drain");
@@ -1182,7 +1253,11 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
         for (int c = 0; c < kChunk; ++c, ++k) {
           const int p = (int)(k & 1);
           SWR_CUDA(timer.begin(stream, kTimeShade));
-          round(stream, p);
+          switch (block) {
+            case 128: k_shade<128><<<shade_grid, 128, 0, stream>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+            case 512: k_shade<512><<<shade_grid, 512, 0, stream>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+            default: k_shade<256><<<shade_grid, 256, 0, stream>>>(s->dev, FR, ws->ctrl, Q[p], Q[p ^ 1], p); break;
+          }
           SWR_CUDA(timer.end(stream));
           SWR_CUDA(timer.begin(stream, kTimeTrace));
           trace_kernel<<<trace_grid, kTraceBlock, 0, stream>>>(s->dev, FR, ws->ctrl, Q[p ^ 1], p);
@@ -1207,12 +1282,12 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
           break;
         }
       }
+      SWR_CUDA(timer.begin(stream, kTimeResolve));
+      k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
+      SWR_CUDA(timer.end(stream));
+      SWR_CUDA(cudaGetLastError());
+      P.launches++;
     }
-    SWR_CUDA(timer.begin(stream, kTimeResolve));
-    k_resolve<<<(np + 255) / 256, 256, 0, stream>>>(F, img);
-    SWR_CUDA(timer.end(stream));
-    SWR_CUDA(cudaGetLastError());
-    P.launches++;
     if (want_samples) {
       const size_t bytes = (size_t)np * o->spp * sizeof(float4);
       SWR_CUDA(cudaMemcpyAsync(samples_out + (size_t)q0 * o->spp * 4, F.contrib, bytes,
@@ -1250,7 +1325,11 @@ void free_workspace(swr_scene* s) {
   if (ws->bd_head) cudaFree(ws->bd_head);
   if (ws->ctrl) cudaFree(ws->ctrl);
   if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
-  if (ws->graph) cudaGraphExecDestroy(ws->graph);
+  for (int h = 0; h < 2; ++h)
+    if (ws->graph[h]) cudaGraphExecDestroy(ws->graph[h]);
+  if (ws->side) cudaStreamDestroy(ws->side);
+  if (ws->fork) cudaEventDestroy(ws->fork);
+  if (ws->join) cudaEventDestroy(ws->join);
   delete ws;
   s->workspace = nullptr;
 }
@@ -1281,8 +1360,8 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if (!ws->ctrl) {
-    SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
-    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
+    SWR_CUDA(cudaMalloc(&ws->ctrl, 2 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 2 * sizeof(Ctrl)));
   }
   SWR_CUDA(cudaMemsetAsync(g_alb, 0, (size_t)s->dev.num_tris * 3 * sizeof(float), stream));
   SWR_CUDA(cudaMemsetAsync(g_em, 0, (size_t)s->dev.num_objects * 3 * sizeof(float), stream));
@@ -1385,8 +1464,8 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   if ((rc = ensure(&ws->bd_vtx, ws->bd_vtx_n, px_per_chunk * o->spp * 3 * slots, sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->bd_head, ws->bd_head_n, px_per_chunk * o->spp, sizeof(uint4)))) return rc;
   if (!ws->ctrl) {
-    SWR_CUDA(cudaMalloc(&ws->ctrl, sizeof(Ctrl)));
-    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, sizeof(Ctrl)));
+    SWR_CUDA(cudaMalloc(&ws->ctrl, 2 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 2 * sizeof(Ctrl)));
   }
   float* img = rgb_out;
   const bool host_img = is_host_pointer(rgb_out);

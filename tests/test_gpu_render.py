@@ -105,3 +105,32 @@ def test_gpu_converged_image_within_statistical_error_of_fp64(tmp_path):
     assert 0.6 < float(np.mean(z ** 2)) < 1.5, float(np.mean(z ** 2))
     assert float(np.mean(np.abs(z) > 4.5)) < 2e-3
     assert np.all(np.abs(g - m64)[~live] < 1e-6)
+
+
+def test_two_subwavefronts_equal_one_wavefront(tmp_path):
+    """A chunk of 2^20 samples or more runs as two concurrent sub-wavefronts on two streams; the
+    image and every sample equal those of a single wavefront (SWR_RENDER_ONE_WAVEFRONT)."""
+    s = scenes.cornell(9, str(tmp_path))
+    sd = swr.load_scene(s["scene"], s["basepath"])
+    sc = swr.Scene(sd)
+    W, H, spp, depth = 200, 150, 40, 5  # 1.2 M samples
+    cam = swr.load_camera(s["camera"], W, H)
+    import ctypes
+    from master_thesis_b200 import _native as N
+    outs = []
+    for flags in (0, N.RENDER_ONE_WAVEFRONT):
+        out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+        smp = torch.empty((H * W, spp, 4), dtype=torch.float32, device="cuda")
+        o = N.RenderOpts(W, H, spp, depth, 5, 0, 0, 1.0, 1 << 16, 0, flags | N.RENDER_SAMPLES_OUT, 0, 0, 0)
+        N.check(N.lib.swr_render(sc.handle, ctypes.byref(cam), ctypes.byref(o), out.data_ptr(), smp.data_ptr(),
+                                 torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        outs.append((out.cpu().numpy(), smp.cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][0].max() > 0
+    # and on a host output buffer, twice in a row (graphs and streams reused)
+    for _ in range(2):
+        host = np.zeros((H, W, 3), np.float32)
+        sc.render(cam, W, H, spp, depth, seed=5, wave_size=1 << 16, out=host)
+        assert np.array_equal(host, outs[0][0])
