@@ -32,8 +32,10 @@ using swrx::mk;
 constexpr uint32_t kDeadSlot = 0xFFFFFFFFu;
 constexpr int kTraceBlock = 128;
 constexpr uint64_t kChunkSamples = 1ull << 27;
-// chunks of at least this many samples run as two concurrent sub-wavefronts (SWR_RENDER_ONE_WAVEFRONT)
+// chunks of at least this many samples run as kSubWaves concurrent sub-wavefronts
+// (SWR_RENDER_ONE_WAVEFRONT)
 constexpr uint64_t kTwoWaveSamples = 1ull << 20;
+constexpr int kSubWaves = 2;
 
 struct Ctrl {
   unsigned int count[2];
@@ -822,12 +824,12 @@ struct Workspace {
   void* stage = nullptr;  // device image for callers that pass a host output buffer
   void* bd_vtx = nullptr;   // bidirectional tracer: per-sample vertex tables
   void* bd_head = nullptr;  // bidirectional tracer: per-sample vertex counts
-  Ctrl* ctrl = nullptr;       // [2] control blocks (the second for a concurrent sub-wavefront)
-  Ctrl* host_ctrl = nullptr;  // [2] pinned copies
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // device-side round loop per sub-wavefront
-  std::vector<char> graph_key[2];
-  cudaStream_t side = nullptr;  // the second sub-wavefront's stream
-  cudaEvent_t fork = nullptr, join = nullptr;
+  Ctrl* ctrl = nullptr;       // [4] control blocks (one per concurrent sub-wavefront)
+  Ctrl* host_ctrl = nullptr;  // [4] pinned copies
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // round loop per sub-wavefront
+  std::vector<char> graph_key[4];
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};  // streams of sub-wavefronts 1..3
+  cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
 
 // End of one iteration of the device-side round loop (eight shade/trace rounds, after which the
@@ -1028,8 +1030,8 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->contrib, ws->contrib_n, px_per_chunk * o->spp, sizeof(float4)))) return rc;
   if (!ws->ctrl) {
-    SWR_CUDA(cudaMalloc(&ws->ctrl, 2 * sizeof(Ctrl)));
-    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 2 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMalloc(&ws->ctrl, 4 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 4 * sizeof(Ctrl)));
   }
 
   Queue Q[2];
@@ -1199,27 +1201,33 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     const uint64_t total = (uint64_t)np * o->spp;
     SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control blocks may still be in flight
     if (!timer.on) {
-      // Large chunks run as two sub-wavefronts (half the pixels and half the paths in flight
-      // each) on two streams: when one's traversal launch runs out of rays and its SMs idle while
-      // the last rays finish, the other's kernels fill them. Per-pixel results do not depend on it.
-      const bool two = !(o->flags & SWR_RENDER_ONE_WAVEFRONT) && total >= kTwoWaveSamples && np >= 2 &&
-                       cap >= 512;
-      if (two) {
-        if (!ws->side) {
-          SWR_CUDA(cudaStreamCreateWithFlags(&ws->side, cudaStreamNonBlocking));
+      // Large chunks run as kSubWaves sub-wavefronts (a share of the pixels and of the paths in
+      // flight each) on as many streams: when one's traversal launch runs out of rays and its SMs
+      // idle while the last rays finish, the others' kernels fill them. Per-pixel results do not
+      // depend on it.
+      const int nsub = (!(o->flags & SWR_RENDER_ONE_WAVEFRONT) && total >= kTwoWaveSamples &&
+                        np >= (uint32_t)kSubWaves && cap >= 256u * kSubWaves) ? kSubWaves : 1;
+      if (nsub > 1) {
+        if (!ws->fork) {
           SWR_CUDA(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));
-          SWR_CUDA(cudaEventCreateWithFlags(&ws->join, cudaEventDisableTiming));
+          for (int h = 0; h < 3; ++h) {
+            SWR_CUDA(cudaStreamCreateWithFlags(&ws->side[h], cudaStreamNonBlocking));
+            SWR_CUDA(cudaEventCreateWithFlags(&ws->join[h], cudaEventDisableTiming));
+          }
         }
-        const uint32_t capw = (cap / 2) & ~255u;
-        const uint32_t n0 = np / 2;
+        const uint32_t capw = (cap / nsub) & ~255u;
         SWR_CUDA(cudaEventRecord(ws->fork, stream));
-        SWR_CUDA(cudaStreamWaitEvent(ws->side, ws->fork, 0));
-        if ((rc = launch_wave(0, stream, p0, 0, n0, capw))) return rc;
-        if ((rc = launch_wave(1, ws->side, p0, n0, np - n0, capw))) return rc;
-        SWR_CUDA(cudaEventRecord(ws->join, ws->side));
-        SWR_CUDA(cudaStreamWaitEvent(stream, ws->join, 0));
+        for (int h = 0; h < nsub; ++h) {
+          const uint64_t a = (uint64_t)np * h / nsub, b = (uint64_t)np * (h + 1) / nsub;
+          cudaStream_t st = h ? ws->side[h - 1] : stream;
+          if (h) SWR_CUDA(cudaStreamWaitEvent(st, ws->fork, 0));
+          if ((rc = launch_wave(h, st, p0, a, (uint32_t)(b - a), capw))) return rc;
+          if (h) SWR_CUDA(cudaEventRecord(ws->join[h - 1], st));
+        }
+        for (int h = 1; h < nsub; ++h) SWR_CUDA(cudaStreamWaitEvent(stream, ws->join[h - 1], 0));
         SWR_CUDA(cudaStreamSynchronize(stream));
-        if ((rc = collect(ws->host_ctrl[0])) || (rc = collect(ws->host_ctrl[1]))) return rc;
+        for (int h = 0; h < nsub; ++h)
+          if ((rc = collect(ws->host_ctrl[h]))) return rc;
       } else {
         if ((rc = launch_wave(0, stream, p0, 0, np, cap))) return rc;
         SWR_CUDA(cudaStreamSynchronize(stream));
@@ -1325,11 +1333,13 @@ void free_workspace(swr_scene* s) {
   if (ws->bd_head) cudaFree(ws->bd_head);
   if (ws->ctrl) cudaFree(ws->ctrl);
   if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
-  for (int h = 0; h < 2; ++h)
+  for (int h = 0; h < 4; ++h)
     if (ws->graph[h]) cudaGraphExecDestroy(ws->graph[h]);
-  if (ws->side) cudaStreamDestroy(ws->side);
+  for (int h = 0; h < 3; ++h) {
+    if (ws->side[h]) cudaStreamDestroy(ws->side[h]);
+    if (ws->join[h]) cudaEventDestroy(ws->join[h]);
+  }
   if (ws->fork) cudaEventDestroy(ws->fork);
-  if (ws->join) cudaEventDestroy(ws->join);
   delete ws;
   s->workspace = nullptr;
 }
@@ -1360,8 +1370,8 @@ int render_adjoint_impl(swr_scene* s, const swr_camera* cam, const swr_render_op
   const uint64_t px_per_chunk = std::max<uint64_t>(1, std::min<uint64_t>(npix_total, kChunkSamples / o->spp));
   if ((rc = ensure(&ws->cam, ws->cam_px, px_per_chunk, 2 * sizeof(float4)))) return rc;
   if (!ws->ctrl) {
-    SWR_CUDA(cudaMalloc(&ws->ctrl, 2 * sizeof(Ctrl)));
-    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 2 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMalloc(&ws->ctrl, 4 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 4 * sizeof(Ctrl)));
   }
   SWR_CUDA(cudaMemsetAsync(g_alb, 0, (size_t)s->dev.num_tris * 3 * sizeof(float), stream));
   SWR_CUDA(cudaMemsetAsync(g_em, 0, (size_t)s->dev.num_objects * 3 * sizeof(float), stream));
@@ -1464,8 +1474,8 @@ int render_bdpt_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts*
   if ((rc = ensure(&ws->bd_vtx, ws->bd_vtx_n, px_per_chunk * o->spp * 3 * slots, sizeof(float4)))) return rc;
   if ((rc = ensure(&ws->bd_head, ws->bd_head_n, px_per_chunk * o->spp, sizeof(uint4)))) return rc;
   if (!ws->ctrl) {
-    SWR_CUDA(cudaMalloc(&ws->ctrl, 2 * sizeof(Ctrl)));
-    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 2 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMalloc(&ws->ctrl, 4 * sizeof(Ctrl)));
+    SWR_CUDA(cudaMallocHost(&ws->host_ctrl, 4 * sizeof(Ctrl)));
   }
   float* img = rgb_out;
   const bool host_img = is_host_pointer(rgb_out);
