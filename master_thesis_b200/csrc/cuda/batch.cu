@@ -30,6 +30,9 @@ using swrx::mk;
 constexpr uint32_t kDead = 0xFFFFFFFFu;
 constexpr int kTB = 128;
 constexpr double kFix = 4294967296.0;  // 2^32
+// batches of at least this many samples run as kBatchSubWaves concurrent sub-wavefronts
+constexpr uint64_t kBatchTwoWaveSamples = 1ull << 20;
+constexpr int kBatchSubWaves = 2;
 
 struct BJob {
   float vi[16], pi[16];
@@ -426,9 +429,11 @@ int ensure_bytes(void** p, size_t& have, size_t want) {
 struct swr_batch {
   void *qbuf = nullptr, *cam = nullptr, *accum = nullptr, *jobs = nullptr, *scenes = nullptr, *ctrl = nullptr;
   size_t qbytes = 0, cambytes = 0, accbytes = 0, jobbytes = 0, scenebytes = 0, ctrlbytes = 0;
-  swr::BCtrl* host_ctrl = nullptr;
-  cudaGraphExec_t graph = nullptr;
-  std::vector<char> graph_key;
+  swr::BCtrl* host_ctrl = nullptr;                                  // [4] pinned control blocks
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // round loop per sub-wavefront
+  std::vector<char> graph_key[4];
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};  // streams of sub-wavefronts 1..3
+  cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
   int device = -1;
 };
 
@@ -487,14 +492,20 @@ int swr_batch_create(swr_batch** out) {
   if (!out) return set_error(SWR_ERR_INVALID, "swr: null output handle");
   std::unique_ptr<swr_batch> b(new swr_batch());
   SWR_CUDA(cudaGetDevice(&b->device));
-  SWR_CUDA(cudaMallocHost(&b->host_ctrl, sizeof(swr::BCtrl)));
+  SWR_CUDA(cudaMallocHost(&b->host_ctrl, 4 * sizeof(swr::BCtrl)));
   *out = b.release();
   return SWR_OK;
 }
 
 void swr_batch_destroy(swr_batch* b) {
   if (!b) return;
-  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (int h = 0; h < 4; ++h)
+    if (b->graph[h]) cudaGraphExecDestroy(b->graph[h]);
+  for (int h = 0; h < 3; ++h) {
+    if (b->side[h]) cudaStreamDestroy(b->side[h]);
+    if (b->join[h]) cudaEventDestroy(b->join[h]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   for (void* p : {b->qbuf, b->cam, b->accum, b->jobs, b->scenes, b->ctrl})
     if (p) cudaFree(p);
   if (b->host_ctrl) cudaFreeHost(b->host_ctrl);
@@ -532,21 +543,10 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
   if ((rc = ensure_bytes(&b->accum, b->accbytes, pixels * 3 * sizeof(unsigned long long)))) return rc;
   if ((rc = ensure_bytes(&b->jobs, b->jobbytes, n * sizeof(BJob)))) return rc;
   if ((rc = ensure_bytes(&b->scenes, b->scenebytes, hs.size() * sizeof(DevScene)))) return rc;
-  if ((rc = ensure_bytes(&b->ctrl, b->ctrlbytes, sizeof(BCtrl)))) return rc;
+  if ((rc = ensure_bytes(&b->ctrl, b->ctrlbytes, 4 * sizeof(BCtrl)))) return rc;
   SWR_CUDA(cudaMemcpyAsync(b->jobs, hj.data(), n * sizeof(BJob), cudaMemcpyHostToDevice, stream));
   SWR_CUDA(cudaMemcpyAsync(b->scenes, hs.data(), hs.size() * sizeof(DevScene), cudaMemcpyHostToDevice, stream));
   SWR_CUDA(cudaMemsetAsync(b->accum, 0, pixels * 3 * sizeof(unsigned long long), stream));
-  BQueue Q[2];
-  {
-    char* p = (char*)b->qbuf;
-    for (int k = 0; k < 2; ++k) {
-      Q[k].o = (float4*)p; p += (size_t)cap * sizeof(float4);
-      Q[k].d = (float4*)p; p += (size_t)cap * sizeof(float4);
-      Q[k].c = (float4*)p; p += (size_t)cap * sizeof(float4);
-      Q[k].l = (float4*)p; p += (size_t)cap * sizeof(float4);
-      Q[k].hit = (uint2*)p; p += (size_t)cap * sizeof(uint2);
-    }
-  }
   // zero-filled first: the struct's bytes, padding included, are the graph cache's key
   BArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -560,92 +560,131 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
   A.accum = (unsigned long long*)b->accum;
   uint32_t maxdepth = 0;
   for (uint32_t k = 0; k < n; ++k) maxdepth = std::max(maxdepth, jobs[k].opts.max_depth);
-  // every path ends within max_depth rounds of its injection and each round injects up to the
-  // queue capacity, so this many rounds always suffice; more means a logic error
-  const uint64_t max_rounds = (samples / cap + 2) * (uint64_t)(maxdepth + 2) + 64;
-  BCtrl init;
-  std::memset(&init, 0, sizeof(init));
-  init.total = samples;
-  init.inj_n[0] = (unsigned)std::min<uint64_t>(cap, samples);
-  init.injected = init.inj_n[0];
-  init.max_rounds = max_rounds;
-  SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
-  *b->host_ctrl = init;
-  SWR_CUDA(cudaMemcpyAsync(b->ctrl, b->host_ctrl, sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
-  k_bcamera<<<(unsigned)((pixels + kTB - 1) / kTB), kTB, 0, stream>>>(A, (BCtrl*)b->ctrl);
+  const bool use_graph = !(bo && (bo->flags & SWR_BATCH_NO_GRAPH));
+  // With the graph, large batches run as kBatchSubWaves sub-wavefronts over consecutive ranges of
+  // the global sample index (a share of the paths in flight each) on as many streams, so that the
+  // SMs one leaves idle at the end of a traversal launch take another's work; the per-pixel sums
+  // are order-independent fixed point, so the images do not depend on it.
+  const int nsub = (use_graph && samples >= kBatchTwoWaveSamples && cap >= 256u * kBatchSubWaves) ? kBatchSubWaves : 1;
+  const uint32_t capw = nsub > 1 ? (cap / nsub) & ~255u : cap;
+  A.capacity = capw;  // each sub-wavefront's queue
+  BCtrl* dctrl = (BCtrl*)b->ctrl;
+  SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control blocks may still be in flight
+  for (int h = 0; h < nsub; ++h) {
+    const uint64_t s0 = samples * h / nsub, s1 = samples * (h + 1) / nsub;
+    BCtrl init;
+    std::memset(&init, 0, sizeof(init));
+    init.total = s1;  // the sub-wavefront's end in the global sample index
+    init.inj_base[0] = s0;
+    init.inj_n[0] = (unsigned)std::min<uint64_t>(capw, s1 - s0);
+    init.injected = s0 + init.inj_n[0];
+    // every path ends within max_depth rounds of its injection and each round injects up to the
+    // queue capacity, so this many rounds always suffice; more means a logic error
+    init.max_rounds = ((s1 - s0) / capw + 2) * (uint64_t)(maxdepth + 2) + 64;
+    b->host_ctrl[h] = init;
+  }
+  SWR_CUDA(cudaMemcpyAsync(dctrl, b->host_ctrl, nsub * sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
+  k_bcamera<<<(unsigned)((pixels + kTB - 1) / kTB), kTB, 0, stream>>>(A, dctrl);
   SWR_CUDA(cudaGetLastError());
   int per_sm = 0;
   SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_btrace, kTB, 0));
   const unsigned tgrid = (unsigned)(num_sms * std::max(per_sm, 1));
-  const unsigned sgrid = (cap + 255) / 256;
-  const bool use_graph = !(bo && (bo->flags & SWR_BATCH_NO_GRAPH));
-  auto enqueue_rounds = [&](cudaStream_t st) {
+  const unsigned sgrid = (capw + 255) / 256;
+  auto queues = [&](int h, BQueue* Qh) {
+    char* p = (char*)b->qbuf + (size_t)h * ((size_t)capw * (4 * sizeof(float4) + sizeof(uint2)) * 2);
+    for (int k = 0; k < 2; ++k) {
+      Qh[k].o = (float4*)p; p += (size_t)capw * sizeof(float4);
+      Qh[k].d = (float4*)p; p += (size_t)capw * sizeof(float4);
+      Qh[k].c = (float4*)p; p += (size_t)capw * sizeof(float4);
+      Qh[k].l = (float4*)p; p += (size_t)capw * sizeof(float4);
+      Qh[k].hit = (uint2*)p; p += (size_t)capw * sizeof(uint2);
+    }
+  };
+  auto enqueue_rounds = [&](cudaStream_t st, BCtrl* ctrl, const BQueue* Qh) {
     for (int k = 0; k < 8; ++k) {
       const int p = k & 1;
-      k_bshade<<<sgrid, 256, 0, st>>>(A, (BCtrl*)b->ctrl, Q[p], Q[p ^ 1], p);
-      k_btrace<<<tgrid, kTB, 0, st>>>(A, (BCtrl*)b->ctrl, Q[p ^ 1], p);
+      k_bshade<<<sgrid, 256, 0, st>>>(A, ctrl, Qh[p], Qh[p ^ 1], p);
+      k_btrace<<<tgrid, kTB, 0, st>>>(A, ctrl, Qh[p ^ 1], p);
     }
   };
   if (use_graph) {
-    // the whole round loop as one graph (a WHILE node over eight rounds and k_bcheck), rebuilt
-    // whenever an argument baked into it changes
-    std::vector<char> key(sizeof(A) + sizeof(Q) + 3 * sizeof(void*));
-    {
-      char* k = key.data();
-      std::memset(k, 0, key.size());
-      std::memcpy(k, &A, sizeof(A));
-      std::memcpy(k + sizeof(A), Q, sizeof(Q));
-      const void* extra[3] = {b->ctrl, (void*)(uintptr_t)sgrid, (void*)(uintptr_t)tgrid};
-      std::memcpy(k + sizeof(A) + sizeof(Q), extra, sizeof(extra));
-    }
-    if (!b->graph || key != b->graph_key) {
-      if (b->graph) cudaGraphExecDestroy(b->graph);
-      b->graph = nullptr;
-      b->graph_key.clear();
-      cudaGraph_t g = nullptr;
-      cudaStream_t cs = nullptr;
-      auto build = [&]() -> int {
-        SWR_CUDA(cudaGraphCreate(&g, 0));
-        cudaGraphConditionalHandle loop;
-        SWR_CUDA(cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault));
-        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = loop;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        SWR_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        SWR_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        SWR_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        enqueue_rounds(cs);
-        k_bcheck<<<1, 1, 0, cs>>>((BCtrl*)b->ctrl, loop);
-        cudaGraph_t captured = nullptr;
-        SWR_CUDA(cudaStreamEndCapture(cs, &captured));
-        SWR_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
-        return SWR_OK;
-      };
-      const int brc = build();
-      if (cs) cudaStreamDestroy(cs);
-      if (g) cudaGraphDestroy(g);
-      if (brc) {
-        if (b->graph) cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-        return brc;
+    if (nsub > 1 && !b->fork) {
+      SWR_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+      for (int h = 0; h < 3; ++h) {
+        SWR_CUDA(cudaStreamCreateWithFlags(&b->side[h], cudaStreamNonBlocking));
+        SWR_CUDA(cudaEventCreateWithFlags(&b->join[h], cudaEventDisableTiming));
       }
-      b->graph_key = key;
     }
-    SWR_CUDA(cudaGraphLaunch(b->graph, stream));
-    SWR_CUDA(cudaGetLastError());
+    if (nsub > 1) SWR_CUDA(cudaEventRecord(b->fork, stream));
+    for (int h = 0; h < nsub; ++h) {
+      BQueue Qh[2];
+      queues(h, Qh);
+      BCtrl* ctrl = dctrl + h;
+      // the whole round loop as one graph (a WHILE node over eight rounds and k_bcheck), rebuilt
+      // whenever an argument baked into it changes
+      std::vector<char> key(sizeof(A) + sizeof(Qh) + 3 * sizeof(void*));
+      {
+        char* k = key.data();
+        std::memset(k, 0, key.size());
+        std::memcpy(k, &A, sizeof(A));
+        std::memcpy(k + sizeof(A), Qh, sizeof(Qh));
+        const void* extra[3] = {ctrl, (void*)(uintptr_t)sgrid, (void*)(uintptr_t)tgrid};
+        std::memcpy(k + sizeof(A) + sizeof(Qh), extra, sizeof(extra));
+      }
+      if (!b->graph[h] || key != b->graph_key[h]) {
+        if (b->graph[h]) cudaGraphExecDestroy(b->graph[h]);
+        b->graph[h] = nullptr;
+        b->graph_key[h].clear();
+        cudaGraph_t g = nullptr;
+        cudaStream_t cs = nullptr;
+        auto build = [&]() -> int {
+          SWR_CUDA(cudaGraphCreate(&g, 0));
+          cudaGraphConditionalHandle loop;
+          SWR_CUDA(cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault));
+          cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+          cp.conditional.handle = loop;
+          cp.conditional.type = cudaGraphCondTypeWhile;
+          cp.conditional.size = 1;
+          cudaGraphNode_t node;
+          SWR_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+          SWR_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+          SWR_CUDA(cudaStreamBeginCaptureToGraph(cs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal));
+          enqueue_rounds(cs, ctrl, Qh);
+          k_bcheck<<<1, 1, 0, cs>>>(ctrl, loop);
+          cudaGraph_t captured = nullptr;
+          SWR_CUDA(cudaStreamEndCapture(cs, &captured));
+          SWR_CUDA(cudaGraphInstantiate(&b->graph[h], g, 0));
+          return SWR_OK;
+        };
+        const int brc = build();
+        if (cs) cudaStreamDestroy(cs);
+        if (g) cudaGraphDestroy(g);
+        if (brc) {
+          if (b->graph[h]) cudaGraphExecDestroy(b->graph[h]);
+          b->graph[h] = nullptr;
+          return brc;
+        }
+        b->graph_key[h] = key;
+      }
+      cudaStream_t st = h ? b->side[h - 1] : stream;
+      if (h) SWR_CUDA(cudaStreamWaitEvent(st, b->fork, 0));
+      SWR_CUDA(cudaGraphLaunch(b->graph[h], st));
+      SWR_CUDA(cudaGetLastError());
+      if (h) SWR_CUDA(cudaEventRecord(b->join[h - 1], st));
+    }
+    for (int h = 1; h < nsub; ++h) SWR_CUDA(cudaStreamWaitEvent(stream, b->join[h - 1], 0));
   } else {
     // without a graph the host runs the loop: eight rounds, then a look at the control block
+    BQueue Q0[2];
+    queues(0, Q0);
     uint64_t rounds = 0;
     for (;;) {
-      if (rounds > max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
-      enqueue_rounds(stream);
+      if (rounds > b->host_ctrl[0].max_rounds) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
+      enqueue_rounds(stream, dctrl, Q0);
       rounds += 8;
       SWR_CUDA(cudaGetLastError());
-      SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, b->ctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
+      SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, dctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
       SWR_CUDA(cudaStreamSynchronize(stream));
       const BCtrl& h = *b->host_ctrl;
       // after an even number of rounds the next shade reads parity 0
@@ -655,10 +694,11 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
   k_bresolve<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(A);
   SWR_CUDA(cudaGetLastError());
   if (use_graph) {
-    // the one wait of the call: the device-side loop's status
-    SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, b->ctrl, sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
+    // the one wait of the call: the device-side loops' status
+    SWR_CUDA(cudaMemcpyAsync(b->host_ctrl, dctrl, nsub * sizeof(BCtrl), cudaMemcpyDeviceToHost, stream));
     SWR_CUDA(cudaStreamSynchronize(stream));
-    if (b->host_ctrl->status) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
+    for (int h = 0; h < nsub; ++h)
+      if (b->host_ctrl[h].status) return set_error(SWR_ERR_TIMEOUT, "swr: batch wavefront did not drain");
   }
   return SWR_OK;
 }
@@ -713,7 +753,7 @@ int swr_render_adjoint_batch(swr_batch* b, const swr_adjoint_job* jobs, uint32_t
   if ((rc = ensure_bytes(&b->cam, b->cambytes, pixels * 2 * sizeof(float4)))) return rc;
   if ((rc = ensure_bytes(&b->jobs, b->jobbytes, n * sizeof(BJob)))) return rc;
   if ((rc = ensure_bytes(&b->scenes, b->scenebytes, hs.size() * sizeof(DevScene)))) return rc;
-  if ((rc = ensure_bytes(&b->ctrl, b->ctrlbytes, sizeof(BCtrl)))) return rc;
+  if ((rc = ensure_bytes(&b->ctrl, b->ctrlbytes, 4 * sizeof(BCtrl)))) return rc;
   SWR_CUDA(cudaMemcpyAsync(b->jobs, hj.data(), n * sizeof(BJob), cudaMemcpyHostToDevice, stream));
   SWR_CUDA(cudaMemcpyAsync(b->scenes, hs.data(), hs.size() * sizeof(DevScene), cudaMemcpyHostToDevice, stream));
   for (auto& z : zero) SWR_CUDA(cudaMemsetAsync(z.first, 0, z.second, stream));
