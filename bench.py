@@ -889,6 +889,19 @@ def main():
     torch.cuda.synchronize()
     t4 = time.time()
     cam = swr.load_camera(files["camera"], W, H)
+    # launch shape: the configuration's paths in flight, or with --tune the autotuner's tree
+    # (BVH width, leaf size; the scene is rebuilt with it) and launch shape (cached per workload)
+    shape = {"wave_size": cfg.get("wave_size", 0)}
+    tuned = None
+    if args.tune:
+        from master_thesis_b200 import autotune
+        bo = autotune.tune_build(sd, cam, W, H, spp, depth)
+        scene.close()
+        scene = swr.Scene(sd, **bo)
+        torch.cuda.synchronize()
+        stats = scene.stats()
+        shape = autotune.tune_render(scene, cam, W, H, spp, depth)
+        tuned = {"build": bo, "launch": shape}
     # images: every rank renders its own image (seed 1000 + rank); spp / tiles: all ranks render
     # one image (seed 1000) split by sample range or pixel tile (sharding.render_split)
     split = args.split  # with one GPU a split renders the whole image as its one part
@@ -902,13 +915,12 @@ def main():
     def render(o, **kw):
         if split == "images":
             return scene.render(cam, W, H, spp, depth, seed=seed, out=o, stream=stream, return_profile=True,
-                                wave_size=cfg.get("wave_size", 0), **kw)
+                                **shape, **kw)
         profile = []
 
         def part(pb, pc, sb, sc):
             r, pr = scene.render(cam, W, H, sc, depth, seed=seed, stream=stream, return_profile=True,
-                                 wave_size=cfg.get("wave_size", 0), pixel_begin=pb, pixel_count=pc, sample_begin=sb,
-                                 spp_total=spp, **kw)
+                                 pixel_begin=pb, pixel_count=pc, sample_begin=sb, spp_total=spp, **shape, **kw)
             profile.append(pr)
             return r.reshape(pc, 3)
 
@@ -1033,6 +1045,7 @@ def main():
             "data": "synthetic (seeded scene files)",
             "config": bench_config(cfg, files, world, workload, split),
             "bvh": {"nodes": stats["nodes"], "depth": stats["depth"]},
+            "tuned": tuned,
             "e2e": {"value": e2e_value, "unit": "Msamples/s",
                     "h2d_bytes_per_step": int(e2e_prof[-1]["h2d_bytes"]),
                     "d2h_bytes_per_step": int(e2e_prof[-1]["d2h_bytes"]),
