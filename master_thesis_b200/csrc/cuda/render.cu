@@ -1175,6 +1175,12 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     SWR_CUDA(cudaGetLastError());
     k_resolve<<<(n + 255) / 256, 256, 0, st>>>(Fh, img);
     SWR_CUDA(cudaGetLastError());
+    if (host_img) {  // this part of a host image goes out while the other sub-wavefronts still run
+      const size_t first = (size_t)(Fh.pixel0 - F.out0) * 3;
+      SWR_CUDA(cudaMemcpyAsync(rgb_out + first, img_dev + first, (size_t)n * 3 * sizeof(float),
+                               cudaMemcpyDeviceToHost, st));
+      P.d2h_bytes += (size_t)n * 3 * sizeof(float);
+    }
     SWR_CUDA(cudaMemcpyAsync(ws->host_ctrl + h, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     P.d2h_bytes += sizeof(Ctrl);
     return SWR_OK;
@@ -1303,7 +1309,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
       if (host_samples) P.d2h_bytes += bytes;
     }
   }
-  if (host_img) {
+  if (host_img && timer.on) {  // the graph path copied each sub-wavefront's part as it finished
     SWR_CUDA(cudaMemcpyAsync(rgb_out, img_dev, npix_total * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream));
     P.d2h_bytes += npix_total * 3 * sizeof(float);
   }
