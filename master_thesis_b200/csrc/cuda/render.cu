@@ -1570,7 +1570,8 @@ constexpr uint32_t kNoAllocCap = 1u << 16;              // paths in flight
 constexpr uint64_t kNoAllocChunkSamples = 1ull << 21;   // samples per chunk
 constexpr uint64_t kNoAllocChunkPixels = 1ull << 18;    // pixels per chunk
 constexpr size_t kNoAllocQueueBytes = (size_t)kNoAllocCap * (4 * sizeof(float4) + sizeof(uint2));
-constexpr size_t kNoAllocCamOffset = 256 + 2 * kNoAllocQueueBytes;
+constexpr size_t kNoAllocCamOffset = 256 + 2 * kNoAllocQueueBytes;  // the control block takes the first 256 bytes
+static_assert(sizeof(Ctrl) <= 256, "the allocation-free render keeps its control block in 256 bytes");
 constexpr size_t kNoAllocContribOffset = kNoAllocCamOffset + kNoAllocChunkPixels * 2 * sizeof(float4);
 static_assert(kNoAllocContribOffset + kNoAllocChunkSamples * sizeof(float4) <= kNoAllocBytes,
               "no-allocation scratch layout exceeds its array");
