@@ -826,8 +826,15 @@ struct Workspace {
   void* bd_head = nullptr;  // bidirectional tracer: per-sample vertex counts
   Ctrl* ctrl = nullptr;       // [4] control blocks (one per concurrent sub-wavefront)
   Ctrl* host_ctrl = nullptr;  // [4] pinned copies
-  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // round loop per sub-wavefront
-  std::vector<char> graph_key[4];
+  // round-loop graphs per sub-wavefront, the last kGraphsKept launch shapes each (a render that
+  // alternates, e.g. counting and plain renders, reuses them instead of rebuilding)
+  struct GraphEntry {
+    std::vector<char> key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t used = 0;
+  };
+  std::vector<GraphEntry> graphs[4];
+  uint64_t graph_clock = 0;
   cudaStream_t side[3] = {nullptr, nullptr, nullptr};  // streams of sub-wavefronts 1..3
   cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
@@ -848,15 +855,22 @@ __global__ void k_round_check(Ctrl* __restrict__ ctrl, cudaGraphConditionalHandl
   cudaGraphSetConditional(loop, go);
 }
 
-// (Re)builds graph: a WHILE node whose body is `rounds` (eight shade/trace rounds, enqueued on
-// the given stream) followed by k_round_check. The key holds every argument baked into it.
+constexpr size_t kGraphsKept = 4;
+
+// The round-loop graph for `key` from the cache (built when missing, evicting the least recently
+// used beyond kGraphsKept): a WHILE node whose body is `rounds` (eight shade/trace rounds, enqueued
+// on the given stream) followed by k_round_check. The key holds every argument baked into it.
 template <class Enqueue>
-int round_loop_graph(cudaGraphExec_t& graph, std::vector<char>& graph_key, const std::vector<char>& key, Ctrl* ctrl,
-                     Enqueue rounds) {
-  if (graph && key == graph_key) return SWR_OK;
-  if (graph) cudaGraphExecDestroy(graph);
-  graph = nullptr;
-  graph_key.clear();
+int round_loop_graph(Workspace* ws, int slot, const std::vector<char>& key, Ctrl* ctrl, Enqueue rounds,
+                     cudaGraphExec_t* out) {
+  auto& cache = ws->graphs[slot];
+  for (auto& e : cache)
+    if (e.key == key) {
+      e.used = ++ws->graph_clock;
+      *out = e.exec;
+      return SWR_OK;
+    }
+  cudaGraphExec_t exec = nullptr;
   cudaGraph_t g = nullptr;
   cudaStream_t cs = nullptr;
   auto build = [&]() -> int {
@@ -876,18 +890,29 @@ int round_loop_graph(cudaGraphExec_t& graph, std::vector<char>& graph_key, const
     k_round_check<<<1, 1, 0, cs>>>(ctrl, loop);
     cudaGraph_t captured = nullptr;
     SWR_CUDA(cudaStreamEndCapture(cs, &captured));
-    SWR_CUDA(cudaGraphInstantiate(&graph, g, 0));
+    SWR_CUDA(cudaGraphInstantiate(&exec, g, 0));
     return SWR_OK;
   };
   const int rc = build();
   if (cs) cudaStreamDestroy(cs);
   if (g) cudaGraphDestroy(g);
   if (rc) {
-    if (graph) cudaGraphExecDestroy(graph);
-    graph = nullptr;
+    if (exec) cudaGraphExecDestroy(exec);
     return rc;
   }
-  graph_key = key;
+  if (cache.size() >= kGraphsKept) {
+    size_t lru = 0;
+    for (size_t i = 1; i < cache.size(); ++i)
+      if (cache[i].used < cache[lru].used) lru = i;
+    cudaGraphExecDestroy(cache[lru].exec);
+    cache.erase(cache.begin() + (long)lru);
+  }
+  Workspace::GraphEntry e;
+  e.key = key;
+  e.exec = exec;
+  e.used = ++ws->graph_clock;
+  cache.push_back(std::move(e));
+  *out = exec;
   return SWR_OK;
 }
 
@@ -1159,7 +1184,8 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
                               (void*)(uintptr_t)sgrid};
       std::memcpy(kp + sizeof(DevScene) + sizeof(Frame) + sizeof(Qh), extra, sizeof(extra));
     }
-    int grc = round_loop_graph(ws->graph[h], ws->graph_key[h], key, ctrl, [&](cudaStream_t cs) {
+    cudaGraphExec_t graph = nullptr;
+    int grc = round_loop_graph(ws, h, key, ctrl, [&](cudaStream_t cs) {
       for (int c = 0; c < 8; ++c) {
         const int q = c & 1;
         switch (block) {
@@ -1169,9 +1195,9 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
         }
         trace_kernel<<<trace_grid, kTraceBlock, 0, cs>>>(s->dev, FR, ctrl, Qh[q ^ 1], q);
       }
-    });
+    }, &graph);
     if (grc) return grc;
-    SWR_CUDA(cudaGraphLaunch(ws->graph[h], st));
+    SWR_CUDA(cudaGraphLaunch(graph, st));
     SWR_CUDA(cudaGetLastError());
     k_resolve<<<(n + 255) / 256, 256, 0, st>>>(Fh, img);
     SWR_CUDA(cudaGetLastError());
@@ -1339,8 +1365,8 @@ void free_workspace(swr_scene* s) {
   if (ws->bd_head) cudaFree(ws->bd_head);
   if (ws->ctrl) cudaFree(ws->ctrl);
   if (ws->host_ctrl) cudaFreeHost(ws->host_ctrl);
-  for (int h = 0; h < 4; ++h)
-    if (ws->graph[h]) cudaGraphExecDestroy(ws->graph[h]);
+  for (auto& cache : ws->graphs)
+    for (auto& e : cache) cudaGraphExecDestroy(e.exec);
   for (int h = 0; h < 3; ++h) {
     if (ws->side[h]) cudaStreamDestroy(ws->side[h]);
     if (ws->join[h]) cudaEventDestroy(ws->join[h]);
