@@ -241,8 +241,8 @@ int swr_render(swr_scene* scene, const swr_camera* cam, const swr_render_opts* o
 #define SWR_RENDER_POSTPONE 16u     /* bounce traversal postpones triangle tests while few lanes of
                                        a warp have any (keeps warps in one phase) */
 #define SWR_RENDER_ONE_WAVEFRONT 32u /* run every chunk as one wavefront on the caller's stream. By
-                                       default a chunk of 2^20 samples or more runs as two
-                                       sub-wavefronts (half the pixels and half the paths in flight
+                                       default a chunk of 2^20 samples or more of a scene of 2^16
+                                       triangles or more runs as two sub-wavefronts (half the pixels and half the paths in flight
                                        each) on the caller's stream and an internal one, so that the
                                        SMs one of them leaves idle at the end of a traversal launch
                                        take the other's work; results are identical either way.

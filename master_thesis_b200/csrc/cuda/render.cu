@@ -32,9 +32,12 @@ using swrx::mk;
 constexpr uint32_t kDeadSlot = 0xFFFFFFFFu;
 constexpr int kTraceBlock = 128;
 constexpr uint64_t kChunkSamples = 1ull << 27;
-// chunks of at least this many samples run as kSubWaves concurrent sub-wavefronts
-// (SWR_RENDER_ONE_WAVEFRONT)
+// chunks of at least this many samples, on scenes of at least kTwoWaveTriangles triangles, run as
+// kSubWaves concurrent sub-wavefronts (SWR_RENDER_ONE_WAVEFRONT). Measured on B200: 28.02 vs 28.49
+// ms for the 2.4 M-triangle terrain image; 1-2 % slower on the 36-triangle Cornell box, whose
+// traversal launches have no long tail to fill.
 constexpr uint64_t kTwoWaveSamples = 1ull << 20;
+constexpr uint32_t kTwoWaveTriangles = 1u << 16;
 constexpr int kSubWaves = 2;
 
 struct Ctrl {
@@ -1233,12 +1236,13 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     const uint64_t total = (uint64_t)np * o->spp;
     SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control blocks may still be in flight
     if (!timer.on) {
-      // Large chunks run as kSubWaves sub-wavefronts (a share of the pixels and of the paths in
-      // flight each) on as many streams: when one's traversal launch runs out of rays and its SMs
+      // Large chunks of large scenes run as kSubWaves sub-wavefronts (a share of the pixels and of
+      // the paths in flight each) on as many streams: when one's traversal launch runs out of rays and its SMs
       // idle while the last rays finish, the others' kernels fill them. Per-pixel results do not
       // depend on it.
       const int nsub = (!(o->flags & SWR_RENDER_ONE_WAVEFRONT) && total >= kTwoWaveSamples &&
-                        np >= (uint32_t)kSubWaves && cap >= 256u * kSubWaves) ? kSubWaves : 1;
+                        s->dev.num_tris >= kTwoWaveTriangles && np >= (uint32_t)kSubWaves &&
+                        cap >= 256u * kSubWaves) ? kSubWaves : 1;
       if (nsub > 1) {
         if (!ws->fork) {
           SWR_CUDA(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));

@@ -108,12 +108,14 @@ def test_gpu_converged_image_within_statistical_error_of_fp64(tmp_path):
 
 
 def test_two_subwavefronts_equal_one_wavefront(tmp_path):
-    """A chunk of 2^20 samples or more runs as two concurrent sub-wavefronts on two streams; the
-    image and every sample equal those of a single wavefront (SWR_RENDER_ONE_WAVEFRONT)."""
-    s = scenes.cornell(9, str(tmp_path))
+    """A chunk of 2^20 samples or more of a scene of 2^16 triangles or more runs as two concurrent
+    sub-wavefronts on two streams; the image and every sample equal those of a single wavefront
+    (SWR_RENDER_ONE_WAVEFRONT)."""
+    s = scenes.terrain(6, str(tmp_path), cells=192, tile=16, spheres=8, sphere_subdiv=2, lights=2)
     sd = swr.load_scene(s["scene"], s["basepath"])
+    assert sd.num_triangles >= 1 << 16
     sc = swr.Scene(sd)
-    W, H, spp, depth = 200, 150, 40, 5  # 1.2 M samples
+    W, H, spp, depth = 200, 150, 40, 6  # 1.2 M samples
     cam = swr.load_camera(s["camera"], W, H)
     import ctypes
     from master_thesis_b200 import _native as N
