@@ -790,7 +790,7 @@ def main():
     ap.add_argument("--scene-dir", default=None)
     ap.add_argument("--tune", action="store_true", help="autotune the launch shape (cached) before timing")
     ap.add_argument("--no-graph", action="store_true",
-                    help="batched configurations: launch the shade/trace rounds from the host instead of one graph")
+                    help="launch the shade/trace rounds from the host instead of a CUDA graph (for profilers)")
     ap.add_argument("--split", default="images", choices=["images", "spp", "tiles"],
                     help="with N>1: independent images per GPU (weak scaling) or one image split by sample "
                          "range / pixel tile over the GPUs (strong scaling)")
@@ -902,6 +902,8 @@ def main():
         stats = scene.stats()
         shape = autotune.tune_render(scene, cam, W, H, spp, depth)
         tuned = {"build": bo, "launch": shape}
+    if args.no_graph:  # every round launched from the host (kernels visible to a profiler one by one)
+        shape = dict(shape, host_loop=True)
     # images: every rank renders its own image (seed 1000 + rank); spp / tiles: all ranks render
     # one image (seed 1000) split by sample range or pixel tile (sharding.render_split)
     split = args.split  # with one GPU a split renders the whole image as its one part

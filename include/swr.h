@@ -120,7 +120,7 @@ typedef struct swr_render_opts {
   uint32_t flags;          /* SWR_RENDER_* */
   uint32_t refill;         /* bounce traversal: idle lanes (1..32) that trigger a refill, 0 = 8 */
   uint32_t trace_blocks;   /* bounce traversal: resident blocks per SM targeted by the register
-                              budget, one of 0 (compiler's choice), 9, 10 */
+                              budget, one of 0 (the library's default, 9), 9, 10 */
   uint32_t shade_batch;    /* adjoint: lanes of a warp with a pending hit that shade together
                               (1..32; fewer when no trace of the warp is in flight), 0 = the
                               library's choice; the wavefront renders ignore it */
@@ -247,6 +247,12 @@ int swr_render(swr_scene* scene, const swr_camera* cam, const swr_render_opts* o
                                        SMs one of them leaves idle at the end of a traversal launch
                                        take the other's work; results are identical either way.
                                        Profiled renders (SWR_RENDER_PROFILE) always use one. */
+#define SWR_RENDER_HOST_LOOP 64u    /* the host launches every shade/trace round itself, one
+                                       wavefront per chunk (as profiled renders do), instead of
+                                       launching a CUDA graph whose round loop ends on the device.
+                                       Profilers that capture kernels one launch at a time cannot
+                                       capture the kernel nodes of such a graph. Results are
+                                       identical; it is slower (a host wait every 8 rounds). */
 
 /* Per-call instrumentation of swr_render_profiled. Times are device milliseconds summed over the
  * launches of each kernel kind (with SWR_RENDER_PROFILE). */

@@ -28,6 +28,7 @@ RENDER_COUNT = 4
 RENDER_STATIC_FETCH = 8
 RENDER_POSTPONE = 16
 RENDER_ONE_WAVEFRONT = 32
+RENDER_HOST_LOOP = 64
 
 
 class SwrError(RuntimeError):

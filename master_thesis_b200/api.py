@@ -240,9 +240,12 @@ class Scene:
     def render(self, cam, width, height, spp, depth, seed=0, mode=N.MODE_REFERENCE, rr_depth=0,
                rr_survive=1.0, wave_size=0, block_size=0, out=None, samples=None, stream=None,
                profile=False, count=False, return_profile=False, static_fetch=False, refill=0,
-               trace_blocks=0, sample_begin=0, spp_total=0, pixel_begin=0, pixel_count=0):
+               trace_blocks=0, sample_begin=0, spp_total=0, pixel_begin=0, pixel_count=0, host_loop=False):
         """Renders an image (height, width, 3) float32 into `out` (torch cuda tensor or numpy array;
         a numpy array makes the library stage the result through the device).
+
+        host_loop: the host launches every shade/trace round (SWR_RENDER_HOST_LOOP) instead of a
+        CUDA graph whose loop ends on the device, so that a profiler can capture single launches.
 
         Part of an image: samples [sample_begin, sample_begin + spp) of an image of spp_total
         samples per pixel (scaled by that image's 1/spp_total, so parts over a partition of the
@@ -250,7 +253,8 @@ class Scene:
         row-major order (out then holds (pixel_count, 3) floats, bit-identical to those pixels of
         the whole image)."""
         flags = (N.RENDER_SAMPLES_OUT if samples is not None else 0) | (N.RENDER_PROFILE if profile else 0) | \
-            (N.RENDER_COUNT if count else 0) | (N.RENDER_STATIC_FETCH if static_fetch else 0)
+            (N.RENDER_COUNT if count else 0) | (N.RENDER_STATIC_FETCH if static_fetch else 0) | \
+            (N.RENDER_HOST_LOOP if host_loop else 0)
         o = N.RenderOpts(width, height, spp, depth, seed, mode, rr_depth, rr_survive, wave_size, block_size, flags,
                          refill, trace_blocks, 0, sample_begin, spp_total, pixel_begin, pixel_count)
         if out is None:

@@ -110,7 +110,7 @@ def test_gpu_converged_image_within_statistical_error_of_fp64(tmp_path):
 def test_two_subwavefronts_equal_one_wavefront(tmp_path):
     """A chunk of 2^20 samples or more of a scene of 2^16 triangles or more runs as two concurrent
     sub-wavefronts on two streams; the image and every sample equal those of a single wavefront
-    (SWR_RENDER_ONE_WAVEFRONT)."""
+    (SWR_RENDER_ONE_WAVEFRONT) and of the host-driven round loop (SWR_RENDER_HOST_LOOP)."""
     s = scenes.terrain(6, str(tmp_path), cells=192, tile=16, spheres=8, sphere_subdiv=2, lights=2)
     sd = swr.load_scene(s["scene"], s["basepath"])
     assert sd.num_triangles >= 1 << 16
@@ -120,7 +120,7 @@ def test_two_subwavefronts_equal_one_wavefront(tmp_path):
     import ctypes
     from master_thesis_b200 import _native as N
     outs = []
-    for flags in (0, N.RENDER_ONE_WAVEFRONT):
+    for flags in (0, N.RENDER_ONE_WAVEFRONT, N.RENDER_HOST_LOOP):
         out = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
         smp = torch.empty((H * W, spp, 4), dtype=torch.float32, device="cuda")
         o = N.RenderOpts(W, H, spp, depth, 5, 0, 0, 1.0, 1 << 16, 0, flags | N.RENDER_SAMPLES_OUT, 0, 0, 0)
@@ -128,8 +128,9 @@ def test_two_subwavefronts_equal_one_wavefront(tmp_path):
                                  torch.cuda.current_stream().cuda_stream))
         torch.cuda.synchronize()
         outs.append((out.cpu().numpy(), smp.cpu().numpy()))
-    assert np.array_equal(outs[0][0], outs[1][0])
-    assert np.array_equal(outs[0][1], outs[1][1])
+    for k in (1, 2):
+        assert np.array_equal(outs[0][0], outs[k][0])
+        assert np.array_equal(outs[0][1], outs[k][1])
     assert outs[0][0].max() > 0
     # and on a host output buffer, twice in a row (graphs and streams reused)
     for _ in range(2):
