@@ -2,7 +2,7 @@
 
 For a workload it times a small grid of the tunable knobs with CUDA events, keeps the fastest, and
 caches the choice in a JSON file keyed by the workload's shape and the GPU name:
-  - the tree (tune_build): children per wide node (BVH width 4 or 8; the node record keeps 8
+  - the tree (tune_build, tune_batch_build): children per wide node (BVH width 4 or 8; the node record keeps 8
     slots) and triangles per leaf, each candidate built and rendered;
   - the launch (tune_render, tune_batch): paths in flight (wave size), the idle-lane refill
     threshold of the traversal, the shading kernel's block size and the traversal's register
@@ -10,6 +10,7 @@ caches the choice in a JSON file keyed by the workload's shape and the GPU name:
 
     bo = tune_build(scene_data, cam, width, height, spp, depth, mode=...)  # -> dict of Scene kwargs
     cfg = tune_render(scene, cam, width, height, spp, depth, mode=...)   # -> dict of render kwargs
+    bo = tune_batch_build(scene_datas, jobs)                             # -> dict of Scene kwargs
     cfg = tune_batch(batch, jobs)                                        # -> dict of batch kwargs
     cfg = tune_bdpt(scene, cam, width, height, spp, vj, lj, md)          # -> dict of render_bdpt kwargs
     cfg = tune_rt(scene, cam, width, height, spp, vision_jumps)          # -> dict of rt.render kwargs
@@ -120,6 +121,39 @@ def tune_render(scene, cam, width, height, spp, depth, mode=0, rr_depth=0, rr_su
         scene.render(cam, width, height, spp, depth, mode=mode, rr_depth=rr_depth, rr_survive=rr_survive, out=out,
                      **cfg)
     return _search(key, grid or RENDER_GRID, run, reps, force)
+
+
+def tune_batch_build(datas, jobs, reps=1, force=False, grid=None, builder="host"):
+    """Tree options for the scenes of a batch: datas[i] is the SceneData of jobs[i] (jobs as for
+    Batch.render, without their "scene"). Each candidate of the grid builds every scene with the
+    same options and times one batched render with the library's default launch shape; returns
+    the fastest as Scene kwargs."""
+    from .api import Batch, Scene
+    tris = sum(d.num_triangles for d in datas)
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    key = "batchbuild|%s|%s|jobs=%d|tris=%d|samples=%d" % (torch.cuda.get_device_name(), builder, len(jobs), tris,
+                                                          samples)
+    outs = [torch.empty((j["height"], j["width"], 3), dtype=torch.float32, device="cuda") for j in jobs]
+    batch = Batch()
+    built = {}
+
+    def release():
+        for scs in built.values():
+            for sc in scs:
+                sc.close()
+        built.clear()
+
+    def run(cfg):
+        k = tuple(sorted(cfg.items()))
+        if k not in built:
+            release()
+            built[k] = [Scene(d, builder=builder, **cfg) for d in datas]
+        batch.render([dict(j, scene=sc, out=o) for j, sc, o in zip(jobs, built[k], outs)])
+    try:
+        return _search(key, grid or BUILD_GRID, run, reps, force)
+    finally:
+        release()
+        batch.close()
 
 
 def tune_batch(batch, jobs, reps=1, force=False, grid=None):

@@ -88,3 +88,37 @@ def test_tune_build_on_gpu(tmp_path, monkeypatch):
     a = swr.Scene(sd, **best).render(c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL)
     b = swr.Scene(sd).render(c, 64, 48, 4, 4, mode=swr.MODE_PHYSICAL)
     assert torch.equal(a, b)
+
+
+@pytest.mark.gpu
+def test_tune_batch_build_on_gpu(tmp_path, monkeypatch):
+    """The batch's tree options (BVH width, leaf size) are tuned on the batch itself and cached;
+    the chosen trees render the same batch images as the default ones."""
+    import torch
+    import master_thesis_b200 as swr
+    from master_thesis_b200 import scenes
+    monkeypatch.setattr(autotune, "CACHE", str(tmp_path / "tune.json"))
+    datas, jobs = [], []
+    for k, (n, side, spp) in enumerate([(2000, 32, 4), (6000, 48, 2), (800, 24, 8)]):
+        sd, cam = scenes.random_scene(40 + k, n)
+        datas.append(sd)
+        jobs.append(dict(cam=swr.make_camera(cam["position"], cam["angle"], side, side, fov_deg=40), width=side,
+                         height=side, spp=spp, depth=4, seed=k, mode=swr.MODE_PHYSICAL))
+    best = autotune.tune_batch_build(datas, jobs)
+    assert best["width"] in (4, 8) and best["max_leaf"] in (2, 3)
+    db = json.loads((tmp_path / "tune.json").read_text())
+    (entry,) = [v for k, v in db.items() if k.startswith("batchbuild|")]
+    assert len(entry["tried"]) == 4 and entry["best"] == best
+    imgs = []
+    for opts in (best, {}):
+        b = swr.Batch()
+        scs = [swr.Scene(sd, **opts) for sd in datas]
+        outs = [torch.empty((j["height"], j["width"], 3), dtype=torch.float32, device="cuda") for j in jobs]
+        b.render([dict(j, scene=sc, out=o) for j, sc, o in zip(jobs, scs, outs)])
+        torch.cuda.synchronize()
+        imgs.append([o.cpu() for o in outs])
+        b.close()
+        for sc in scs:
+            sc.close()
+    for x, y in zip(*imgs):
+        assert torch.equal(x, y)
