@@ -171,83 +171,139 @@ static unsigned camera_grid(const swr_scene* s, uint32_t np) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)s->num_sms * std::max(per_sm, 1)));
 }
 
+// One entry of a shading round: a continuing path (its ray and the hit the traversal found) or an
+// injected camera sample (its pixel's camera-prefix record).
+struct ShadeEntry {
+  swrx::PathState st;
+  uint32_t pixel, sample, slot;
+  float t;
+};
+
+__device__ __forceinline__ ShadeEntry load_entry(const Frame& F, const Queue& in, uint32_t i, uint32_t n_in,
+                                                 unsigned long long inj_base) {
+  ShadeEntry e;
+  e.slot = kDeadSlot;
+  e.t = 0.0f;
+  if (i < n_in) {
+    const float4 qo = __ldcs(in.o + i), qd = __ldcs(in.d + i), qc = __ldcs(in.c + i);
+    const uint2 h = __ldcs(in.hit + i);
+    e.pixel = __float_as_uint(qo.w);
+    e.sample = __float_as_uint(qd.w);
+    const uint32_t meta = __float_as_uint(qc.w);
+    e.st.o = mk(qo.x, qo.y, qo.z);
+    e.st.d = mk(qd.x, qd.y, qd.z);
+    e.st.c = mk(qc.x, qc.y, qc.z);
+    e.st.i = (meta >> 8) & 0xFFu;
+    e.st.v = meta & 0xFFu;
+    if (F.mode == 1) {
+      const float4 ql = __ldcs(in.l + i);
+      e.st.L = mk(ql.x, ql.y, ql.z);
+    } else {
+      e.st.L = mk(0, 0, 0);
+    }
+    e.slot = h.x;
+    e.t = __uint_as_float(h.y);
+  } else {
+    const unsigned long long g = inj_base + (i - n_in);
+    e.pixel = (uint32_t)(g / F.spp);
+    e.sample = (uint32_t)(g % F.spp);
+    const float4 r0 = F.cam[2 * (size_t)e.pixel], r1 = F.cam[2 * (size_t)e.pixel + 1];
+    const uint32_t bits = __float_as_uint(r1.w);
+    e.st.c = mk(1.0f, 1.0f, 1.0f);
+    e.st.L = mk(0.0f, 0.0f, 0.0f);
+    e.st.v = 0;
+    e.st.o = mk(r0.x, r0.y, r0.z);
+    e.st.d = mk(r1.x, r1.y, r1.z);
+    e.st.i = bits >> 27;
+    if (bits != kDeadSlot) {
+      e.slot = bits & 0x07FFFFFFu;
+      e.t = r0.w;
+    }
+  }
+  return e;
+}
+
+// Shading round: entries [0, n_in) are the traced paths of the previous round, [n_in, n_in +
+// n_inj) new camera samples. An entry without a hit (a ray that left the scene, a camera sample
+// of a background pixel) ends dark at once; the block lists the others in shared memory and its
+// first warps shade them, so the long shading code (Philox, double-precision trigonometry and
+// normalisation) runs on full warps although most bounce rays miss. Results do not depend on which
+// thread shades which entry.
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock)
     k_shade(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, Queue in, Queue out, int parity) {
+  __shared__ uint32_t work[kBlock];
+  __shared__ uint32_t nwork;
   const uint32_t n_in = ctrl->count[parity];
   const uint32_t n_inj = ctrl->inj_n[parity];
   const unsigned long long inj_base = ctrl->inj_base[parity];
   const uint32_t pixel0 = ctrl->pixel0;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (blockIdx.x * kBlock >= n_in + n_inj) return;
+  if (blockIdx.x * kBlock >= n_in + n_inj) return;  // the whole block
+  if (threadIdx.x == 0) nwork = 0u;
+  __syncthreads();
 
-  bool live = false;
-  swrx::PathState st;
-  uint32_t pixel = 0, sample = 0, slot = kDeadSlot;
-  float t = 0.0f;
-  bool have = false;
+  // entries without a hit: their dark end; the rest: listed
+  bool has_hit = false;
   if (i < n_in) {
-    const float4 qo = __ldcs(in.o + i), qd = __ldcs(in.d + i), qc = __ldcs(in.c + i);
-    const uint2 h = __ldcs(in.hit + i);
-    pixel = __float_as_uint(qo.w);
-    sample = __float_as_uint(qd.w);
-    const uint32_t meta = __float_as_uint(qc.w);
-    st.o = mk(qo.x, qo.y, qo.z);
-    st.d = mk(qd.x, qd.y, qd.z);
-    st.c = mk(qc.x, qc.y, qc.z);
-    st.i = (meta >> 8) & 0xFFu;
-    st.v = meta & 0xFFu;
-    if (F.mode == 1) {
-      const float4 ql = __ldcs(in.l + i);
-      st.L = mk(ql.x, ql.y, ql.z);
+    const uint2 h = in.hit[i];
+    if (h.x != kDeadSlot) {
+      has_hit = true;
     } else {
-      st.L = mk(0, 0, 0);
+      const uint32_t pixel = __float_as_uint(__ldcs(&in.o[i].w));
+      const uint32_t sample = __float_as_uint(__ldcs(&in.d[i].w));
+      float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (F.mode == 1) {
+        const float4 ql = __ldcs(in.l + i);
+        r = make_float4(ql.x, ql.y, ql.z, 1.0f);
+      }
+      __stcs(F.contrib + (size_t)pixel * F.spp + sample, r);
     }
-    slot = h.x;
-    t = __uint_as_float(h.y);
-    have = true;
   } else if (i < n_in + n_inj) {
     const unsigned long long g = inj_base + (i - n_in);
-    pixel = (uint32_t)(g / F.spp);
-    sample = (uint32_t)(g % F.spp);
-    const float4 r0 = F.cam[2 * (size_t)pixel], r1 = F.cam[2 * (size_t)pixel + 1];
-    const uint32_t bits = __float_as_uint(r1.w);
-    st.c = mk(1.0f, 1.0f, 1.0f);
-    st.L = mk(0.0f, 0.0f, 0.0f);
-    st.v = 0;
-    if (bits != kDeadSlot) {
-      st.o = mk(r0.x, r0.y, r0.z);
-      st.d = mk(r1.x, r1.y, r1.z);
-      st.i = bits >> 27;
-      slot = bits & 0x07FFFFFFu;
-      t = r0.w;
+    const uint32_t pixel = (uint32_t)(g / F.spp);
+    if (__float_as_uint(F.cam[2 * (size_t)pixel + 1].w) != kDeadSlot) {
+      has_hit = true;
+    } else {
+      const float4 r = (F.mode == 1) ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      __stcs(F.contrib + (size_t)pixel * F.spp + (uint32_t)(g % F.spp), r);
     }
-    have = true;
   }
-  if (have) {
-    uint32_t outcome = swrx::kEndDark;
-    if (slot != kDeadSlot) {
-      swrx::ShadeParams P;
-      P.seed = F.seed;
-      P.pixel = pixel0 + pixel;
-      P.sample = F.sample0 + sample;
-      P.depth = F.depth;
-      P.mode = F.mode;
-      P.rr_depth = F.rr_depth;
-      P.rr_q = F.rr_q;
-      outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
-    }
+  {
+    const unsigned m = __ballot_sync(0xffffffffu, has_hit);
+    unsigned base = 0;
+    if (lane_id() == 0 && m) base = atomicAdd(&nwork, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (has_hit) work[base + __popc(m & ((1u << lane_id()) - 1u))] = i;
+  }
+  __syncthreads();
+  const uint32_t cnt = nwork;
+  if ((threadIdx.x & ~31u) >= cnt) return;  // the whole warp: nothing listed for it
+
+  bool live = false;
+  ShadeEntry e;
+  if (threadIdx.x < cnt) {
+    e = load_entry(F, in, work[threadIdx.x], n_in, inj_base);
+    swrx::ShadeParams P;
+    P.seed = F.seed;
+    P.pixel = pixel0 + e.pixel;
+    P.sample = F.sample0 + e.sample;
+    P.depth = F.depth;
+    P.mode = F.mode;
+    P.rr_depth = F.rr_depth;
+    P.rr_q = F.rr_q;
+    const uint32_t outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, e.slot, e.t, P, e.st);
     if (outcome == swrx::kContinue) {
       live = true;
     } else {
       float4 r;
       if (F.mode == 0)
-        r = (outcome == swrx::kEndLight) ? make_float4(st.c.x, st.c.y, st.c.z, 1.0f)
+        r = (outcome == swrx::kEndLight) ? make_float4(e.st.c.x, e.st.c.y, e.st.c.z, 1.0f)
                                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       else
-        r = make_float4(st.L.x, st.L.y, st.L.z, 1.0f);
-      __stcs(F.contrib + (size_t)pixel * F.spp + sample, r);
+        r = make_float4(e.st.L.x, e.st.L.y, e.st.L.z, 1.0f);
+      __stcs(F.contrib + (size_t)e.pixel * F.spp + e.sample, r);
     }
   }
   // warp-aggregated append of the live paths
@@ -259,10 +315,10 @@ __global__ void __launch_bounds__(kBlock)
   base = __shfl_sync(0xffffffffu, base, leader);
   if (live) {
     const unsigned j = base + __popc(mask & ((1u << lane_id()) - 1u));
-    __stcs(out.o + j, make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel)));
-    __stcs(out.d + j, make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample)));
-    __stcs(out.c + j, make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((st.i << 8) | st.v)));
-    if (F.mode == 1) __stcs(out.l + j, make_float4(st.L.x, st.L.y, st.L.z, 0.0f));
+    __stcs(out.o + j, make_float4(e.st.o.x, e.st.o.y, e.st.o.z, __uint_as_float(e.pixel)));
+    __stcs(out.d + j, make_float4(e.st.d.x, e.st.d.y, e.st.d.z, __uint_as_float(e.sample)));
+    __stcs(out.c + j, make_float4(e.st.c.x, e.st.c.y, e.st.c.z, __uint_as_float((e.st.i << 8) | e.st.v)));
+    if (F.mode == 1) __stcs(out.l + j, make_float4(e.st.L.x, e.st.L.y, e.st.L.z, 0.0f));
   }
 }
 
