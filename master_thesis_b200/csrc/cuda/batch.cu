@@ -137,73 +137,107 @@ __device__ __forceinline__ void accumulate(unsigned long long* acc, float r, flo
   atomicAdd(acc + 2, (unsigned long long)__double2ll_rn((double)b * kFix));
 }
 
+// Shading round of the batch (as the single-scene k_shade): entries without a hit end at once, the
+// rest are listed in shared memory (entry, job) and shaded by the block's first warps.
 __global__ void __launch_bounds__(256) k_bshade(BArgs A, BCtrl* __restrict__ ctrl, BQueue in, BQueue out,
                                                 int parity) {
+  __shared__ uint2 work[256];
+  __shared__ uint32_t nwork;
   const uint32_t n_in = ctrl->count[parity];
   const uint32_t n_inj = ctrl->inj_n[parity];
   const unsigned long long inj_base = ctrl->inj_base[parity];
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
   const uint32_t i = blockIdx.x * 256 + threadIdx.x;
-  if (blockIdx.x * 256 >= n_in + n_inj) return;
-  bool live = false, have = false;
-  swrx::PathState st;
-  uint32_t pixel = 0, sample = 0, job = 0, slot = kDead;
-  float t = 0.0f;
+  if (blockIdx.x * 256 >= n_in + n_inj) return;  // the whole block
+  if (threadIdx.x == 0) nwork = 0u;
+  __syncthreads();
+
+  bool has_hit = false;
+  uint32_t job = 0;
   if (i < n_in) {
-    const float4 qo = in.o[i], qd = in.d[i], qc = in.c[i];
     const uint2 h = in.hit[i];
-    pixel = __float_as_uint(qo.w);
-    sample = __float_as_uint(qd.w);
-    const uint32_t meta = __float_as_uint(qc.w);
+    const uint32_t meta = __float_as_uint(in.c[i].w);
     job = meta >> 16;
-    st.o = mk(qo.x, qo.y, qo.z);
-    st.d = mk(qd.x, qd.y, qd.z);
-    st.c = mk(qc.x, qc.y, qc.z);
-    st.i = (meta >> 8) & 0xFFu;
-    st.v = meta & 0xFFu;
-    const float4 ql = in.l[i];
-    st.L = mk(ql.x, ql.y, ql.z);
-    slot = h.x;
-    t = __uint_as_float(h.y);
-    have = true;
+    if (h.x != kDead) {
+      has_hit = true;
+    } else {
+      const BJob& J = A.jobs[job];
+      if (J.mode != 0) {  // physical mode: the path ends with the radiance it gathered
+        const uint32_t pixel = __float_as_uint(in.o[i].w);
+        const float4 ql = in.l[i];
+        accumulate(A.accum + 3 * (J.pixel_base + pixel), ql.x, ql.y, ql.z);
+      }
+    }
   } else if (i < n_in + n_inj) {
     const unsigned long long g = inj_base + (i - n_in);
     job = find_job(A.jobs, A.njobs, g, false);
     const BJob& J = A.jobs[job];
-    const uint64_t local = g - J.sample_base;
-    pixel = (uint32_t)(local / J.spp);
-    sample = (uint32_t)(local % J.spp);
-    const uint64_t p = J.pixel_base + pixel;
-    const float4 r0 = A.cam[2 * p], r1 = A.cam[2 * p + 1];
-    const uint32_t bits = __float_as_uint(r1.w);
-    st.c = mk(1.0f, 1.0f, 1.0f);
-    st.L = mk(0.0f, 0.0f, 0.0f);
-    st.v = 0;
-    st.i = 0;
-    if (bits != kDead) {
+    const uint64_t p = J.pixel_base + (g - J.sample_base) / J.spp;
+    has_hit = __float_as_uint(A.cam[2 * p + 1].w) != kDead;  // else: a background pixel, nothing gathered
+  }
+  {
+    const unsigned m = __ballot_sync(0xffffffffu, has_hit);
+    unsigned base = 0;
+    if (lane() == 0 && m) base = atomicAdd(&nwork, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (has_hit) work[base + __popc(m & ((1u << lane()) - 1u))] = make_uint2(i, job);
+  }
+  __syncthreads();
+  const uint32_t cnt = nwork;
+  if ((threadIdx.x & ~31u) >= cnt) return;  // the whole warp: nothing listed for it
+
+  bool live = false;
+  swrx::PathState st;
+  uint32_t pixel = 0, sample = 0, slot = kDead;
+  float t = 0.0f;
+  job = 0;
+  if (threadIdx.x < cnt) {
+    const uint2 w = work[threadIdx.x];
+    const uint32_t e = w.x;
+    job = w.y;
+    const BJob& J = A.jobs[job];
+    if (e < n_in) {
+      const float4 qo = in.o[e], qd = in.d[e], qc = in.c[e];
+      const uint2 h = in.hit[e];
+      pixel = __float_as_uint(qo.w);
+      sample = __float_as_uint(qd.w);
+      const uint32_t meta = __float_as_uint(qc.w);
+      st.o = mk(qo.x, qo.y, qo.z);
+      st.d = mk(qd.x, qd.y, qd.z);
+      st.c = mk(qc.x, qc.y, qc.z);
+      st.i = (meta >> 8) & 0xFFu;
+      st.v = meta & 0xFFu;
+      const float4 ql = in.l[e];
+      st.L = mk(ql.x, ql.y, ql.z);
+      slot = h.x;
+      t = __uint_as_float(h.y);
+    } else {
+      const unsigned long long g = inj_base + (e - n_in);
+      const uint64_t local = g - J.sample_base;
+      pixel = (uint32_t)(local / J.spp);
+      sample = (uint32_t)(local % J.spp);
+      const uint64_t p = J.pixel_base + pixel;
+      const float4 r0 = A.cam[2 * p], r1 = A.cam[2 * p + 1];
+      const uint32_t bits = __float_as_uint(r1.w);
+      st.c = mk(1.0f, 1.0f, 1.0f);
+      st.L = mk(0.0f, 0.0f, 0.0f);
+      st.v = 0;
       st.o = mk(r0.x, r0.y, r0.z);
       st.d = mk(r1.x, r1.y, r1.z);
       st.i = bits >> 27;
       slot = bits & 0x07FFFFFFu;
       t = r0.w;
     }
-    have = true;
-  }
-  if (have) {
-    const BJob& J = A.jobs[job];
-    uint32_t outcome = swrx::kEndDark;
-    if (slot != kDead) {
-      const DevScene& sc = A.scenes[J.scene];
-      swrx::ShadeParams P;
-      P.seed = J.seed;
-      P.pixel = pixel;
-      P.sample = sample;
-      P.depth = J.depth;
-      P.mode = J.mode;
-      P.rr_depth = J.rr_depth;
-      P.rr_q = J.rr_q;
-      outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
-    }
+    const DevScene& sc = A.scenes[J.scene];
+    swrx::ShadeParams P;
+    P.seed = J.seed;
+    P.pixel = pixel;
+    P.sample = sample;
+    P.depth = J.depth;
+    P.mode = J.mode;
+    P.rr_depth = J.rr_depth;
+    P.rr_q = J.rr_q;
+    const uint32_t outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
     if (outcome == swrx::kContinue) {
       live = true;
     } else {
