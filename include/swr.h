@@ -481,7 +481,11 @@ typedef struct swr_rt_renderer_params {
 int swr_rt_renderer_load(const char* renderer_path, swr_rt_renderer_params* out);
 
 /* One frame of GraphicsEngine::render (src/graphic/graphics_engine.cpp:30-70): the PathTracer
- * image, then each denoiser reading the previous image; rgba8_out receives the last image. */
+ * image, then each denoiser reading the previous image; rgba8_out receives the last image.
+ * The denoisers' intermediate images and the device copy of a host rgba8_out live in a buffer the
+ * scene keeps (grown by the first call that needs more), so frame loops allocate nothing per
+ * frame; as the render workspace, it is the scene's, so one scene renders on one stream at a time
+ * (swr_rt_render's host outputs use it too). */
 int swr_rt_render_frame(swr_scene* scene, const swr_camera* cam, const swr_rt_opts* opts,
                         const swr_rt_denoiser* denoisers, uint32_t num_denoisers,
                         uint8_t* rgba8_out, void* stream);

@@ -341,6 +341,34 @@ void release(Staged& st, cudaStream_t stream) {
   st.dev = nullptr;
 }
 
+// The scene's RayTrace buffer, at least `need` bytes (grown on demand; growing waits for the
+// stream, whose earlier frames may still read the old buffer). Frames into host memory and frames
+// with denoisers then allocate nothing per call.
+int rt_buffer(swr_scene* s, size_t need, cudaStream_t stream, char** out) {
+  if (need > s->rt_buf_bytes) {
+    SWR_CUDA(cudaStreamSynchronize(stream));
+    if (s->rt_buf) SWR_CUDA(cudaFree(s->rt_buf));
+    s->rt_buf = nullptr;
+    s->rt_buf_bytes = 0;
+    SWR_CUDA(cudaMalloc(&s->rt_buf, need));
+    s->rt_buf_bytes = need;
+  }
+  *out = (char*)s->rt_buf;
+  return SWR_OK;
+}
+
+// Device view of an output buffer from the scene's RayTrace buffer at `*at` (advanced past it)
+// when it is host memory.
+void stage_out(void* user, size_t bytes, char* buf, size_t* at, Staged& st) {
+  st.user = user;
+  st.bytes = bytes;
+  st.dev = user;
+  st.host = user && is_host_pointer(user);
+  if (!st.host) return;
+  st.dev = buf + *at;
+  *at += (bytes + 255) & ~(size_t)255;
+}
+
 int copy_back(Staged& st, cudaStream_t stream) {
   if (st.host) SWR_CUDA(cudaMemcpyAsync(st.user, st.dev, st.bytes, cudaMemcpyDeviceToHost, stream));
   return SWR_OK;
@@ -432,17 +460,17 @@ int swr_rt_render(swr_scene* s, const swr_camera* cam, const swr_rt_opts* opts, 
   cudaStream_t stream = (cudaStream_t)stream_;
   SWR_CUDA(cudaSetDevice(s->device));
   const size_t npix = (size_t)opts->width * opts->height;
+  const size_t need = (rgb_out && swr::is_host_pointer(rgb_out) ? ((npix * 12 + 255) & ~(size_t)255) : 0) +
+                      (rgba8_out && swr::is_host_pointer(rgba8_out) ? ((npix * 4 + 255) & ~(size_t)255) : 0);
+  char* buf = nullptr;
+  if (need && (rc = swr::rt_buffer(s, need, stream, &buf))) return rc;
   swr::Staged a, b;
-  if ((rc = swr::stage(rgb_out, npix * 12, false, stream, a))) return rc;
-  if ((rc = swr::stage(rgba8_out, npix * 4, false, stream, b))) {
-    swr::release(a, stream);
-    return rc;
-  }
+  size_t at = 0;
+  swr::stage_out(rgb_out, npix * 12, buf, &at, a);
+  swr::stage_out(rgba8_out, npix * 4, buf, &at, b);
   rc = swr::render_impl(s, cam, opts, (float*)a.dev, (uchar4*)b.dev, stream);
   if (!rc) rc = swr::copy_back(a, stream);
   if (!rc) rc = swr::copy_back(b, stream);
-  swr::release(a, stream);
-  swr::release(b, stream);
   if (!rc && (a.host || b.host)) SWR_CUDA(cudaStreamSynchronize(stream));
   return rc;
 }
@@ -509,15 +537,17 @@ int swr_rt_render_frame(swr_scene* s, const swr_camera* cam, const swr_rt_opts* 
   SWR_CUDA(cudaSetDevice(s->device));
   const uint32_t W = opts->width, H = opts->height;
   const size_t bytes = (size_t)W * H * 4;
-  swr::Staged so;
-  if ((rc = swr::stage(rgba8_out, bytes, false, stream, so))) return rc;
+  const size_t slot = (bytes + 255) & ~(size_t)255;
   // ping-pong images: the renderer writes the first denoiser's input, the last denoiser the output
-  void* tmp[2] = {nullptr, nullptr};
   const int ntmp = num_denoisers == 0 ? 0 : (num_denoisers == 1 ? 1 : 2);
-  for (int k = 0; k < ntmp && !rc; ++k) {
-    cudaError_t e = cudaMallocAsync(&tmp[k], bytes, stream);
-    if (e != cudaSuccess) rc = swr::cuda_fail(e, "cudaMallocAsync");
-  }
+  const size_t need = (size_t)ntmp * slot + (swr::is_host_pointer(rgba8_out) ? slot : 0);
+  char* buf = nullptr;
+  if (need && (rc = swr::rt_buffer(s, need, stream, &buf))) return rc;
+  void* tmp[2] = {nullptr, nullptr};
+  for (int k = 0; k < ntmp; ++k) tmp[k] = buf + (size_t)k * slot;
+  swr::Staged so;
+  size_t at = (size_t)ntmp * slot;
+  swr::stage_out(rgba8_out, bytes, buf, &at, so);
   uchar4* cur = num_denoisers ? (uchar4*)tmp[0] : (uchar4*)so.dev;
   if (!rc) rc = swr::render_impl(s, cam, opts, nullptr, cur, stream);
   for (uint32_t k = 0; k < num_denoisers && !rc; ++k) {
@@ -534,9 +564,6 @@ int swr_rt_render_frame(swr_scene* s, const swr_camera* cam, const swr_rt_opts* 
     cur = dst;
   }
   if (!rc) rc = swr::copy_back(so, stream);
-  for (void* p : tmp)
-    if (p) cudaFreeAsync(p, stream);
-  swr::release(so, stream);
   if (!rc && so.host) SWR_CUDA(cudaStreamSynchronize(stream));
   return rc;
 }

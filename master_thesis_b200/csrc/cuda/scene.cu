@@ -344,7 +344,7 @@ void swr_scene_destroy(swr_scene* s) {
   swr::free_workspace(s);
   swr::free_instance(s);
   for (void* p : {s->d_nodes, s->d_tris, s->d_shade, s->d_tri_boxes, s->d_obj_boxes, s->d_mats,
-                  s->d_albedo, s->d_slot_of, s->d_scratch, s->d_lights, s->d_light_tris})
+                  s->d_albedo, s->d_slot_of, s->d_scratch, s->d_lights, s->d_light_tris, s->rt_buf})
     if (p) cudaFree(p);
   delete s;
 }

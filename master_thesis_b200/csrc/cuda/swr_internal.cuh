@@ -53,6 +53,8 @@ struct swr_scene {
   std::vector<uint32_t> slot_to_id;  // host copy
   void* workspace = nullptr;          // render workspace (render.cu), grown on demand
   void* instance = nullptr;           // object-space data for moving objects (instance.cu)
+  void* rt_buf = nullptr;             // RayTrace frames: host-output staging and denoiser
+  size_t rt_buf_bytes = 0;            //   ping-pong images (rt.cu), grown on demand
 };
 
 namespace swr {

@@ -129,6 +129,26 @@ def test_gpu_rt_frame_with_denoiser_chain_matches_oracle_composition():
     host = np.zeros((H, W, 4), np.uint8)
     rt.render_frame(sc, cam, W, H, dict(vision_jumps=5, spp=13), out=host)
     assert np.array_equal(host, frame)
+    # the denoised frame into host memory, twice (the scene's buffer reused), then a larger frame
+    # (the buffer grows) and the smaller one again
+    for _ in range(2):
+        host = np.zeros((H, W, 4), np.uint8)
+        rt.render_frame(sc, cam, W, H, params, out=host)
+        assert np.array_equal(host, got)
+    big = rt.render_frame(sc, cam, 2 * W, 2 * H, params)
+    big_host = np.zeros((2 * H, 2 * W, 4), np.uint8)
+    rt.render_frame(sc, cam, 2 * W, 2 * H, params, out=big_host)
+    torch.cuda.synchronize()
+    assert np.array_equal(big_host, big.cpu().numpy())
+    host = np.zeros((H, W, 4), np.uint8)
+    rt.render_frame(sc, cam, W, H, params, out=host)
+    assert np.array_equal(host, got)
+    # swr_rt_render's host outputs go through the same buffer
+    rgb_d, rgba_d = rt.render(sc, cam, W, H, 13, 5)
+    rgb_h, rgba_h = np.zeros((H, W, 3), np.float32), np.zeros((H, W, 4), np.uint8)
+    rt.render(sc, cam, W, H, 13, 5, rgb=rgb_h, rgba=rgba_h)
+    torch.cuda.synchronize()
+    assert np.array_equal(rgb_h, rgb_d.cpu().numpy()) and np.array_equal(rgba_h, rgba_d.cpu().numpy())
 
 
 def test_gpu_rt_invalid_arguments():
