@@ -225,101 +225,123 @@ __device__ __forceinline__ ShadeEntry load_entry(const Frame& F, const Queue& in
 
 // Shading round: entries [0, n_in) are the traced paths of the previous round, [n_in, n_in +
 // n_inj) new camera samples. An entry without a hit (a ray that left the scene, a camera sample
-// of a background pixel) ends dark at once; the block lists the others in shared memory and its
-// first warps shade them, so the long shading code (Philox, double-precision trigonometry and
-// normalisation) runs on full warps although most bounce rays miss. Results do not depend on which
-// thread shades which entry.
+// of a background pixel) ends dark at once. The grid is persistent: each warp walks chunks of 32
+// entries, lists the entries with a hit in its own shared-memory list and shades them 32 at a
+// time, so that the long shading code (Philox, double-precision trigonometry and normalisation)
+// runs on full warps although most bounce rays miss, and no warp waits at a block barrier or
+// leaves its block's slot idle. Results do not depend on which lane shades which entry.
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock)
     k_shade(DevScene sc, Frame F, Ctrl* __restrict__ ctrl, Queue in, Queue out, int parity) {
-  __shared__ uint32_t work[kBlock];
-  __shared__ uint32_t nwork;
+  __shared__ uint32_t pending[kBlock / 32][64];
   const uint32_t n_in = ctrl->count[parity];
   const uint32_t n_inj = ctrl->inj_n[parity];
   const unsigned long long inj_base = ctrl->inj_base[parity];
   const uint32_t pixel0 = ctrl->pixel0;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (blockIdx.x * kBlock >= n_in + n_inj) return;  // the whole block
-  if (threadIdx.x == 0) nwork = 0u;
-  __syncthreads();
-
-  // entries without a hit: their dark end; the rest: listed
-  bool has_hit = false;
-  if (i < n_in) {
-    const uint2 h = in.hit[i];
-    if (h.x != kDeadSlot) {
-      has_hit = true;
-    } else {
-      const uint32_t pixel = __float_as_uint(__ldcs(&in.o[i].w));
-      const uint32_t sample = __float_as_uint(__ldcs(&in.d[i].w));
-      float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      if (F.mode == 1) {
-        const float4 ql = __ldcs(in.l + i);
-        r = make_float4(ql.x, ql.y, ql.z, 1.0f);
+  const uint64_t total = (uint64_t)n_in + n_inj;
+  const uint32_t lane = lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t* list = pending[threadIdx.x >> 5];
+  const uint64_t stride = (uint64_t)gridDim.x * kBlock;
+  uint32_t npend = 0;  // entries in the warp's list (the same in every lane)
+  for (uint64_t base = (uint64_t)blockIdx.x * kBlock + (threadIdx.x & ~31u);; base += stride) {
+    const bool more = base < total;
+    if (more) {
+      // entries without a hit: their dark end; the rest: listed
+      const uint64_t i = base + lane;
+      bool has_hit = false;
+      if (i < n_in) {
+        const uint2 h = in.hit[i];
+        if (h.x != kDeadSlot) {
+          has_hit = true;
+        } else {
+          const uint32_t pixel = __float_as_uint(__ldcs(&in.o[i].w));
+          const uint32_t sample = __float_as_uint(__ldcs(&in.d[i].w));
+          float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          if (F.mode == 1) {
+            const float4 ql = __ldcs(in.l + i);
+            r = make_float4(ql.x, ql.y, ql.z, 1.0f);
+          }
+          __stcs(F.contrib + (size_t)pixel * F.spp + sample, r);
+        }
+      } else if (i < total) {
+        const unsigned long long g = inj_base + (i - n_in);
+        const uint32_t pixel = (uint32_t)(g / F.spp);
+        if (__float_as_uint(F.cam[2 * (size_t)pixel + 1].w) != kDeadSlot) {
+          has_hit = true;
+        } else {
+          const float4 r = (F.mode == 1) ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          __stcs(F.contrib + (size_t)pixel * F.spp + (uint32_t)(g % F.spp), r);
+        }
       }
-      __stcs(F.contrib + (size_t)pixel * F.spp + sample, r);
+      const unsigned m = __ballot_sync(0xffffffffu, has_hit);
+      if (has_hit) list[npend + __popc(m & lt)] = (uint32_t)i;
+      npend += (uint32_t)__popc(m);
+      __syncwarp();
     }
-  } else if (i < n_in + n_inj) {
-    const unsigned long long g = inj_base + (i - n_in);
-    const uint32_t pixel = (uint32_t)(g / F.spp);
-    if (__float_as_uint(F.cam[2 * (size_t)pixel + 1].w) != kDeadSlot) {
-      has_hit = true;
-    } else {
-      const float4 r = (F.mode == 1) ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      __stcs(F.contrib + (size_t)pixel * F.spp + (uint32_t)(g % F.spp), r);
+    // a full warp of listed entries (or, after the last chunk, what is left) is shaded
+    while (npend >= 32u || (!more && npend > 0u)) {
+      const uint32_t cnt = npend < 32u ? npend : 32u;
+      npend -= cnt;
+      bool live = false;
+      ShadeEntry e;
+      if (lane < cnt) {
+        e = load_entry(F, in, list[npend + lane], n_in, inj_base);
+        swrx::ShadeParams P;
+        P.seed = F.seed;
+        P.pixel = pixel0 + e.pixel;
+        P.sample = F.sample0 + e.sample;
+        P.depth = F.depth;
+        P.mode = F.mode;
+        P.rr_depth = F.rr_depth;
+        P.rr_q = F.rr_q;
+        const uint32_t outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, e.slot, e.t, P, e.st);
+        if (outcome == swrx::kContinue) {
+          live = true;
+        } else {
+          float4 r;
+          if (F.mode == 0)
+            r = (outcome == swrx::kEndLight) ? make_float4(e.st.c.x, e.st.c.y, e.st.c.z, 1.0f)
+                                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          else
+            r = make_float4(e.st.L.x, e.st.L.y, e.st.L.z, 1.0f);
+          __stcs(F.contrib + (size_t)e.pixel * F.spp + e.sample, r);
+        }
+      }
+      __syncwarp();  // the list slots just read may be refilled by the next chunk
+      // warp-aggregated append of the live paths
+      const unsigned mask = __ballot_sync(0xffffffffu, live);
+      if (mask != 0u) {
+        unsigned obase = 0;
+        const unsigned leader = __ffs(mask) - 1;
+        if (lane == leader) obase = atomicAdd(&ctrl->count[parity ^ 1], (unsigned)__popc(mask));
+        obase = __shfl_sync(0xffffffffu, obase, leader);
+        if (live) {
+          const unsigned j = obase + __popc(mask & lt);
+          __stcs(out.o + j, make_float4(e.st.o.x, e.st.o.y, e.st.o.z, __uint_as_float(e.pixel)));
+          __stcs(out.d + j, make_float4(e.st.d.x, e.st.d.y, e.st.d.z, __uint_as_float(e.sample)));
+          __stcs(out.c + j, make_float4(e.st.c.x, e.st.c.y, e.st.c.z, __uint_as_float((e.st.i << 8) | e.st.v)));
+          if (F.mode == 1) __stcs(out.l + j, make_float4(e.st.L.x, e.st.L.y, e.st.L.z, 0.0f));
+        }
+      }
     }
+    if (!more) break;
   }
-  {
-    const unsigned m = __ballot_sync(0xffffffffu, has_hit);
-    unsigned base = 0;
-    if (lane_id() == 0 && m) base = atomicAdd(&nwork, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (has_hit) work[base + __popc(m & ((1u << lane_id()) - 1u))] = i;
-  }
-  __syncthreads();
-  const uint32_t cnt = nwork;
-  if ((threadIdx.x & ~31u) >= cnt) return;  // the whole warp: nothing listed for it
+}
 
-  bool live = false;
-  ShadeEntry e;
-  if (threadIdx.x < cnt) {
-    e = load_entry(F, in, work[threadIdx.x], n_in, inj_base);
-    swrx::ShadeParams P;
-    P.seed = F.seed;
-    P.pixel = pixel0 + e.pixel;
-    P.sample = F.sample0 + e.sample;
-    P.depth = F.depth;
-    P.mode = F.mode;
-    P.rr_depth = F.rr_depth;
-    P.rr_q = F.rr_q;
-    const uint32_t outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, e.slot, e.t, P, e.st);
-    if (outcome == swrx::kContinue) {
-      live = true;
-    } else {
-      float4 r;
-      if (F.mode == 0)
-        r = (outcome == swrx::kEndLight) ? make_float4(e.st.c.x, e.st.c.y, e.st.c.z, 1.0f)
-                                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      else
-        r = make_float4(e.st.L.x, e.st.L.y, e.st.L.z, 1.0f);
-      __stcs(F.contrib + (size_t)e.pixel * F.spp + e.sample, r);
-    }
+// persistent grid of the shading kernel for a queue of cap entries
+static unsigned shade_grid_for(const swr_scene* s, uint32_t cap, int block) {
+  int per_sm = 0;
+  cudaError_t e = block == 128   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade<128>, 128, 0)
+                  : block == 512 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade<512>, 512, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade<256>, 256, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
   }
-  // warp-aggregated append of the live paths
-  const unsigned mask = __ballot_sync(0xffffffffu, live);
-  if (mask == 0u) return;
-  unsigned base = 0;
-  const unsigned leader = __ffs(mask) - 1;
-  if (lane_id() == leader) base = atomicAdd(&ctrl->count[parity ^ 1], (unsigned)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (live) {
-    const unsigned j = base + __popc(mask & ((1u << lane_id()) - 1u));
-    __stcs(out.o + j, make_float4(e.st.o.x, e.st.o.y, e.st.o.z, __uint_as_float(e.pixel)));
-    __stcs(out.d + j, make_float4(e.st.d.x, e.st.d.y, e.st.d.z, __uint_as_float(e.sample)));
-    __stcs(out.c + j, make_float4(e.st.c.x, e.st.c.y, e.st.c.z, __uint_as_float((e.st.i << 8) | e.st.v)));
-    if (F.mode == 1) __stcs(out.l + j, make_float4(e.st.L.x, e.st.L.y, e.st.L.z, 0.0f));
-  }
+  const uint64_t need = ((uint64_t)cap + block - 1) / block;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)s->num_sms * std::max(per_sm, 1)));
 }
 
 template <bool kStats>
@@ -1185,7 +1207,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
   int trace_per_sm = 0;
   SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_per_sm, trace_kernel, kTraceBlock, 0));
   const unsigned trace_grid = (unsigned)(s->num_sms * std::max(trace_per_sm, 1));
-  const unsigned shade_grid = (cap + block - 1) / block;
+  const unsigned shade_grid = shade_grid_for(s, cap, block);
 
   // Sub-wavefront h of a chunk: pixels [off, off + n) of it, queues of capw paths carved from the
   // h-th half of the queue buffer (the whole buffer when the chunk runs as one wavefront), control
@@ -1229,7 +1251,7 @@ int render_impl(swr_scene* s, const swr_camera* cam, const swr_render_opts* o, f
     Frame FR = Fh;
     FR.pixel0 = 0;
     FR.npix = 0;
-    const unsigned sgrid = (capw + block - 1) / block;
+    const unsigned sgrid = shade_grid_for(s, capw, block);
     std::vector<char> key(sizeof(DevScene) + sizeof(Frame) + sizeof(Qh) + 5 * sizeof(void*));
     {
       char* kp = key.data();
