@@ -137,130 +137,136 @@ __device__ __forceinline__ void accumulate(unsigned long long* acc, float r, flo
   atomicAdd(acc + 2, (unsigned long long)__double2ll_rn((double)b * kFix));
 }
 
-// Shading round of the batch (as the single-scene k_shade): entries without a hit end at once, the
-// rest are listed in shared memory (entry, job) and shaded by the block's first warps.
+// Shading round of the batch (as the single-scene k_shade): entries without a hit end at once; a
+// persistent grid's warps walk chunks of 32 entries, list the rest (entry, job) in their own
+// shared-memory lists and shade them 32 at a time.
 __global__ void __launch_bounds__(256) k_bshade(BArgs A, BCtrl* __restrict__ ctrl, BQueue in, BQueue out,
                                                 int parity) {
-  __shared__ uint2 work[256];
-  __shared__ uint32_t nwork;
+  __shared__ uint2 pending[8][64];
   const uint32_t n_in = ctrl->count[parity];
   const uint32_t n_inj = ctrl->inj_n[parity];
   const unsigned long long inj_base = ctrl->inj_base[parity];
   if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->cursor[parity ^ 1] = 0u;
-  const uint32_t i = blockIdx.x * 256 + threadIdx.x;
-  if (blockIdx.x * 256 >= n_in + n_inj) return;  // the whole block
-  if (threadIdx.x == 0) nwork = 0u;
-  __syncthreads();
-
-  bool has_hit = false;
-  uint32_t job = 0;
-  if (i < n_in) {
-    const uint2 h = in.hit[i];
-    const uint32_t meta = __float_as_uint(in.c[i].w);
-    job = meta >> 16;
-    if (h.x != kDead) {
-      has_hit = true;
-    } else {
-      const BJob& J = A.jobs[job];
-      if (J.mode != 0) {  // physical mode: the path ends with the radiance it gathered
-        const uint32_t pixel = __float_as_uint(in.o[i].w);
-        const float4 ql = in.l[i];
-        accumulate(A.accum + 3 * (J.pixel_base + pixel), ql.x, ql.y, ql.z);
+  const uint64_t total = (uint64_t)n_in + n_inj;
+  const uint32_t ln = lane();
+  const uint32_t lt = (1u << ln) - 1u;
+  uint2* list = pending[threadIdx.x >> 5];
+  const uint64_t stride = (uint64_t)gridDim.x * 256;
+  uint32_t npend = 0;  // entries in the warp's list (the same in every lane)
+  for (uint64_t base = (uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u);; base += stride) {
+    const bool more = base < total;
+    if (more) {
+      const uint64_t i = base + ln;
+      bool has_hit = false;
+      uint32_t job = 0;
+      if (i < n_in) {
+        const uint2 h = in.hit[i];
+        const uint32_t meta = __float_as_uint(in.c[i].w);
+        job = meta >> 16;
+        if (h.x != kDead) {
+          has_hit = true;
+        } else {
+          const BJob& J = A.jobs[job];
+          if (J.mode != 0) {  // physical mode: the path ends with the radiance it gathered
+            const uint32_t pixel = __float_as_uint(in.o[i].w);
+            const float4 ql = in.l[i];
+            accumulate(A.accum + 3 * (J.pixel_base + pixel), ql.x, ql.y, ql.z);
+          }
+        }
+      } else if (i < total) {
+        const unsigned long long g = inj_base + (i - n_in);
+        job = find_job(A.jobs, A.njobs, g, false);
+        const BJob& J = A.jobs[job];
+        const uint64_t p = J.pixel_base + (g - J.sample_base) / J.spp;
+        has_hit = __float_as_uint(A.cam[2 * p + 1].w) != kDead;  // else: a background pixel, nothing gathered
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, has_hit);
+      if (has_hit) list[npend + __popc(m & lt)] = make_uint2((uint32_t)i, job);
+      npend += (uint32_t)__popc(m);
+      __syncwarp();
+    }
+    while (npend >= 32u || (!more && npend > 0u)) {
+      const uint32_t cnt = npend < 32u ? npend : 32u;
+      npend -= cnt;
+      bool live = false;
+      swrx::PathState st;
+      uint32_t pixel = 0, sample = 0, slot = kDead, job = 0;
+      float t = 0.0f;
+      if (ln < cnt) {
+        const uint2 w = list[npend + ln];
+        const uint32_t e = w.x;
+        job = w.y;
+        const BJob& J = A.jobs[job];
+        if (e < n_in) {
+          const float4 qo = in.o[e], qd = in.d[e], qc = in.c[e];
+          const uint2 h = in.hit[e];
+          pixel = __float_as_uint(qo.w);
+          sample = __float_as_uint(qd.w);
+          const uint32_t meta = __float_as_uint(qc.w);
+          st.o = mk(qo.x, qo.y, qo.z);
+          st.d = mk(qd.x, qd.y, qd.z);
+          st.c = mk(qc.x, qc.y, qc.z);
+          st.i = (meta >> 8) & 0xFFu;
+          st.v = meta & 0xFFu;
+          const float4 ql = in.l[e];
+          st.L = mk(ql.x, ql.y, ql.z);
+          slot = h.x;
+          t = __uint_as_float(h.y);
+        } else {
+          const unsigned long long g = inj_base + (e - n_in);
+          const uint64_t local = g - J.sample_base;
+          pixel = (uint32_t)(local / J.spp);
+          sample = (uint32_t)(local % J.spp);
+          const uint64_t p = J.pixel_base + pixel;
+          const float4 r0 = A.cam[2 * p], r1 = A.cam[2 * p + 1];
+          const uint32_t bits = __float_as_uint(r1.w);
+          st.c = mk(1.0f, 1.0f, 1.0f);
+          st.L = mk(0.0f, 0.0f, 0.0f);
+          st.v = 0;
+          st.o = mk(r0.x, r0.y, r0.z);
+          st.d = mk(r1.x, r1.y, r1.z);
+          st.i = bits >> 27;
+          slot = bits & 0x07FFFFFFu;
+          t = r0.w;
+        }
+        const DevScene& sc = A.scenes[J.scene];
+        swrx::ShadeParams P;
+        P.seed = J.seed;
+        P.pixel = pixel;
+        P.sample = sample;
+        P.depth = J.depth;
+        P.mode = J.mode;
+        P.rr_depth = J.rr_depth;
+        P.rr_q = J.rr_q;
+        const uint32_t outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
+        if (outcome == swrx::kContinue) {
+          live = true;
+        } else {
+          unsigned long long* acc = A.accum + 3 * (J.pixel_base + pixel);
+          if (J.mode == 0) {
+            if (outcome == swrx::kEndLight) accumulate(acc, st.c.x, st.c.y, st.c.z);
+          } else {
+            accumulate(acc, st.L.x, st.L.y, st.L.z);
+          }
+        }
+      }
+      __syncwarp();  // the list slots just read may be refilled by the next chunk
+      const unsigned mask = __ballot_sync(0xffffffffu, live);
+      if (mask != 0u) {
+        unsigned obase = 0;
+        const unsigned leader = __ffs(mask) - 1;
+        if (ln == leader) obase = atomicAdd(&ctrl->count[parity ^ 1], (unsigned)__popc(mask));
+        obase = __shfl_sync(0xffffffffu, obase, leader);
+        if (live) {
+          const unsigned j = obase + __popc(mask & lt);
+          out.o[j] = make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel));
+          out.d[j] = make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample));
+          out.c[j] = make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((job << 16) | (st.i << 8) | st.v));
+          out.l[j] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+        }
       }
     }
-  } else if (i < n_in + n_inj) {
-    const unsigned long long g = inj_base + (i - n_in);
-    job = find_job(A.jobs, A.njobs, g, false);
-    const BJob& J = A.jobs[job];
-    const uint64_t p = J.pixel_base + (g - J.sample_base) / J.spp;
-    has_hit = __float_as_uint(A.cam[2 * p + 1].w) != kDead;  // else: a background pixel, nothing gathered
-  }
-  {
-    const unsigned m = __ballot_sync(0xffffffffu, has_hit);
-    unsigned base = 0;
-    if (lane() == 0 && m) base = atomicAdd(&nwork, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (has_hit) work[base + __popc(m & ((1u << lane()) - 1u))] = make_uint2(i, job);
-  }
-  __syncthreads();
-  const uint32_t cnt = nwork;
-  if ((threadIdx.x & ~31u) >= cnt) return;  // the whole warp: nothing listed for it
-
-  bool live = false;
-  swrx::PathState st;
-  uint32_t pixel = 0, sample = 0, slot = kDead;
-  float t = 0.0f;
-  job = 0;
-  if (threadIdx.x < cnt) {
-    const uint2 w = work[threadIdx.x];
-    const uint32_t e = w.x;
-    job = w.y;
-    const BJob& J = A.jobs[job];
-    if (e < n_in) {
-      const float4 qo = in.o[e], qd = in.d[e], qc = in.c[e];
-      const uint2 h = in.hit[e];
-      pixel = __float_as_uint(qo.w);
-      sample = __float_as_uint(qd.w);
-      const uint32_t meta = __float_as_uint(qc.w);
-      st.o = mk(qo.x, qo.y, qo.z);
-      st.d = mk(qd.x, qd.y, qd.z);
-      st.c = mk(qc.x, qc.y, qc.z);
-      st.i = (meta >> 8) & 0xFFu;
-      st.v = meta & 0xFFu;
-      const float4 ql = in.l[e];
-      st.L = mk(ql.x, ql.y, ql.z);
-      slot = h.x;
-      t = __uint_as_float(h.y);
-    } else {
-      const unsigned long long g = inj_base + (e - n_in);
-      const uint64_t local = g - J.sample_base;
-      pixel = (uint32_t)(local / J.spp);
-      sample = (uint32_t)(local % J.spp);
-      const uint64_t p = J.pixel_base + pixel;
-      const float4 r0 = A.cam[2 * p], r1 = A.cam[2 * p + 1];
-      const uint32_t bits = __float_as_uint(r1.w);
-      st.c = mk(1.0f, 1.0f, 1.0f);
-      st.L = mk(0.0f, 0.0f, 0.0f);
-      st.v = 0;
-      st.o = mk(r0.x, r0.y, r0.z);
-      st.d = mk(r1.x, r1.y, r1.z);
-      st.i = bits >> 27;
-      slot = bits & 0x07FFFFFFu;
-      t = r0.w;
-    }
-    const DevScene& sc = A.scenes[J.scene];
-    swrx::ShadeParams P;
-    P.seed = J.seed;
-    P.pixel = pixel;
-    P.sample = sample;
-    P.depth = J.depth;
-    P.mode = J.mode;
-    P.rr_depth = J.rr_depth;
-    P.rr_q = J.rr_q;
-    const uint32_t outcome = swrx::shade_vertex(sc.tris, sc.shade, sc.mats, sc.albedo, slot, t, P, st);
-    if (outcome == swrx::kContinue) {
-      live = true;
-    } else {
-      unsigned long long* acc = A.accum + 3 * (J.pixel_base + pixel);
-      if (J.mode == 0) {
-        if (outcome == swrx::kEndLight) accumulate(acc, st.c.x, st.c.y, st.c.z);
-      } else {
-        accumulate(acc, st.L.x, st.L.y, st.L.z);
-      }
-    }
-  }
-  const unsigned mask = __ballot_sync(0xffffffffu, live);
-  if (mask == 0u) return;
-  unsigned base = 0;
-  const unsigned leader = __ffs(mask) - 1;
-  if (lane() == leader) base = atomicAdd(&ctrl->count[parity ^ 1], (unsigned)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (live) {
-    const unsigned j = base + __popc(mask & ((1u << lane()) - 1u));
-    out.o[j] = make_float4(st.o.x, st.o.y, st.o.z, __uint_as_float(pixel));
-    out.d[j] = make_float4(st.d.x, st.d.y, st.d.z, __uint_as_float(sample));
-    out.c[j] = make_float4(st.c.x, st.c.y, st.c.z, __uint_as_float((job << 16) | (st.i << 8) | st.v));
-    out.l[j] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+    if (!more) break;
   }
 }
 
@@ -623,7 +629,14 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
   int per_sm = 0;
   SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_btrace, kTB, 0));
   const unsigned tgrid = (unsigned)(num_sms * std::max(per_sm, 1));
-  const unsigned sgrid = (capw + 255) / 256;
+  int shade_per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, k_bshade, 256, 0) != cudaSuccess) {
+    cudaGetLastError();
+    shade_per_sm = 1;
+  }
+  // persistent shading grid (its warps stride over the queue)
+  const unsigned sgrid = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>((capw + 255) / 256, (uint64_t)num_sms * std::max(shade_per_sm, 1)));
   auto queues = [&](int h, BQueue* Qh) {
     char* p = (char*)b->qbuf + (size_t)h * ((size_t)capw * (4 * sizeof(float4) + sizeof(uint2)) * 2);
     for (int k = 0; k < 2; ++k) {
