@@ -245,15 +245,22 @@ __global__ void __launch_bounds__(kBlock)
   uint32_t* list = pending[threadIdx.x >> 5];
   const uint64_t stride = (uint64_t)gridDim.x * kBlock;
   uint32_t npend = 0;  // entries in the warp's list (the same in every lane)
-  for (uint64_t base = (uint64_t)blockIdx.x * kBlock + (threadIdx.x & ~31u);; base += stride) {
+  // the hit word of entry i (the traced slot, or the camera record's slot bits), kDeadSlot for none
+  auto hit_word = [&](uint64_t i) -> uint32_t {
+    if (i < n_in) return in.hit[i].x;
+    if (i < total) return __float_as_uint(F.cam[2 * (size_t)((inj_base + (i - n_in)) / F.spp) + 1].w);
+    return kDeadSlot;
+  };
+  uint64_t base = (uint64_t)blockIdx.x * kBlock + (threadIdx.x & ~31u);
+  uint32_t word = hit_word(base + lane);
+  for (;; base += stride) {
     const bool more = base < total;
     if (more) {
       // entries without a hit: their dark end; the rest: listed
       const uint64_t i = base + lane;
       bool has_hit = false;
       if (i < n_in) {
-        const uint2 h = in.hit[i];
-        if (h.x != kDeadSlot) {
+        if (word != kDeadSlot) {
           has_hit = true;
         } else {
           const uint32_t pixel = __float_as_uint(__ldcs(&in.o[i].w));
@@ -266,19 +273,20 @@ __global__ void __launch_bounds__(kBlock)
           __stcs(F.contrib + (size_t)pixel * F.spp + sample, r);
         }
       } else if (i < total) {
-        const unsigned long long g = inj_base + (i - n_in);
-        const uint32_t pixel = (uint32_t)(g / F.spp);
-        if (__float_as_uint(F.cam[2 * (size_t)pixel + 1].w) != kDeadSlot) {
+        if (word != kDeadSlot) {
           has_hit = true;
         } else {
+          const unsigned long long g = inj_base + (i - n_in);
           const float4 r = (F.mode == 1) ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          __stcs(F.contrib + (size_t)pixel * F.spp + (uint32_t)(g % F.spp), r);
+          __stcs(F.contrib + (size_t)(g / F.spp) * F.spp + (uint32_t)(g % F.spp), r);
         }
       }
       const unsigned m = __ballot_sync(0xffffffffu, has_hit);
       if (has_hit) list[npend + __popc(m & lt)] = (uint32_t)i;
       npend += (uint32_t)__popc(m);
       __syncwarp();
+      // the next chunk's hit words are fetched now, so that their loads overlap the shading below
+      word = hit_word(base + stride + lane);
     }
     // a full warp of listed entries (or, after the last chunk, what is left) is shaded
     while (npend >= 32u || (!more && npend > 0u)) {
