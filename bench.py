@@ -32,11 +32,12 @@ sys.path.insert(0, ROOT)
 
 CONFIGS = {
     # name: scene parameters, image, spp, depth
-    # wave_size: paths in flight, 2^26 measured best for this image by the autotuner (2^24..2^26
-    # with refill 4-12 and shading blocks 256/512; the library's default of 2^23 bounds a scene's
-    # queue memory at 1.2 GB, 2^26 takes 9.7 GB)
+    # wave_size: paths in flight, 2^27 measured best for this image by the autotuner (2^24..2^27
+    # with refill 4-12 and shading blocks 256/512): the whole image's 132.7 M samples are in flight
+    # at once. The library's default of 2^23 bounds a scene's queue memory at 1.2 GB; 2^27 takes
+    # 19.3 GB
     "c2": dict(kind="terrain", cells=1024, tile=16, spheres=64, subdiv=4, lights=4, W=1920, H=1080, spp=64,
-               depth=8, seed=2024, microbench_rays=1 << 24, wave_size=1 << 26),
+               depth=8, seed=2024, microbench_rays=1 << 24, wave_size=1 << 27),
     "c1": dict(kind="cornell", W=256, H=256, spp=16, depth=5, seed=1),
     # the Cornell scene through the bidirectional tracer with the reference's own BDPT renderer
     # settings (res/renderer/SoftwareRendererBidirectionalPathTracer.renderer: 5/5/5)

@@ -29,7 +29,7 @@ import torch
 CACHE = os.environ.get("SWR_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "swr_b200", "tune.json"))
 
 BUILD_GRID = dict(width=[4, 8], max_leaf=[2, 3])
-RENDER_GRID = dict(wave_size=[1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26], refill=[4, 8, 16], block_size=[128, 256, 512],
+RENDER_GRID = dict(wave_size=[1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26, 1 << 27], refill=[4, 8, 16], block_size=[128, 256, 512],
                    trace_blocks=[0, 10])
 BATCH_GRID = dict(wave_size=[1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25], refill=[4, 8, 16])
 BDPT_GRID = dict(shade_batch=[12 | (16 << 8), 20 | (16 << 8), 24 | (16 << 8), 20 | (8 << 8), 20 | (24 << 8)],

@@ -1,6 +1,6 @@
 """The configuration the benchmark times, checked against the oracle: the terrain scene (2,424,840
 triangles in 4,164 objects) rendered with the reference's PathTracer semantics at depth 8 with
-2^26 paths in flight, per sample on image rows spread over the whole 1920x1080 image. Also a small
+2^27 paths in flight (the whole image at once), per sample on image rows spread over the whole 1920x1080 image. Also a small
 terrain at depth 8 with few and with many paths in flight, and batched jobs compared with the
 oracle directly (not only with single-scene renders).
 
@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 RTOL, ATOL = 1e-4, 1e-7
 
 # The benchmark's terrain image (bench.py, configuration c2): rank 0 renders with seed 1000.
-BENCH_W, BENCH_H, BENCH_SPP, BENCH_DEPTH, BENCH_SEED, BENCH_WAVE = 1920, 1080, 64, 8, 1000, 1 << 26
+BENCH_W, BENCH_H, BENCH_SPP, BENCH_DEPTH, BENCH_SEED, BENCH_WAVE = 1920, 1080, 64, 8, 1000, 1 << 27
 
 
 def _close(a, b):
@@ -75,10 +75,10 @@ def test_terrain_bench_image_vs_oracle(tmp_path):
     sc.close()
 
 
-@pytest.mark.parametrize("wave", [4096, 1 << 26])
+@pytest.mark.parametrize("wave", [4096, 1 << 27])
 def test_small_terrain_depth8_vs_oracle(tmp_path, wave):
     """Depth 8 on a terrain with few paths in flight (many injections and compactions) and with a
-    request for 2^26 (clamped to the image's samples): every pixel and sample against the oracle."""
+    request for 2^27 (clamped to the image's samples): every pixel and sample against the oracle."""
     s = scenes.terrain(9, str(tmp_path), cells=64, tile=16, spheres=8, sphere_subdiv=2, lights=2)
     sd = swr.load_scene(s["scene"], s["basepath"])
     assert sd.ranks_exact
