@@ -113,7 +113,10 @@ typedef struct swr_render_opts {
   uint32_t mode;           /* SWR_MODE_* */
   uint32_t rr_depth;       /* physical mode: Russian roulette at path vertices >= rr_depth (0=off) */
   float rr_survive;        /* physical mode: survival probability, (0, 1] */
-  uint32_t wave_size;      /* paths in flight, 0 = 2^23 (capped by the samples of a chunk); the
+  uint32_t wave_size;      /* paths in flight, 0 = 2^23 (capped by the samples of a chunk). Each
+                              path in flight holds 144 bytes of the scene's queue memory; a large
+                              image renders fastest with all of its samples in flight (1920x1080
+                              at 64 spp: 2^27 paths, 19.3 GB). The
                               bidirectional tracer: samples per chunk, 0 = as many as keep the
                               chunk's vertex tables within 2 GB */
   uint32_t block_size;     /* threads per block of the shading kernel, 0 = automatic */
