@@ -61,6 +61,7 @@ struct BCtrl {
   unsigned long long rays;
   unsigned long long rounds;      // shade/trace rounds run by the device-side loop
   unsigned long long max_rounds;  // its bound (every path ends within depth rounds of injection)
+  unsigned long long cam_cursor;  // next pixel of the persistent camera-prefix kernel
 };
 
 struct BQueue {
@@ -96,39 +97,90 @@ __device__ __forceinline__ uint32_t find_job(const BJob* jobs, uint32_t n, uint6
   return lo;
 }
 
+// Camera prefix of every pixel of every job, persistent as the single-scene k_camera: idle lanes
+// take the next pixels from ctrl->cam_cursor (refill), find their job by binary search and trace
+// the pixel-centre ray; a back-facing first hit restarts the lane's traversal past it (using up a
+// depth slot), so lanes do not wait for the warp's slowest pixel.
 __global__ void __launch_bounds__(kTB) k_bcamera(BArgs A, BCtrl* __restrict__ ctrl) {
   __shared__ uint2 stack[swrx::kStackShared * kTB];
-  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned ln = lane();
+  const unsigned lt = (1u << ln) - 1u;
+  const unsigned refill = A.refill ? A.refill : 8u;
+  swrx::Traversal tr;
+  const DevScene* sc = nullptr;
+  bool active = false, exhausted = false;
+  uint64_t p = 0;
+  uint32_t i = 0, depth = 0;
+  f3 d = mk(0.0f, 0.0f, 0.0f);
   unsigned traced = 0;
-  if (p < A.npix) {
-    const uint32_t j = find_job(A.jobs, A.njobs, p, true);
-    const BJob& J = A.jobs[j];
-    const DevScene& sc = A.scenes[J.scene];
-    const uint32_t pix = (uint32_t)(p - J.pixel_base);
-    f3 o = mk(J.org[0], J.org[1], J.org[2]);
-    const f3 d = swrx::primary_dir(J.vi, J.pi, pix % J.W, pix / J.W, J.W, J.H);
-    float4 r0 = make_float4(0, 0, 0, 0), r1 = make_float4(0, 0, 0, __uint_as_float(kDead));
-    for (uint32_t i = 0; i < J.depth; ++i) {
-      swrx::Hit h;
-      ++traced;
-      if (!swrx::trace_closest<false>(sc.nodes, sc.tris, sc.tri_boxes, sc.obj_boxes, o, d, stack + threadIdx.x,
-                                      kTB, h, nullptr))
-        break;
-      const f3 hp = swrx::hit_point(o, d, h.t);
-      const f3 n = swrx::shading_normal(sc.tris, sc.shade, h.slot, hp);
-      if (swrx::vdot(n, d) > 0.0f) {
-        o = swrx::vadd(hp, swrx::vscale(0.01f, d));
-        continue;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && (unsigned)__popc(idle) >= refill) {
+      unsigned long long base = 0;
+      if (ln == 0) base = atomicAdd(&ctrl->cam_cursor, (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= A.npix) exhausted = true;
+      if (!active) {
+        const uint64_t q = base + (unsigned)__popc(idle & lt);
+        if (q < A.npix) {
+          p = q;
+          i = 0;
+          const uint32_t j = find_job(A.jobs, A.njobs, p, true);
+          const BJob& J = A.jobs[j];
+          sc = &A.scenes[J.scene];
+          depth = J.depth;
+          const uint32_t pix = (uint32_t)(p - J.pixel_base);
+          d = swrx::primary_dir(J.vi, J.pi, pix % J.W, pix / J.W, J.W, J.H);
+          tr.init(mk(J.org[0], J.org[1], J.org[2]), d, stack + threadIdx.x, kTB);
+          ++traced;
+          active = true;
+        }
       }
-      r0 = make_float4(o.x, o.y, o.z, h.t);
-      r1 = make_float4(d.x, d.y, d.z, __uint_as_float(h.slot | (i << 27)));
-      break;
     }
-    A.cam[2 * p] = r0;
-    A.cam[2 * p + 1] = r1;
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active && tr.step<false>(sc->nodes, sc->tris, sc->tri_boxes, sc->obj_boxes, nullptr)) {
+      // depth slot i traced: a miss ends the prefix, a back face uses up the slot
+      float4 r0 = make_float4(0, 0, 0, 0), r1 = make_float4(0, 0, 0, __uint_as_float(kDead));
+      bool done = true;
+      if (tr.hit.slot != 0xFFFFFFFFu) {
+        const f3 o = tr.o;
+        const f3 hp = swrx::hit_point(o, d, tr.hit.t);
+        const f3 n = swrx::shading_normal(sc->tris, sc->shade, tr.hit.slot, hp);
+        if (swrx::vdot(n, d) > 0.0f) {
+          if (i + 1 < depth) {
+            tr.init(swrx::vadd(hp, swrx::vscale(0.01f, d)), d, stack + threadIdx.x, kTB);
+            ++i;
+            ++traced;
+            done = false;
+          }
+        } else {
+          r0 = make_float4(o.x, o.y, o.z, tr.hit.t);
+          r1 = make_float4(d.x, d.y, d.z, __uint_as_float(tr.hit.slot | (i << 27)));
+        }
+      }
+      if (done) {
+        A.cam[2 * p] = r0;
+        A.cam[2 * p + 1] = r1;
+        active = false;
+      }
+    }
   }
   for (int off = 16; off > 0; off >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, off);
-  if (lane() == 0 && traced) atomicAdd(&ctrl->rays, (unsigned long long)traced);
+  if (ln == 0 && traced) atomicAdd(&ctrl->rays, (unsigned long long)traced);
+}
+
+// persistent grid of the batch's camera-prefix kernel for np pixels
+static unsigned bcamera_grid(int num_sms, uint64_t np) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bcamera, kTB, 0) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const uint64_t need = (np + kTB - 1) / kTB;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)num_sms * std::max(per_sm, 1)));
 }
 
 __device__ __forceinline__ void accumulate(unsigned long long* acc, float r, float g, float b) {
@@ -624,7 +676,7 @@ int swr_render_batch(swr_batch* b, const swr_batch_job* jobs, uint32_t n, const 
     b->host_ctrl[h] = init;
   }
   SWR_CUDA(cudaMemcpyAsync(dctrl, b->host_ctrl, nsub * sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
-  k_bcamera<<<(unsigned)((pixels + kTB - 1) / kTB), kTB, 0, stream>>>(A, dctrl);
+  k_bcamera<<<bcamera_grid(num_sms, pixels), kTB, 0, stream>>>(A, dctrl);
   SWR_CUDA(cudaGetLastError());
   int per_sm = 0;
   SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_btrace, kTB, 0));
@@ -819,7 +871,7 @@ int swr_render_adjoint_batch(swr_batch* b, const swr_adjoint_job* jobs, uint32_t
   SWR_CUDA(cudaStreamSynchronize(stream));  // the pinned control block may still be in flight
   *b->host_ctrl = init;
   SWR_CUDA(cudaMemcpyAsync(b->ctrl, b->host_ctrl, sizeof(BCtrl), cudaMemcpyHostToDevice, stream));
-  k_bcamera<<<(unsigned)((pixels + kTB - 1) / kTB), kTB, 0, stream>>>(A, (BCtrl*)b->ctrl);
+  k_bcamera<<<bcamera_grid(num_sms, pixels), kTB, 0, stream>>>(A, (BCtrl*)b->ctrl);
   SWR_CUDA(cudaGetLastError());
   int per_sm = 0;
   SWR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_badjoint, kTB, 0));
