@@ -883,23 +883,45 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks)
   }
 }
 
-__global__ void k_resolve(Frame F, float* __restrict__ img) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= F.npix) return;
+// Per-pixel sum of the sample slots in sample order (path_tracer.cpp:28-37), 256 pixels per block.
+// A warp takes 32 consecutive pixels and loads their slots 8 samples at a time with coalesced loads
+// (each load instruction reads whole 128-byte lines) into a shared-memory tile padded to 9 slots
+// per pixel (conflict-free reads); each lane then adds its pixel's slots in sample order, as the
+// reference's renderPixel does.
+__global__ void __launch_bounds__(256) k_resolve(Frame F, float* __restrict__ img) {
+  __shared__ float4 tile[8][32 * 9];
+  const uint32_t w = threadIdx.x >> 5, lane = lane_id();
+  const uint64_t p0 = ((uint64_t)blockIdx.x * 8 + w) * 32;  // the warp's first pixel
+  if (p0 >= F.npix) return;
+  const uint32_t np = (uint32_t)((F.npix - p0) < 32 ? (F.npix - p0) : 32);
+  const uint32_t spp = F.spp;
+  float4* t = tile[w];
   float r = 0.0f, g = 0.0f, b = 0.0f;
-  const float4* c = F.contrib + (size_t)k * F.spp;
-  for (uint32_t s = 0; s < F.spp; ++s) {
-    const float4 v = c[s];
-    if (v.w != 0.0f) {
-      r = __fadd_rn(r, v.x);
-      g = __fadd_rn(g, v.y);
-      b = __fadd_rn(b, v.z);
+  for (uint32_t s0 = 0; s0 < spp; s0 += 8) {
+    const uint32_t ns = (spp - s0) < 8 ? (spp - s0) : 8;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint32_t e = lane + 32u * j, pe = e >> 3, se = e & 7u;
+      if (pe < np && se < ns) t[pe * 9 + se] = __ldcs(F.contrib + (size_t)(p0 + pe) * spp + s0 + se);
     }
+    __syncwarp();
+    if (lane < np) {
+      for (uint32_t k = 0; k < ns; ++k) {
+        const float4 v = t[lane * 9 + k];
+        if (v.w != 0.0f) {
+          r = __fadd_rn(r, v.x);
+          g = __fadd_rn(g, v.y);
+          b = __fadd_rn(b, v.z);
+        }
+      }
+    }
+    __syncwarp();
   }
+  if (lane >= np) return;
   // reference: finalColor *= 2.0f * M_PI * (1.0f / float(spp)), scalar and products in double
   const float inv = __fdiv_rn(1.0f, (float)F.spp_scale);
   const double s = (F.mode == 0) ? __dmul_rn(6.283185307179586, (double)inv) : (double)inv;
-  float* o = img + (size_t)(F.pixel0 - F.out0 + k) * 3;
+  float* o = img + (size_t)(F.pixel0 - F.out0 + p0 + lane) * 3;
   o[0] = __double2float_rn(__dmul_rn((double)r, s));
   o[1] = __double2float_rn(__dmul_rn((double)g, s));
   o[2] = __double2float_rn(__dmul_rn((double)b, s));
