@@ -22,6 +22,7 @@ RTOL, ATOL = 1e-4, 1e-7
 
 # The benchmark's terrain image (bench.py, configuration c2): rank 0 renders with seed 1000.
 BENCH_W, BENCH_H, BENCH_SPP, BENCH_DEPTH, BENCH_SEED, BENCH_WAVE = 1920, 1080, 64, 8, 1000, 1 << 27
+BENCH_SCENE = dict(seed=2024, cells=1024, tile=16, spheres=64, sphere_subdiv=4, lights=4)
 
 
 def _close(a, b):
@@ -49,7 +50,8 @@ def _check_rows(samples, img, osc, cam, W, H, spp, depth, seed, rows):
 def test_terrain_bench_image_vs_oracle(tmp_path):
     """The benchmarked render itself: same scene files, camera, seed, depth and paths in flight as
     bench.py's default run; eight image rows (15,360 pixels x 64 samples) against the oracle."""
-    s = scenes.terrain(2024, str(tmp_path), cells=1024, tile=16, spheres=64, sphere_subdiv=4, lights=4)
+    kw = dict(BENCH_SCENE)
+    s = scenes.terrain(kw.pop("seed"), str(tmp_path), **kw)
     sd = swr.load_scene(s["scene"], s["basepath"])
     assert sd.num_triangles == 2424840 and sd.ranks_exact
     sc = swr.Scene(sd)
